@@ -1,0 +1,332 @@
+/*
+ * prism_b200.h -- C-ABI of the B200 (sm_100a) implementation of Prism's
+ * finite-volume hot path: mesh flattening, face-loop assembly, gradients,
+ * BiCGSTAB/Jacobi and the SIMPLE/PISO/PRIME drivers.
+ *
+ * Conventions (all entry points):
+ *   - every function returns an int status (PRISM_OK == 0) and never throws;
+ *     prism_last_error() returns a thread-local message for the last failure;
+ *   - handles are opaque and own their device memory; destroy them with the
+ *     matching *_destroy function (children before the mesh);
+ *   - host buffers passed in are borrowed for the duration of the call only;
+ *   - vector fields are exchanged as structure-of-arrays: x[0..n), y[0..n),
+ *     z[0..n); tensors as 9 blocks of n values, block (3*i+j) = T(i,j);
+ *   - calls on one mesh (and the fields/equations built on it) are not
+ *     thread-safe, matching the single-threaded reference; all device work of
+ *     one mesh runs on the mesh's CUDA stream.
+ *
+ * Reference (eigemx/prism) interfaces replaced, by entry point:
+ *   prism_mesh_from_unv      mesh/unv.cpp:61-110 UnvToPMeshConverter +
+ *                            mesh/pmesh.cpp:10-49 PMesh ctor (face reorder)
+ *   prism_scalar_*           field/scalar.h:14-127 field::Scalar
+ *   prism_vector_*           field/vector.h:17-101 field::GeneralVector
+ *   prism_tensor_*           field/tensor.h:7-38 field::Tensor
+ *   prism_scalar_grad        gradient/gradient.h:12-43 IGradient::gradAtCell
+ *   prism_transport_*        equation/transport.h:27-97 eqn::Transport
+ *   prism_transport_add_*    scheme/convection/convection.h:50-136,
+ *                            scheme/diffusion/diffusion.h:42-79,
+ *                            scheme/source/{constant_scalar,divergence,gradient}.h,
+ *                            equation/symmetry.cpp:54-90
+ *   prism_solve              numerics/solver.h:43-49 ISolver::solve
+ *                            (BiCGSTAB numerics/bicgstab.cpp:7-9,
+ *                             Jacobi numerics/jacobi.cpp:5-9)
+ *   prism_solve_csr          numerics/solver.h:49 ISolver::step on a raw matrix
+ *   prism_simple_step        algorithm/SIMPLE.cpp:200-216 IncompressibleSIMPLE::step
+ *   prism_prime_step         algorithm/PRIME.cpp:11-37 PRIME::step
+ *   prism_piso_step          algorithm/PISO.cpp:10-55 PISO::step
+ *   prism_needs_pressure_reference  algorithm/SIMPLE.cpp:110-122
+ */
+#ifndef PRISM_B200_H
+#define PRISM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PRISM_OK 0
+#define PRISM_NOT_CONVERGED 1 /* Krylov iteration cap reached (reported, not fatal) */
+#define PRISM_BREAKDOWN 2     /* BiCGSTAB rho or omega became zero */
+#define PRISM_NONFINITE 3     /* NaN/Inf met in the system or the iterate */
+#define PRISM_BAD_ARG 4
+#define PRISM_CUDA_ERROR 5
+#define PRISM_INVALID_MESH 6  /* error::InvalidMesh (exceptions.h:20-27) */
+#define PRISM_NO_BC_HANDLER 7 /* error::NonImplementedBoundaryCondition (exceptions.h:9-18) */
+#define PRISM_SPIN_TIMEOUT 8  /* a bounded device-side wait expired */
+#define PRISM_INTERNAL 9
+#define PRISM_OUT_OF_MEMORY 10
+
+/* ---- enumerations ------------------------------------------------------- */
+/* element kinds of a UNV element list (unv.cpp:124-160) */
+#define PRISM_ELEM_LINE 1
+#define PRISM_ELEM_TRIANGLE 2
+#define PRISM_ELEM_QUAD 3
+#define PRISM_ELEM_TETRA 4
+#define PRISM_ELEM_WEDGE 5
+#define PRISM_ELEM_HEX 6
+
+/* boundary-condition kinds, i.e. the "type" strings of <field>.json */
+#define PRISM_BC_EMPTY 0          /* "empty" */
+#define PRISM_BC_FIXED 1          /* "fixed" */
+#define PRISM_BC_NOSLIP 2         /* "no-slip" */
+#define PRISM_BC_SYMMETRY 3       /* "symmetry" */
+#define PRISM_BC_OUTLET 4         /* "outlet" */
+#define PRISM_BC_ZERO_GRADIENT 5  /* "zero-gradient" */
+#define PRISM_BC_FIXED_GRADIENT 6 /* "fixed-gradient" */
+#define PRISM_BC_UNKNOWN 7        /* any other string: no handler registered */
+
+/* value kind of a boundary condition (mesh/boundary.h BoundaryConditionValueKind) */
+#define PRISM_BCV_NIL 0
+#define PRISM_BCV_SCALAR 1
+#define PRISM_BCV_VECTOR 2
+
+#define PRISM_GRAD_LEAST_SQUARES 0 /* gradient/least_squares.cpp */
+#define PRISM_GRAD_GREEN_GAUSS 1   /* gradient/green_gauss.cpp */
+
+#define PRISM_CONV_UPWIND 0 /* convection.cpp:89-128 weightsNVF */
+#define PRISM_CONV_CENTRAL 1
+#define PRISM_CONV_LINEAR_UPWIND 2 /* "SecondOrderUpwind" */
+#define PRISM_CONV_QUICK 3
+#define PRISM_CONV_FROMM 4
+#define PRISM_CONV_MINMOD 5
+#define PRISM_CONV_MUSCL 6
+#define PRISM_CONV_SMART 7
+
+#define PRISM_CORR_OVER_RELAXED 0 /* nonortho.cpp:7-21 */
+#define PRISM_CORR_MINIMUM 1
+#define PRISM_CORR_ORTHOGONAL 2
+
+#define PRISM_SRC_CONSTANT 0   /* source::ConstantScalar */
+#define PRISM_SRC_DIVERGENCE 1 /* source::Divergence */
+#define PRISM_SRC_GRADIENT 2   /* source::Gradient */
+
+#define PRISM_SIGN_POSITIVE 0
+#define PRISM_SIGN_NEGATIVE 1
+
+#define PRISM_SOLVER_BICGSTAB 0
+#define PRISM_SOLVER_JACOBI 1
+
+#define PRISM_PREC_FP64 0  /* FP64 Krylov */
+#define PRISM_PREC_MIXED 1 /* FP32 inner BiCGSTAB (FP64 dots) in FP64 iterative refinement */
+
+/* ---- handles ------------------------------------------------------------ */
+typedef struct PrismMesh PrismMesh;
+typedef struct PrismScalar PrismScalar;
+typedef struct PrismVector PrismVector;
+typedef struct PrismTensor PrismTensor;
+typedef struct PrismTransport PrismTransport;
+
+/* ---- errors --------------------------------------------------------------- */
+const char* prism_status_string(int status);
+const char* prism_last_error(void);
+
+/* ---- mesh ----------------------------------------------------------------- */
+/* A UNV mesh as the converter sees it: nodes, the element list in file order
+ * (boundary faces as TRIANGLE/QUAD elements, cells as TETRA/WEDGE/HEX), the
+ * element groups (boundary patches) and the patches defined by fields.json in
+ * their sorted-name order with their "empty" flag. Node and element indices
+ * are 0-based positions in these lists. */
+typedef struct {
+    int64_t n_nodes;
+    const double* xyz; /* 3*n_nodes, interleaved x,y,z */
+    int64_t n_elements;
+    const int32_t* elem_kind;     /* PRISM_ELEM_* */
+    const int64_t* elem_offsets;  /* n_elements+1 */
+    const int64_t* elem_nodes;    /* node indices */
+    int32_t n_groups;
+    const char* const* group_names;
+    const int32_t* group_is_vertex; /* 1 for node groups (skipped, unv.cpp:303) */
+    const int64_t* group_offsets;   /* n_groups+1 */
+    const int64_t* group_elements;  /* element indices */
+    int32_t n_patches;
+    const char* const* patch_names;
+    const int32_t* patch_is_empty;
+} PrismUnvMesh;
+
+typedef struct {
+    int64_t n_cells;
+    int64_t n_faces;
+    int64_t n_boundary_faces;
+    int64_t n_nonempty_boundary_faces;
+    int64_t nnz; /* entries of the CSR pattern (diagonal + face neighbours) */
+    int32_t n_patches;
+    int32_t n_gs_levels; /* levels of the Green-Gauss in-place sweep schedule */
+} PrismMeshInfo;
+
+/* Caller-allocated export buffers; any pointer may be NULL. Vectors are SoA. */
+typedef struct {
+    int64_t* owner;        /* n_faces */
+    int64_t* neighbor;     /* n_faces, -1 for boundary faces */
+    int32_t* face_patch;   /* n_faces, -1 for interior faces */
+    double* face_area;     /* n_faces */
+    double* face_normal;   /* 3*n_faces */
+    double* face_center;   /* 3*n_faces */
+    double* cell_volume;   /* n_cells */
+    double* cell_center;   /* 3*n_cells */
+    int64_t* cell_face_offsets; /* n_cells+1 */
+    int64_t* cell_faces;        /* face ids of each cell, in reference order */
+    int64_t* csr_rowptr;        /* n_cells+1 */
+    int64_t* csr_col;           /* nnz, column-sorted rows */
+    int64_t* patch_face_offsets; /* n_patches+1 */
+    int64_t* patch_faces;
+} PrismMeshExport;
+
+int prism_mesh_from_unv(const PrismUnvMesh* desc, PrismMesh** out);
+int prism_mesh_info(const PrismMesh* mesh, PrismMeshInfo* info);
+int prism_mesh_export(const PrismMesh* mesh, PrismMeshExport* out);
+int prism_mesh_destroy(PrismMesh* mesh);
+
+/* ---- fields -------------------------------------------------------------- */
+/* Boundary condition of one patch for one field (mesh/boundary.h:86-111). */
+typedef struct {
+    int32_t kind;       /* PRISM_BC_* */
+    int32_t value_kind; /* PRISM_BCV_* */
+    double value;       /* scalar value */
+    double vector[3];   /* vector value */
+} PrismBC;
+
+/* values: n_cells (NULL = zeros). bcs: one per patch, in patch order. */
+int prism_scalar_create(PrismMesh* mesh, const char* name, const double* values,
+                        int32_t grad_scheme, const PrismBC* bcs, PrismScalar** out);
+int prism_scalar_destroy(PrismScalar* s);
+/* values() = ... (bumps the event number, scalar.cpp:158-162) */
+int prism_scalar_set_values(PrismScalar* s, const double* values);
+int prism_scalar_get_values(const PrismScalar* s, double* values);
+/* setFaceValues (n_faces values) / clearFaceValues when face_values == NULL */
+int prism_scalar_set_face_values(PrismScalar* s, const double* face_values);
+/* valueAtFace for every face (n_faces); empty-patch faces are written as 0 */
+int prism_scalar_face_values(PrismScalar* s, double* out);
+/* gradAtCell for every cell (lazy recompute by event number), SoA 3*n_cells */
+int prism_scalar_grad(PrismScalar* s, double* grad_out);
+/* computeAllCellGradients (forced sweep) */
+int prism_scalar_compute_gradients(PrismScalar* s);
+
+/* values: SoA 3*n_cells (NULL = zeros) */
+int prism_vector_create(PrismMesh* mesh, const char* name, const double* values,
+                        int32_t grad_scheme, const PrismBC* bcs, PrismVector** out);
+/* GeneralVector::clone (vector.h:318-336): components share gradient schemes */
+int prism_vector_clone(const PrismVector* v, PrismVector** out);
+int prism_vector_destroy(PrismVector* v);
+/* borrowed component handle (x()/y()/z()) */
+int prism_vector_component(PrismVector* v, int32_t coord, PrismScalar** out);
+int prism_vector_set_values(PrismVector* v, const double* values);
+int prism_vector_get_values(const PrismVector* v, double* values);
+/* fluxAtFace for every face (n_faces); empty-patch faces are written as 0 */
+int prism_vector_face_flux(PrismVector* v, double* out);
+
+/* values: 9*n_cells SoA, NULL = identity */
+int prism_tensor_create(PrismMesh* mesh, const char* name, const double* values,
+                        PrismTensor** out);
+int prism_tensor_destroy(PrismTensor* t);
+
+/* ---- equations ------------------------------------------------------------ */
+int prism_transport_create(PrismScalar* phi, PrismTransport** out);
+int prism_transport_destroy(PrismTransport* eq);
+int prism_transport_add_convection(PrismTransport* eq, int32_t scheme, PrismVector* U);
+/* exactly one of kappa_scalar / kappa_tensor is non-NULL */
+int prism_transport_add_diffusion(PrismTransport* eq, int32_t corrected, int32_t corrector,
+                                  PrismScalar* kappa_scalar, PrismTensor* kappa_tensor);
+/* CONSTANT: src_scalar; DIVERGENCE: src_vector; GRADIENT: src_scalar + coord */
+int prism_transport_add_source(PrismTransport* eq, int32_t kind, int32_t sign,
+                               PrismScalar* src_scalar, PrismVector* src_vector, int32_t coord);
+/* eqn::boundary::Symmetry<Transport> (needs a convection and a diffusion scheme) */
+int prism_transport_add_symmetry_handler(PrismTransport* eq);
+int prism_transport_set_urf(PrismTransport* eq, double factor);
+int prism_transport_update_coeffs(PrismTransport* eq);
+int prism_transport_relax(PrismTransport* eq);
+int prism_transport_zero_coeffs(PrismTransport* eq);
+/* current A (nnz values in the CSR pattern order of prism_mesh_export) and b */
+int prism_transport_get_system(const PrismTransport* eq, double* csr_values, double* rhs);
+
+/* ---- solvers ------------------------------------------------------------- */
+typedef struct {
+    int32_t method;     /* PRISM_SOLVER_* */
+    int32_t precision;  /* PRISM_PREC_* (BiCGSTAB only) */
+    int64_t n_iter;     /* ISolver::solve n_iter */
+    double eps;         /* ISolver::solve eps (scaled residual) */
+    int64_t ref_cell;   /* -1: none */
+    double ref_value;
+    int32_t clear_coeffs;
+    double krylov_tol;      /* BiCGSTAB step: stop at ||b-Ax||/||b|| <= krylov_tol (0: default 1e-12) */
+    int64_t krylov_max_iter; /* 0: default 2*n_cells */
+    double inner_tol;        /* mixed precision: FP32 inner relative tolerance (0: default 1e-4) */
+} PrismSolveOpts;
+
+typedef struct {
+    int64_t iterations; /* outer step() calls, as SolverResult::iteration */
+    double initial_residual;
+    double final_residual;
+    int32_t converged;
+    int32_t status;           /* worst Krylov status met (PRISM_OK / NOT_CONVERGED / ...) */
+    int64_t krylov_iterations; /* total inner Krylov iterations */
+    double krylov_rel_residual; /* ||b-Ax||/||b|| after the last step */
+} PrismSolveResult;
+
+void prism_solve_opts_default(PrismSolveOpts* opts);
+int prism_solve(PrismTransport* eq, const PrismSolveOpts* opts, PrismSolveResult* result);
+/* x <- step(A, x, b) on a raw CSR matrix (host arrays, int64 indices) */
+int prism_solve_csr(int64_t n, const int64_t* rowptr, const int64_t* col, const double* values,
+                    const double* b, double* x, const PrismSolveOpts* opts,
+                    PrismSolveResult* result);
+
+/* ---- pressure-velocity coupling --------------------------------------------- */
+typedef struct {
+    double momentum_urf;
+    int64_t momentum_max_iter;
+    double momentum_residual;
+    double momentum_residual_stop;
+    int64_t non_ortho_correctors;
+    double pressure_urf;
+    int64_t pressure_max_iter;
+    double pressure_residual;
+    int64_t p_ref_cell; /* -1: none */
+    double p_ref_value;
+} PrismSIMPLEControls;
+
+typedef struct {
+    int64_t outer_iterations;
+    int64_t momentum_implicit_steps;
+    int64_t pressure_correction_steps;
+    double momentum_urf;
+    int64_t momentum_max_iter;
+    double momentum_residual;
+    double momentum_residual_stop;
+    int64_t non_ortho_correctors;
+    double pressure_urf;
+    int64_t pressure_max_iter;
+    double pressure_residual;
+    int64_t p_ref_cell;
+    double p_ref_value;
+} PrismPISOControls;
+
+typedef struct {
+    char field_name[32];
+    int64_t n_iterations;
+    double initial_residual;
+    double final_residual;
+    int32_t converged;
+} PrismReport;
+
+void prism_simple_controls_default(PrismSIMPLEControls* c);
+void prism_piso_controls_default(PrismPISOControls* c);
+/* solver_opts may be NULL: FP64 BiCGSTAB with default Krylov settings */
+int prism_simple_step(const PrismSIMPLEControls* controls, PrismTransport* const* momentum,
+                      int32_t n_momentum, PrismVector* U, PrismVector* mdot, PrismScalar* p,
+                      const PrismSolveOpts* solver_opts, PrismReport* reports,
+                      int32_t max_reports, int32_t* n_reports);
+int prism_prime_step(const PrismSIMPLEControls* controls, PrismTransport* const* momentum,
+                     int32_t n_momentum, PrismVector* U, PrismVector* mdot, PrismScalar* p,
+                     const PrismSolveOpts* solver_opts, PrismReport* reports,
+                     int32_t max_reports, int32_t* n_reports);
+int prism_piso_step(const PrismPISOControls* controls, PrismTransport* const* momentum,
+                    int32_t n_momentum, PrismVector* U, PrismVector* mdot, PrismScalar* p,
+                    const PrismSolveOpts* solver_opts, PrismReport* reports,
+                    int32_t max_reports, int32_t* n_reports);
+int prism_needs_pressure_reference(PrismScalar* p, int32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PRISM_B200_H */

@@ -1,0 +1,531 @@
+"""Python mirror of Prism's operator API over the C-ABI.
+
+Class and argument names follow the reference (field::Scalar/Vector/Tensor,
+eqn::Transport, scheme::convection::*, scheme::diffusion::*, scheme::source::*,
+solver::BiCGSTAB/Jacobi, algo::IncompressibleSIMPLE/PRIME/PISO); errors are
+raised as `PrismError` where the reference throws. Every object drives one
+loaded C-ABI library: by default the sm_100a library (`prism_b200.lib()`).
+The `lib` argument of `Mesh` lets a test build the same case on another
+library exposing the same ABI (the CPU oracle) to compare the two.
+"""
+import ctypes as C
+from dataclasses import dataclass, fields as dc_fields
+from typing import Optional
+
+import numpy as np
+
+from . import _abi as A
+from .io import Case, UnvData
+
+
+def _f64p(a):
+    return a.ctypes.data_as(A.pf64) if a is not None else None
+
+
+def _default_lib():
+    from . import lib
+    return lib()
+
+
+class Mesh:
+    """PMesh built from a UNV-form mesh and the case's patches (UnvToPMeshConverter)."""
+
+    def __init__(self, unv: UnvData, case: Case, lib=None):
+        self.lib = lib if lib is not None else _default_lib()
+        self.case = case
+        self._keep = []
+        d = A.UnvMesh()
+        d.n_nodes = unv.n_nodes
+        d.xyz = _f64p(unv.xyz)
+        d.n_elements = unv.n_elements
+        d.elem_kind = unv.elem_kind.ctypes.data_as(A.pi32)
+        d.elem_offsets = unv.elem_offsets.ctypes.data_as(A.pi64)
+        d.elem_nodes = unv.elem_nodes.ctypes.data_as(A.pi64)
+        gnames = (C.c_char_p * max(1, len(unv.groups)))(*[g[0].encode() for g in unv.groups])
+        gvert = np.array([1 if g[1] else 0 for g in unv.groups] or [0], dtype=np.int32)
+        goff = np.zeros(len(unv.groups) + 1, dtype=np.int64)
+        for i, g in enumerate(unv.groups):
+            goff[i + 1] = goff[i] + len(g[2])
+        gel = (np.concatenate([g[2] for g in unv.groups]).astype(np.int64)
+               if unv.groups else np.zeros(1, np.int64))
+        d.n_groups = len(unv.groups)
+        d.group_names = gnames
+        d.group_is_vertex = gvert.ctypes.data_as(A.pi32)
+        d.group_offsets = goff.ctypes.data_as(A.pi64)
+        d.group_elements = gel.ctypes.data_as(A.pi64)
+        pnames = (C.c_char_p * max(1, len(case.patch_names)))(*[p.encode() for p in case.patch_names])
+        pempty = np.array([1 if e else 0 for e in case.patch_is_empty] or [0], dtype=np.int32)
+        d.n_patches = len(case.patch_names)
+        d.patch_names = pnames
+        d.patch_is_empty = pempty.ctypes.data_as(A.pi32)
+        h = C.c_void_p()
+        self.lib.check(self.lib.mesh_from_unv(C.byref(d), C.byref(h)))
+        self.h = h
+        info = A.MeshInfo()
+        self.lib.check(self.lib.mesh_info(self.h, C.byref(info)))
+        self.info = info
+        self.n_cells = info.n_cells
+        self.n_faces = info.n_faces
+
+    def export(self):
+        """Flattened PMesh + CSR pattern as numpy arrays (SoA vectors)."""
+        i, nc, nf = self.info, self.info.n_cells, self.info.n_faces
+        cfo = np.zeros(nc + 1, np.int64)
+        e = A.MeshExport()
+        e.cell_face_offsets = cfo.ctypes.data_as(A.pi64)
+        self.lib.check(self.lib.mesh_export(self.h, C.byref(e)))
+        pfo = np.zeros(i.n_patches + 1, np.int64)
+        e = A.MeshExport()
+        e.patch_face_offsets = pfo.ctypes.data_as(A.pi64)
+        self.lib.check(self.lib.mesh_export(self.h, C.byref(e)))
+        out = dict(
+            owner=np.zeros(nf, np.int64), neighbor=np.zeros(nf, np.int64),
+            face_patch=np.zeros(nf, np.int32), face_area=np.zeros(nf), face_normal=np.zeros(3 * nf),
+            face_center=np.zeros(3 * nf), cell_volume=np.zeros(nc), cell_center=np.zeros(3 * nc),
+            cell_face_offsets=cfo, cell_faces=np.zeros(max(1, cfo[-1]), np.int64),
+            csr_rowptr=np.zeros(nc + 1, np.int64), csr_col=np.zeros(max(1, i.nnz), np.int64),
+            patch_face_offsets=pfo, patch_faces=np.zeros(max(1, pfo[-1]), np.int64))
+        e = A.MeshExport()
+        for k, v in out.items():
+            ptype = dict(e._fields_)[k]
+            setattr(e, k, v.ctypes.data_as(ptype))
+        self.lib.check(self.lib.mesh_export(self.h, C.byref(e)))
+        for k in ("face_normal", "face_center"):
+            out[k] = out[k].reshape(3, nf)
+        out["cell_center"] = out["cell_center"].reshape(3, nc)
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.mesh_destroy(self.h)
+            self.h = None
+
+
+class Scalar:
+    """field::Scalar. BCs and gradient scheme come from the case unless given."""
+
+    def __init__(self, name, mesh: Mesh, value=0.0, grad_scheme=None, bcs=None, _handle=None,
+                 _owner=None):
+        self.mesh, self.lib, self.name = mesh, mesh.lib, name
+        self._owner = _owner
+        if _handle is not None:
+            self.h = _handle
+            self._borrowed = True
+            return
+        self._borrowed = False
+        vals = np.full(mesh.n_cells, float(value)) if np.isscalar(value) else \
+            np.ascontiguousarray(value, dtype=np.float64)
+        gs = mesh.case.grad_scheme(name) if grad_scheme is None else grad_scheme
+        if bcs is None:
+            bcs = mesh.case.bcs(name) if name in mesh.case.fields else _default_bcs(mesh)
+        self._bcs = bcs
+        h = C.c_void_p()
+        self.lib.check(self.lib.scalar_create(mesh.h, name.encode(), _f64p(vals), gs, bcs, C.byref(h)))
+        self.h = h
+
+    def values(self):
+        out = np.zeros(self.mesh.n_cells)
+        self.lib.check(self.lib.scalar_get_values(self.h, _f64p(out)))
+        return out
+
+    def set_values(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        self.lib.check(self.lib.scalar_set_values(self.h, _f64p(v)))
+
+    def set_face_values(self, fv):
+        fv = None if fv is None else np.ascontiguousarray(fv, dtype=np.float64)
+        self.lib.check(self.lib.scalar_set_face_values(self.h, _f64p(fv)))
+
+    def clear_face_values(self):
+        self.set_face_values(None)
+
+    def face_values(self):
+        out = np.zeros(self.mesh.n_faces)
+        self.lib.check(self.lib.scalar_face_values(self.h, _f64p(out)))
+        return out
+
+    def grad(self):
+        """gradAtCell for every cell, shape (3, n_cells)."""
+        out = np.zeros(3 * self.mesh.n_cells)
+        self.lib.check(self.lib.scalar_grad(self.h, _f64p(out)))
+        return out.reshape(3, -1)
+
+    def compute_all_cell_gradients(self):
+        self.lib.check(self.lib.scalar_compute_gradients(self.h))
+
+    def __del__(self):
+        if not getattr(self, "_borrowed", True) and getattr(self, "h", None):
+            self.lib.scalar_destroy(self.h)
+            self.h = None
+
+
+def _default_bcs(mesh):
+    arr = (A.BC * max(1, mesh.info.n_patches))()
+    for p in range(mesh.info.n_patches):
+        # a field absent from the case has no boundary condition on any patch: asking for a
+        # boundary value raises, as BoundaryPatch::getBoundaryCondition does (boundary.cpp:425-444)
+        arr[p].kind = A.BC_EMPTY if mesh.case.patch_is_empty[p] else A.BC_UNKNOWN
+    return arr
+
+
+Pressure = Scalar
+
+
+class Vector:
+    """field::Vector / field::Velocity (three component Scalars)."""
+
+    def __init__(self, name, mesh: Mesh, value=(0.0, 0.0, 0.0), grad_scheme=None, bcs=None,
+                 _handle=None):
+        self.mesh, self.lib, self.name = mesh, mesh.lib, name
+        if _handle is None:
+            value = np.asarray(value, dtype=np.float64)
+            if value.ndim == 1 and value.shape[0] == 3:
+                vals = np.repeat(value[:, None], mesh.n_cells, axis=1).reshape(-1).copy()
+            else:
+                vals = np.ascontiguousarray(value, dtype=np.float64).reshape(-1)
+            gs = mesh.case.grad_scheme(name) if grad_scheme is None else grad_scheme
+            bcs = mesh.case.bcs(name) if bcs is None else bcs
+            self._bcs = bcs
+            h = C.c_void_p()
+            self.lib.check(self.lib.vector_create(mesh.h, name.encode(), _f64p(vals), gs, bcs,
+                                                  C.byref(h)))
+            _handle = h
+        self.h = _handle
+        comps = []
+        for k in range(3):
+            ch = C.c_void_p()
+            self.lib.check(self.lib.vector_component(self.h, k, C.byref(ch)))
+            comps.append(Scalar(name + "_" + "xyz"[k], mesh, _handle=ch, _owner=self))
+        self._x, self._y, self._z = comps
+
+    def x(self):
+        return self._x
+
+    def y(self):
+        return self._y
+
+    def z(self):
+        return self._z
+
+    def clone(self):
+        h = C.c_void_p()
+        self.lib.check(self.lib.vector_clone(self.h, C.byref(h)))
+        return Vector(self.name, self.mesh, _handle=h)
+
+    def values(self):
+        out = np.zeros(3 * self.mesh.n_cells)
+        self.lib.check(self.lib.vector_get_values(self.h, _f64p(out)))
+        return out.reshape(3, -1)
+
+    def set_values(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+        self.lib.check(self.lib.vector_set_values(self.h, _f64p(v)))
+
+    def face_flux(self):
+        out = np.zeros(self.mesh.n_faces)
+        self.lib.check(self.lib.vector_face_flux(self.h, _f64p(out)))
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.vector_destroy(self.h)
+            self.h = None
+
+
+Velocity = Vector
+
+
+class Tensor:
+    """field::Tensor; values (9, n_cells) SoA or None for the identity."""
+
+    def __init__(self, name, mesh: Mesh, value=None):
+        self.mesh, self.lib = mesh, mesh.lib
+        vals = None
+        if value is not None:
+            value = np.asarray(value, dtype=np.float64)
+            if value.shape == (3, 3):
+                vals = np.repeat(value.reshape(9, 1), mesh.n_cells, axis=1).reshape(-1).copy()
+            else:
+                vals = np.ascontiguousarray(value, dtype=np.float64).reshape(-1)
+        h = C.c_void_p()
+        self.lib.check(self.lib.tensor_create(mesh.h, name.encode(), _f64p(vals), C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.tensor_destroy(self.h)
+            self.h = None
+
+
+# ---- schemes (descriptors consumed by Transport) ------------------------------
+class _Convection:
+    kind = None
+
+    def __init__(self, U, phi):
+        self.U, self.phi = U, phi
+
+
+class convection:  # noqa: N801  (namespace scheme::convection)
+    pass
+
+
+for _name, _code in A.CONV.items():
+    setattr(convection, _name, type(_name, (_Convection,), {"code": _code}))
+convection.SecondOrderUpwind = convection.LinearUpwind
+
+
+class diffusion:  # noqa: N801  (namespace scheme::diffusion)
+    class NonCorrected:
+        corrected = 0
+
+        def __init__(self, kappa, phi, corrector=A.CORR_OVER_RELAXED):
+            self.kappa, self.phi, self.corrector = kappa, phi, corrector
+
+    class Corrected(NonCorrected):
+        corrected = 1
+
+
+class source:  # noqa: N801  (namespace scheme::source)
+    class ConstantScalar:
+        def __init__(self, phi, sign=A.SIGN_POSITIVE):
+            self.phi, self.sign = phi, sign
+
+    class Divergence:
+        def __init__(self, U, sign=A.SIGN_POSITIVE):
+            self.U, self.sign = U, sign
+
+    class Gradient:
+        def __init__(self, phi, coord, sign=A.SIGN_POSITIVE):
+            self.phi, self.coord, self.sign = phi, coord, sign
+
+
+class Transport:
+    """eqn::Transport(schemes...): the conserved field is the first scheme's field."""
+
+    def __init__(self, *schemes):
+        first = schemes[0]
+        phi = first.phi
+        self.phi, self.lib = phi, phi.lib
+        self._keep = list(schemes)
+        h = C.c_void_p()
+        self.lib.check(self.lib.transport_create(phi.h, C.byref(h)))
+        self.h = h
+        for s in schemes:
+            if isinstance(s, _Convection):
+                self.lib.check(self.lib.transport_add_convection(self.h, s.code, s.U.h))
+            elif isinstance(s, diffusion.NonCorrected):
+                ks = s.kappa.h if isinstance(s.kappa, Scalar) else None
+                kt = s.kappa.h if isinstance(s.kappa, Tensor) else None
+                self.lib.check(self.lib.transport_add_diffusion(self.h, s.corrected, s.corrector,
+                                                                ks, kt))
+            elif isinstance(s, source.ConstantScalar):
+                self.lib.check(self.lib.transport_add_source(self.h, A.SRC_CONSTANT, s.sign,
+                                                             s.phi.h, None, 0))
+            elif isinstance(s, source.Divergence):
+                self.lib.check(self.lib.transport_add_source(self.h, A.SRC_DIVERGENCE, s.sign,
+                                                             None, s.U.h, 0))
+            elif isinstance(s, source.Gradient):
+                self.lib.check(self.lib.transport_add_source(self.h, A.SRC_GRADIENT, s.sign,
+                                                             s.phi.h, None, s.coord))
+            else:
+                raise TypeError(f"unknown scheme {s!r}")
+
+    def field(self):
+        return self.phi
+
+    def add_symmetry_handler(self):
+        self.lib.check(self.lib.transport_add_symmetry_handler(self.h))
+
+    def set_under_relax_factor(self, f):
+        self.lib.check(self.lib.transport_set_urf(self.h, float(f)))
+
+    def update_coeffs(self):
+        self.lib.check(self.lib.transport_update_coeffs(self.h))
+
+    def relax(self):
+        self.lib.check(self.lib.transport_relax(self.h))
+
+    def zero_out_coeffs(self):
+        self.lib.check(self.lib.transport_zero_coeffs(self.h))
+
+    def system(self):
+        """(csr values, rhs) of the current A and b."""
+        mesh = self.phi.mesh
+        vals = np.zeros(max(1, mesh.info.nnz))
+        rhs = np.zeros(mesh.n_cells)
+        self.lib.check(self.lib.transport_get_system(self.h, _f64p(vals), _f64p(rhs)))
+        return vals[: mesh.info.nnz], rhs
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.transport_destroy(self.h)
+            self.h = None
+
+
+Momentum = Transport
+
+
+# ---- solvers ---------------------------------------------------------------------
+@dataclass
+class SolverResult:
+    iteration: int
+    initial_residual: float
+    final_residual: float
+    converged: bool
+    status: int
+    krylov_iterations: int
+    krylov_rel_residual: float
+
+
+def _solve_opts(lib, method, precision, n_iter, eps, ref_cell, ref_value, clear, krylov_tol,
+                krylov_max_iter, inner_tol):
+    o = A.SolveOpts()
+    lib.solve_opts_default(C.byref(o))
+    o.method, o.precision, o.n_iter, o.eps = method, precision, n_iter, eps
+    o.ref_cell = -1 if ref_cell is None else ref_cell
+    o.ref_value, o.clear_coeffs = ref_value, 1 if clear else 0
+    if krylov_tol:
+        o.krylov_tol = krylov_tol
+    if krylov_max_iter:
+        o.krylov_max_iter = krylov_max_iter
+    if inner_tol:
+        o.inner_tol = inner_tol
+    return o
+
+
+class _Solver:
+    method = A.SOLVER_BICGSTAB
+
+    def __init__(self, precision=A.PREC_FP64, krylov_tol=0.0, krylov_max_iter=0, inner_tol=0.0):
+        self.precision, self.krylov_tol = precision, krylov_tol
+        self.krylov_max_iter, self.inner_tol = krylov_max_iter, inner_tol
+
+    def opts(self, lib, n_iter=10, eps=1e-7, ref_cell=None, ref_value=0.0, clear_coeffs=True):
+        return _solve_opts(lib, self.method, self.precision, n_iter, eps, ref_cell, ref_value,
+                           clear_coeffs, self.krylov_tol, self.krylov_max_iter, self.inner_tol)
+
+    def solve(self, eqn: Transport, n_iter=10, eps=1e-7, ref_cell=None, ref_value=0.0,
+              clear_coeffs=True) -> SolverResult:
+        """ISolver::solve (numerics/solver.cpp:27-82)."""
+        o = self.opts(eqn.lib, n_iter, eps, ref_cell, ref_value, clear_coeffs)
+        r = A.SolveResult()
+        eqn.lib.check(eqn.lib.solve(eqn.h, C.byref(o), C.byref(r)))
+        return SolverResult(r.iterations, r.initial_residual, r.final_residual, bool(r.converged),
+                            r.status, r.krylov_iterations, r.krylov_rel_residual)
+
+    def step(self, lib, rowptr, col, values, x, b):
+        """ISolver::step on a raw CSR matrix; returns the new x."""
+        rowptr = np.ascontiguousarray(rowptr, np.int64)
+        col = np.ascontiguousarray(col, np.int64)
+        values = np.ascontiguousarray(values, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.array(x, dtype=np.float64)
+        o = self.opts(lib)
+        r = A.SolveResult()
+        lib.check(lib.solve_csr(len(b), rowptr.ctypes.data_as(A.pi64), col.ctypes.data_as(A.pi64),
+                                _f64p(values), _f64p(b), _f64p(x), C.byref(o), C.byref(r)))
+        return x
+
+
+class BiCGSTAB(_Solver):
+    method = A.SOLVER_BICGSTAB
+
+
+class Jacobi(_Solver):
+    method = A.SOLVER_JACOBI
+
+
+# ---- pressure-velocity coupling ------------------------------------------------------
+@dataclass
+class SIMPLEControls:
+    momentum_urf: float = 0.7
+    momentum_max_iter: int = 3
+    momentum_residual: float = 1e-7
+    momentum_residual_stop: float = 1e-5
+    non_ortho_correctors: int = 2
+    pressure_urf: float = 0.3
+    pressure_max_iter: int = 5
+    pressure_residual: float = 1e-7
+    p_ref_cell: Optional[int] = None
+    p_ref_value: float = 0.0
+
+    def to_c(self):
+        c = A.SIMPLEControls()
+        for f in dc_fields(self):
+            v = getattr(self, f.name)
+            setattr(c, f.name, -1 if (f.name == "p_ref_cell" and v is None) else v)
+        return c
+
+
+@dataclass
+class PISOControls:
+    outer_iterations: int = 1
+    momentum_implicit_steps: int = 1
+    pressure_correction_steps: int = 2
+    momentum_urf: float = 1.0
+    momentum_max_iter: int = 3
+    momentum_residual: float = 1e-4
+    momentum_residual_stop: float = 1e-5
+    non_ortho_correctors: int = 2
+    pressure_urf: float = 1.0
+    pressure_max_iter: int = 5
+    pressure_residual: float = 1e-4
+    p_ref_cell: Optional[int] = None
+    p_ref_value: float = 0.0
+
+    def to_c(self):
+        c = A.PISOControls()
+        for f in dc_fields(self):
+            v = getattr(self, f.name)
+            setattr(c, f.name, -1 if (f.name == "p_ref_cell" and v is None) else v)
+        return c
+
+
+@dataclass
+class ReportEntry:
+    field_name: str
+    n_iterations: int
+    initial_residual: float
+    final_residual: float
+    converged: bool
+
+
+class _PressureLinked:
+    fn = None
+
+    def __init__(self, controls=None, solver: Optional[_Solver] = None):
+        self.controls = controls if controls is not None else self.default_controls()
+        self.solver = solver if solver is not None else BiCGSTAB()
+
+    def step(self, momentum_predictors, U, mdot, p):
+        lib = U.lib
+        eqs = (C.c_void_p * len(momentum_predictors))(*[e.h.value for e in momentum_predictors])
+        c = self.controls.to_c()
+        o = self.solver.opts(lib)
+        reps = (A.Report * 64)()
+        n = C.c_int32()
+        lib.check(getattr(lib, self.fn)(C.byref(c), eqs, len(momentum_predictors), U.h, mdot.h,
+                                        p.h, C.byref(o), reps, 64, C.byref(n)))
+        return [ReportEntry(r.field_name.decode(), r.n_iterations, r.initial_residual,
+                            r.final_residual, bool(r.converged)) for r in reps[: min(n.value, 64)]]
+
+
+class IncompressibleSIMPLE(_PressureLinked):
+    fn = "simple_step"
+    default_controls = SIMPLEControls
+
+
+class PRIME(_PressureLinked):
+    fn = "prime_step"
+    default_controls = SIMPLEControls
+
+
+class PISO(_PressureLinked):
+    fn = "piso_step"
+    default_controls = PISOControls
+
+
+def needs_pressure_reference(p: Scalar) -> bool:
+    out = C.c_int32()
+    p.lib.check(p.lib.needs_pressure_reference(p.h, C.byref(out)))
+    return bool(out.value)
