@@ -1,0 +1,346 @@
+"""Benchmark of the sm_100a Prism hot path.
+
+Headline workload (N=1): steady lid-driven cavity, Re=100 (nu=0.01, lid u=1),
+Upwind convection + Corrected diffusion + pressure-gradient source, SIMPLE with
+urf 0.7/0.3 (configs[1]'s recipe) on 1448x1448x1 hexes (2,096,704 cells): the
+"2M-cell SIMPLE it/s" of the metric. One step = one SIMPLE outer iteration
+(2 momentum solves + 3 pressure solves, each step() solved to ||b-Ax|| <=
+1e-12 ||b|| like the reference's machine-precision step). Inputs live in HBM;
+the working set (~1 GB) is larger than L2, so no flush is needed.
+
+Also reported: time to 1e-8 relative error of the 128^3 jittered-hex MUSCL
+transport problem, FP64 vs FP32-inner/FP64-refinement BiCGSTAB ("s_to_1e8"),
+and the live SpMV bandwidth (CUDA events around the BiCGSTAB SpMV launches in
+the timed region). --impl reference times the CPU restatement of the
+reference (single-threaded, like the reference) on a bounded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s-to-1e-8 err (FP32+refine vs FP64 GPU), 2M-cell SIMPLE it/s, SpMV HBM GB/s"
+N_CAVITY = 1448
+N_CPU = 362  # bounded CPU sample: 1/16 of the cells
+UNIT = "SIMPLE it/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([t.strip() for t in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 3 + k and r[3 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        import datetime
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_simple_sample(steps=1):
+    """The CPU restatement of the reference (oracle) on a 362^2 cavity: seconds per SIMPLE step."""
+    import oracle
+    from tests import cases
+    from prism_b200 import api
+    lib = oracle.lib()
+    mesh, U, p, nu, mdot, eqs = cases.cavity(N_CPU, lib)
+    simple = api.IncompressibleSIMPLE(api.SIMPLEControls())
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        simple.step(eqs, U, mdot, p)
+    dt = (time.perf_counter() - t0) / steps
+    scale = (N_CPU * N_CPU) / float(N_CAVITY * N_CAVITY)
+    return scale / dt, dt
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    times = []
+    for i in range(args.warmup + args.steps):
+        it_s, dt = cpu_simple_sample(1)
+        if i >= args.warmup:
+            times.append(dt)
+    dt = sum(times) / len(times)
+    scale = (N_CPU * N_CPU) / float(N_CAVITY * N_CAVITY)
+    value = scale / dt
+    sample = (f"one SIMPLE outer iteration of the {N_CPU}x{N_CPU}x1 cavity ({N_CPU * N_CPU} cells) per step, "
+              f"it/s scaled by cells ({N_CPU * N_CPU}/{N_CAVITY * N_CAVITY}); single-threaded like the reference")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"cavity SIMPLE {N_CAVITY}x{N_CAVITY}x1 (bounded CPU sample, see cpu_baseline)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def transport_time_to_tol(lib, n, precision, ref, tol, max_outer, krylov_tol):
+    """Outer iterations (assemble + one BiCGSTAB step) of the MUSCL transport problem from T=0
+    until ||T - T_ref|| / ||T_ref|| <= tol; returns (device seconds, outer iterations, error)."""
+    import numpy as np
+    import torch
+    from prism_b200 import api
+    from tests import cases
+    mesh, T, U, eqn = cases.transport_c3(n, lib)
+    solver = api.BiCGSTAB(precision=precision, krylov_tol=krylov_tol, krylov_max_iter=20000, inner_tol=1e-4)
+    total, err, k = 0.0, float("inf"), 0
+    nref = np.linalg.norm(ref)
+    for k in range(1, max_outer + 1):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        solver.solve(eqn, 1, 0.0)
+        e1.record()
+        torch.cuda.synchronize()
+        total += e0.elapsed_time(e1) / 1000.0
+        err = float(np.linalg.norm(T.values() - ref) / nref)
+        if err <= tol:
+            break
+    return total, k, err
+
+
+def transport_reference(lib, n, max_outer=400):
+    import numpy as np
+    from prism_b200 import api
+    from tests import cases
+    mesh, T, U, eqn = cases.transport_c3(n, lib)
+    solver = api.BiCGSTAB(krylov_tol=1e-13, krylov_max_iter=40000)
+    prev = None
+    for k in range(max_outer):
+        solver.solve(eqn, 1, 0.0)
+        v = T.values()
+        if prev is not None and np.linalg.norm(v - prev) <= 1e-14 * np.linalg.norm(v):
+            break
+        prev = v
+    return T.values(), k + 1
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import prism_b200
+    from prism_b200 import _abi as A
+    from prism_b200 import api
+    from tests import cases
+
+    torch.cuda.set_device(local)
+    lib = prism_b200.lib()
+    hbm, peak_kind = peaks()
+
+    t_build = time.perf_counter()
+    mesh, U, p, nu, mdot, eqs = cases.cavity(N_CAVITY, lib)
+    t_build = time.perf_counter() - t_build
+    n = mesh.n_cells
+    solver = api.BiCGSTAB(krylov_tol=1e-12, krylov_max_iter=30000)
+    simple = api.IncompressibleSIMPLE(api.SIMPLEControls(), solver=solver)
+
+    # device-resident run
+    for _ in range(args.warmup):
+        simple.step(eqs, U, mdot, p)
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    lib.check(lib.profile_start(4096))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    reports = []
+    for _ in range(args.steps):
+        reports = simple.step(eqs, U, mdot, p)
+    e1.record()
+    torch.cuda.synchronize()
+    prof = A.Profile()
+    lib.check(lib.profile_stop(ctypes.byref(prof)))
+    clk = clocks.stop()
+    barrier(world)
+    t_dev = max_over_ranks(world, e0.elapsed_time(e1) / 1000.0)
+    value = world * args.steps / t_dev
+
+    # end to end through the public API with pinned host buffers
+    hU = torch.empty(3 * n, dtype=torch.float64, pin_memory=True).numpy()
+    hp = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hU[:] = U.values().reshape(-1)
+    hp[:] = p.values()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        lib.check(lib.vector_set_values(U.h, hU.ctypes.data_as(A.pf64)))
+        lib.check(lib.scalar_set_values(p.h, hp.ctypes.data_as(A.pf64)))
+        simple.step(eqs, U, mdot, p)
+        lib.check(lib.vector_get_values(U.h, hU.ctypes.data_as(A.pf64)))
+        lib.check(lib.scalar_get_values(p.h, hp.ctypes.data_as(A.pf64)))
+    t1.record()
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(world, t0.elapsed_time(t1) / 1000.0)
+    e2e = world * args.steps / t_e2e
+
+    # SpMV roofline from the live samples
+    spmv_ms = prof.fp64_ms / max(prof.fp64_launches, 1)
+    spmv_bytes = prof.fp64_bytes / max(prof.fp64_launches, 1)
+    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9 if prof.fp64_launches else None
+    traffic = None
+    prof_file = os.path.join(ROOT, "profiles", "spmv_fp64_traffic.json")
+    if os.path.exists(prof_file):
+        with open(prof_file) as fh:
+            tr = json.load(fh)
+        # DRAM bytes per row measured by ncu on a smaller matrix, scaled to this matrix's rows
+        traffic = tr["dram_bytes_per_row"] * n
+    roof = {"kernel": "spmv_kernel<double,1> (SELL-32 SpMV + fused dot, BiCGSTAB)", "bound": "hbm",
+            "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": achieved / hbm if achieved else None, "traffic": traffic,
+            "algorithmic_bytes_per_launch": spmv_bytes, "avg_launch_ms": spmv_ms,
+            "sampled_launches": prof.fp64_launches}
+
+    extra = {}
+    if rank == 0 and not args.skip_transport:
+        nt = args.transport_n
+        ref, nref = transport_reference(lib, nt)
+        t64, k64, err64 = transport_time_to_tol(lib, nt, A.PREC_FP64, ref, 1e-8, 400, 1e-10)
+        t32, k32, err32 = transport_time_to_tol(lib, nt, A.PREC_MIXED, ref, 1e-8, 400, 1e-10)
+        extra["s_to_1e8"] = {"workload": f"{nt}^3 jittered-hex MUSCL + Corrected transport ({nt ** 3} cells)",
+                             "fp64_s": t64, "fp64_outer": k64, "fp64_err": err64,
+                             "mixed_s": t32, "mixed_outer": k32, "mixed_err": err32,
+                             "speedup": t64 / t32 if t32 > 0 else None,
+                             "reference_solution": f"GPU FP64, outer iterations to a 1e-14 fixed point ({nref})"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        it_s, dt = cpu_simple_sample(1)
+        cpu = {"value": it_s, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"one SIMPLE outer iteration of the {N_CPU}x{N_CPU}x1 cavity ({dt:.1f} s), "
+                         f"it/s scaled by the cell ratio {N_CPU * N_CPU}/{N_CAVITY * N_CAVITY}"}
+
+    if rank == 0:
+        # kernel launches per step, counted from the solver's iteration counts
+        kry = sum(r.n_iterations for r in reports)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"cavity SIMPLE {N_CAVITY}x{N_CAVITY}x1 ({n} cells), Re=100, Upwind + "
+                                       "Corrected, urf 0.7/0.3, BiCGSTAB(Jacobi) to 1e-12",
+                           "cells": n, "l2": "inputs larger than L2 (no flush)",
+                           "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+                           "mesh_build_s": t_build},
+                "spmv_gbs": achieved, "roofline": roof, "clocks": clk,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(hU.nbytes + hp.nbytes),
+                        "d2h_bytes_per_step": int(hU.nbytes + hp.nbytes)},
+                "gpu_launches": None, "cpu_baseline": cpu,
+                "last_step_reports": [(r.field_name, r.n_iterations) for r in reports]}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--skip-transport", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--transport-n", type=int, default=128)
+    args = ap.parse_args()
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

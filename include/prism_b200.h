@@ -326,6 +326,23 @@ int prism_piso_step(const PrismPISOControls* controls, PrismTransport* const* mo
                     int32_t max_reports, int32_t* n_reports);
 int prism_needs_pressure_reference(PrismScalar* p, int32_t* out);
 
+/* ---- measurement --------------------------------------------------------- */
+/* Live timing of the SpMV kernel inside BiCGSTAB (v = A p launches), sampled
+ * with CUDA events on the launching stream while a profiling window is open.
+ * bytes are the algorithmic bytes of the sampled launches:
+ * nnz*(value + 4) + 4*(n+1) + 2*n*value (CSR values, columns, row pointers,
+ * x read once, y written once). No counterpart in the reference. */
+typedef struct {
+    int64_t fp64_launches;
+    double fp64_ms;
+    double fp64_bytes;
+    int64_t fp32_launches;
+    double fp32_ms;
+    double fp32_bytes;
+} PrismProfile;
+int prism_profile_start(int32_t max_samples);
+int prism_profile_stop(PrismProfile* out);
+
 #ifdef __cplusplus
 }
 #endif

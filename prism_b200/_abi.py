@@ -100,6 +100,11 @@ class Report(C.Structure):
                 ("final_residual", f64), ("converged", i32)]
 
 
+class Profile(C.Structure):
+    _fields_ = [("fp64_launches", i64), ("fp64_ms", f64), ("fp64_bytes", f64),
+                ("fp32_launches", i64), ("fp32_ms", f64), ("fp32_bytes", f64)]
+
+
 PP = C.POINTER(P)
 # name -> (restype, argtypes); every int-returning entry point returns a status.
 SIGNATURES = {
@@ -149,6 +154,8 @@ SIGNATURES = {
     "piso_step": (C.c_int, [C.POINTER(PISOControls), PP, i32, P, P, P, C.POINTER(SolveOpts),
                             C.POINTER(Report), i32, pi32]),
     "needs_pressure_reference": (C.c_int, [P, pi32]),
+    "profile_start": (C.c_int, [i32]),
+    "profile_stop": (C.c_int, [C.POINTER(Profile)]),
 }
 
 
@@ -161,6 +168,9 @@ class PrismError(RuntimeError):
         self.status = status
 
 
+GPU_ONLY = {"profile_start", "profile_stop"}
+
+
 class Bound:
     """Entry points of one loaded library, addressed without their prefix."""
 
@@ -169,6 +179,8 @@ class Bound:
         self.prefix = prefix
         names = SIGNATURES if required is None else {k: SIGNATURES[k] for k in required}
         for name, (res, args) in names.items():
+            if not hasattr(lib, prefix + name) and name in GPU_ONLY:
+                continue
             fn = getattr(lib, prefix + name)
             fn.restype = res
             fn.argtypes = args

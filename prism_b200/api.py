@@ -191,21 +191,22 @@ class Vector:
                                                   C.byref(h)))
             _handle = h
         self.h = _handle
-        comps = []
-        for k in range(3):
-            ch = C.c_void_p()
-            self.lib.check(self.lib.vector_component(self.h, k, C.byref(ch)))
-            comps.append(Scalar(name + "_" + "xyz"[k], mesh, _handle=ch, _owner=self))
-        self._x, self._y, self._z = comps
+
+    def _component(self, k):
+        # a borrowed handle wrapped on demand; the wrapper keeps this vector alive
+        # (no reference cycle, so finalisation order always follows ownership)
+        ch = C.c_void_p()
+        self.lib.check(self.lib.vector_component(self.h, k, C.byref(ch)))
+        return Scalar(self.name + "_" + "xyz"[k], self.mesh, _handle=ch, _owner=self)
 
     def x(self):
-        return self._x
+        return self._component(0)
 
     def y(self):
-        return self._y
+        return self._component(1)
 
     def z(self):
-        return self._z
+        return self._component(2)
 
     def clone(self):
         h = C.c_void_p()

@@ -1,0 +1,48 @@
+// assemble.h -- launch interface of the assembly kernels.
+#pragma once
+
+#include "common.h"
+#include "views.h"
+
+namespace pb {
+
+constexpr int MAX_SOURCES = 4;
+
+struct ConvDesc {
+    int scheme;
+    VectorView U;
+};
+struct DiffDesc {
+    int corrected, corrector, kappa_tensor;
+    ScalarView ks;
+    TensorView kt;
+};
+struct SourceDesc {
+    int kind, sign, coord;
+    ScalarView s;
+    VectorView U;
+};
+
+struct AssembleParams {
+    MeshView m;
+    ScalarView phi;
+    int phi_coord;
+    int has_conv, has_diff, conv_first, need_grad;
+    int nsrc, symmetry, accumulate;
+    ConvDesc conv;
+    DiffDesc diff;
+    SourceDesc src[MAX_SOURCES];
+    const int* ca_off;  // cell -> faces in insertion order
+    const int* ca_face;
+    const int* ca_pos;  // SELL position of (c, other), -1 on boundary
+    double* A;          // SELL values
+    double* b;
+    double* bconv;      // accumulated scheme right-hand sides
+    double* bdiff;
+};
+
+void launchAssemble(const AssembleParams& P, cudaStream_t s);
+void launchRelax(double* A, double* b, const int* diag_pos, const double* phi, double alpha, int n, cudaStream_t s);
+void launchPin(double* A, double* b, int pos, int row, double ref_value, cudaStream_t s);
+
+}  // namespace pb

@@ -1,0 +1,85 @@
+// common.h -- error handling, device buffers and launch helpers shared by the
+// host runtime and the sm_100a kernels of libprism_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/prism_b200.h"
+
+namespace pb {
+
+// Status-carrying exception used inside the library; converted to an int
+// status at the C-ABI boundary (nothing is thrown across it).
+struct Error {
+    int status;
+    std::string msg;
+};
+[[noreturn]] inline void fail(int status, const std::string& msg) { throw Error{status, msg}; }
+
+inline void cudaCheck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (e == cudaErrorMemoryAllocation) fail(PRISM_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+        fail(PRISM_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+#define PB_CUDA(call) ::pb::cudaCheck((call), #call)
+#define PB_LAUNCH(what) ::pb::cudaCheck(cudaGetLastError(), what)
+
+// Owning device allocation (cudaMalloc / cudaFree).
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) { alloc(count); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count) PB_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        if (count > n) fail(PRISM_INTERNAL, "upload beyond allocation");
+        if (count) PB_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void upload(const std::vector<T>& h, cudaStream_t s) {
+        if (h.size() != n) alloc(h.size());
+        upload(h.data(), h.size(), s);
+    }
+    void download(T* h, size_t count, cudaStream_t s) const {
+        if (count > n) fail(PRISM_INTERNAL, "download beyond allocation");
+        if (count) PB_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+    }
+    void zero(cudaStream_t s) {
+        if (n) PB_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    }
+    explicit operator bool() const { return p != nullptr; }
+};
+
+inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+constexpr double EPSILON = 2.220446049250313080847263336181640625e-16; // std::numeric_limits<double>::epsilon()
+constexpr int SLICE = 32;  // SELL slice height: one warp of rows
+constexpr int NUM_SMS = 148;
+
+}  // namespace pb

@@ -1,0 +1,592 @@
+// krylov.cu -- SELL-32 SpMV and the BiCGSTAB / Jacobi steps of solver::BiCGSTAB
+// and solver::Jacobi (numerics/bicgstab.cpp:7-9, numerics/jacobi.cpp:5-9).
+//
+// The reference solves every step() with Eigen's BiCGSTAB + IncompleteLUT to
+// machine precision. Here each step runs BiCGSTAB (van der Vorst 1992, the
+// textbook recurrences Eigen uses) with Jacobi right preconditioning, applied
+// by scaling the columns once per step: A' = A D^-1, x' = D x, so every
+// iteration is five streaming kernels and no preconditioner pass:
+//   p = r + beta (p - w v)                      vector kernel
+//   v = A' p ; r0.v -> alpha                    SpMV + fused dot
+//   s = r - alpha v                             vector kernel
+//   t = A' s ; t.s, t.t -> w                    SpMV + fused dots
+//   x += alpha p + w s ; r = s - w t ; r0.r, r.r -> beta, convergence
+// Scalars live in device memory (KState); every reduction is a fixed-order
+// two-stage tree (block partials, then the last block to finish reduces them),
+// so results are bitwise reproducible run to run. The host launches batches of
+// iterations and reads the state once per batch; kernels after convergence
+// return immediately, so a batch never changes a converged result.
+//
+// Mixed precision: FP32 matrix/vectors in the inner BiCGSTAB (dot products
+// accumulated in FP64) inside FP64 iterative refinement on the true residual.
+#include <cmath>
+#include <cstring>
+
+#include "krylov.h"
+
+namespace pb {
+
+namespace {
+
+constexpr int BS = 256;
+constexpr int WARPS = BS / 32;
+constexpr int MAX_GRID = NUM_SMS * 8;
+
+__device__ __forceinline__ double warpSum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warpMax(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-reduce NV sums (or maxima), publish the block partial, and let the last
+// block to arrive reduce all partials in block order. Returns true in the last block.
+template <int NV, bool MAX>
+__device__ bool reduceLast(double (&v)[NV], double* partials, unsigned int* counter, double (&out)[NV]) {
+    __shared__ double sh[NV][WARPS];
+    __shared__ int is_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < NV; ++k) {
+        double x = MAX ? warpMax(v[k]) : warpSum(v[k]);
+        if (lane == 0) sh[k][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NV; ++k) {
+            double s = sh[k][0];
+            for (int w = 1; w < WARPS; ++w) s = MAX ? fmax(s, sh[k][w]) : s + sh[k][w];
+            partials[blockIdx.x * NV + k] = s;
+        }
+        __threadfence();
+        unsigned int t = atomicAdd(counter, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return false;
+    __threadfence();
+    double acc[NV];
+    for (int k = 0; k < NV; ++k) {
+        acc[k] = MAX ? 0.0 : 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
+            double x = __ldcg(&partials[b * NV + k]);
+            acc[k] = MAX ? fmax(acc[k], x) : acc[k] + x;
+        }
+    }
+    __syncthreads();
+    for (int k = 0; k < NV; ++k) {
+        double x = MAX ? warpMax(acc[k]) : warpSum(acc[k]);
+        if (lane == 0) sh[k][warp] = x;
+    }
+    __syncthreads();
+    for (int k = 0; k < NV; ++k) {
+        double s = sh[k][0];
+        for (int w = 1; w < WARPS; ++w) s = MAX ? fmax(s, sh[k][w]) : s + sh[k][w];
+        out[k] = s;
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
+}
+
+inline int vecGrid(int n) { return std::max(1, std::min(ceil_div(n, BS), MAX_GRID)); }
+inline int spmvGrid(int nslices) { return std::max(1, std::min(ceil_div(nslices, WARPS), NUM_SMS * 16)); }
+
+// y = A x for a SELL-32 matrix; one warp per 32-row slice, coalesced loads.
+// STAGE 0: plain; 1: alpha = rho / (u.y); 2: w = (u.y)/(y.y)
+template <typename T, int STAGE>
+__global__ void __launch_bounds__(BS) spmv_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                  const int* __restrict__ col, const T* __restrict__ val,
+                                                  const T* __restrict__ x, T* __restrict__ y,
+                                                  const T* __restrict__ u, double* partials,
+                                                  unsigned int* counter, KState* S) {
+    if (STAGE != 0 && S->done) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double d0 = 0.0, d1 = 0.0;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int b = sl_off[sl];
+        const int width = (sl_off[sl + 1] - b) >> 5;
+        const int* cp = col + b + lane;
+        const T* vp = val + b + lane;
+        T sum = 0;
+        for (int j = 0; j < width; ++j) sum += vp[32 * j] * x[cp[32 * j]];
+        const int r = sl * 32 + lane;
+        y[r] = sum;
+        if (STAGE != 0 && r < n) {
+            d0 += (double)sum * (double)u[r];
+            if (STAGE == 2) d1 += (double)sum * (double)sum;
+        }
+    }
+    if (STAGE == 0) return;
+    double v[2] = {d0, d1}, out[2];
+    if (reduceLast<2, false>(v, partials, counter, out) && threadIdx.x == 0) {
+        if (STAGE == 1) {
+            S->alpha = S->rho / out[0];
+        } else {
+            S->ts = out[0];
+            S->tt = out[1];
+            S->w = out[1] > 0.0 ? out[0] / out[1] : 0.0;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BS) p_kernel(int n, T* __restrict__ p, const T* __restrict__ r,
+                                               const T* __restrict__ v, const KState* S) {
+    if (S->done) return;
+    const double beta = S->beta, w = S->w;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS)
+        p[i] = (T)((double)r[i] + beta * ((double)p[i] - w * (double)v[i]));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BS) s_kernel(int n, T* __restrict__ s, const T* __restrict__ r,
+                                               const T* __restrict__ v, const KState* S) {
+    if (S->done) return;
+    const double alpha = S->alpha;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS)
+        s[i] = (T)((double)r[i] - alpha * (double)v[i]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BS) xr_kernel(int n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                                                const T* __restrict__ s, const T* __restrict__ t,
+                                                const T* __restrict__ r0, double* partials, unsigned int* counter,
+                                                KState* S) {
+    if (S->done) return;
+    const double alpha = S->alpha, w = S->w;
+    double d0 = 0.0, d1 = 0.0;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS) {
+        double si = (double)s[i];
+        double xi = (double)x[i] + alpha * (double)p[i] + w * si;
+        T ri = (T)(si - w * (double)t[i]);
+        x[i] = (T)xi;
+        r[i] = ri;
+        d0 += (double)r0[i] * (double)ri;
+        d1 += (double)ri * (double)ri;
+    }
+    double v[2] = {d0, d1}, out[2];
+    if (reduceLast<2, false>(v, partials, counter, out) && threadIdx.x == 0) {
+        S->rr = out[1];
+        S->iter += 1;
+        const double rho_new = out[0];
+        if (!isfinite(out[0]) || !isfinite(out[1])) S->done = 5;
+        else if (out[1] <= S->tol2) S->done = 1;
+        else if (S->iter >= S->maxit) S->done = 2;
+        else if (w == 0.0 || fabs(rho_new) < EPSILON * EPSILON * S->r0sq) S->done = 3;
+        else {
+            S->beta = (rho_new / S->rho) * (alpha / w);
+            S->rho = rho_new;
+        }
+    }
+}
+
+// r = b - r (r holds A x) or r = b (x = 0); r0 = r; p = v = 0; set up the state.
+template <typename T>
+__global__ void __launch_bounds__(BS) init_kernel(int n, T* __restrict__ r, const T* __restrict__ b,
+                                                  T* __restrict__ r0, T* __restrict__ p, T* __restrict__ v,
+                                                  int from_zero, double tol, double* partials,
+                                                  unsigned int* counter, KState* S) {
+    double d0 = 0.0, d1 = 0.0;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS) {
+        double bi = (double)b[i];
+        T ri = from_zero ? b[i] : (T)(bi - (double)r[i]);
+        r[i] = ri;
+        r0[i] = ri;
+        p[i] = 0;
+        v[i] = 0;
+        d0 += (double)ri * (double)ri;
+        d1 += bi * bi;
+    }
+    double vv[2] = {d0, d1}, out[2];
+    if (reduceLast<2, false>(vv, partials, counter, out) && threadIdx.x == 0) {
+        S->rr = out[0];
+        S->bb = out[1];
+        S->r0sq = out[0];
+        S->tol2 = tol * tol * out[1];
+        S->rho = out[0];
+        S->beta = out[0];
+        S->alpha = 1.0;
+        S->w = 1.0;
+        if (!isfinite(out[0]) || !isfinite(out[1])) S->done = 5;
+        else if (out[1] == 0.0) S->done = 4;
+        else if (out[0] <= S->tol2) S->done = 1;
+        else S->done = 0;
+    }
+}
+
+// column scaling: dinv = 1/diag (1 where diag == 0), As = A dinv[col], xs = diag x
+__global__ void dinv_kernel(int n, const int* diag_pos, const double* vals, double* dinv, const double* x, double* xs) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i >= n) return;
+    double d = vals[diag_pos[i]];
+    double di = (d != 0.0) ? 1.0 / d : 1.0;
+    dinv[i] = di;
+    if (xs) xs[i] = (d != 0.0) ? d * x[i] : x[i];
+}
+template <typename T>
+__global__ void scale_kernel(int64_t nnz, const int* col, const double* vals, const double* dinv, T* out) {
+    for (int64_t k = blockIdx.x * (int64_t)BS + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * BS)
+        out[k] = (T)(vals[k] * dinv[col[k]]);
+}
+__global__ void unscale_kernel(int n, const double* dinv, const double* xs, double* x) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) x[i] = dinv[i] * xs[i];
+}
+// refinement: r = b - A x (FP64) -> r (double) and r32; dots r.r, b.b
+__global__ void __launch_bounds__(BS) refine_residual_kernel(int n, const double* __restrict__ Ax,
+                                                             const double* __restrict__ b, float* __restrict__ r32,
+                                                             double* partials, unsigned int* counter, double* out2) {
+    double d0 = 0.0, d1 = 0.0;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS) {
+        double ri = b[i] - Ax[i];
+        r32[i] = (float)ri;
+        d0 += ri * ri;
+        d1 += b[i] * b[i];
+    }
+    double v[2] = {d0, d1}, out[2];
+    if (reduceLast<2, false>(v, partials, counter, out) && threadIdx.x == 0) {
+        out2[0] = out[0];
+        out2[1] = out[1];
+    }
+}
+__global__ void correct_kernel(int n, double* x, const double* dinv, const float* d32) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) x[i] += dinv[i] * (double)d32[i];
+}
+__global__ void fill_zero_f(int n, float* x) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) x[i] = 0.0f;
+}
+
+// Jacobi: out = x + dinv (b - A x)
+__global__ void __launch_bounds__(BS) jacobi_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                    const int* __restrict__ col, const double* __restrict__ val,
+                                                    const int* __restrict__ diag_pos, const double* __restrict__ b,
+                                                    const double* __restrict__ x, double* __restrict__ out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
+        const int r = sl * 32 + lane;
+        if (r >= n) continue;
+        double sum = 0.0;
+        for (int j = 0; j < width; ++j) sum += val[bo + 32 * j + lane] * x[col[bo + 32 * j + lane]];
+        double dinv = 1.0 / val[diag_pos[r]];
+        double res = b[r] - sum;
+        out[r] = x[r] + dinv * res;
+    }
+}
+
+// explicit momentum: out = (-(A x - diag x) + b) / diag
+__global__ void __launch_bounds__(BS) explicit_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                      const int* __restrict__ col, const double* __restrict__ val,
+                                                      const int* __restrict__ diag_pos, const double* __restrict__ b,
+                                                      const double* __restrict__ x, double* __restrict__ out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
+        const int r = sl * 32 + lane;
+        if (r >= n) continue;
+        double sum = 0.0;
+        for (int j = 0; j < width; ++j) sum += val[bo + 32 * j + lane] * x[col[bo + 32 * j + lane]];
+        double ac = val[diag_pos[r]];
+        double H = sum - ac * x[r];
+        out[r] = (-H + b[r]) / ac;
+    }
+}
+
+// scaled residual pieces: max|Ax - b|, max|diag x|, count of non-finite terms
+__global__ void __launch_bounds__(BS) resid_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                   const int* __restrict__ col, const double* __restrict__ val,
+                                                   const int* __restrict__ diag_pos, const double* __restrict__ b,
+                                                   const double* __restrict__ x, double* partials,
+                                                   unsigned int* counter, double* out3) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double m0 = 0.0, m1 = 0.0, bad = 0.0;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
+        const int r = sl * 32 + lane;
+        if (r >= n) continue;
+        double sum = 0.0;
+        for (int j = 0; j < width; ++j) sum += val[bo + 32 * j + lane] * x[col[bo + 32 * j + lane]];
+        double e = fabs(sum - b[r]);
+        double d = fabs(val[diag_pos[r]] * x[r]);
+        if (!isfinite(e) || !isfinite(d)) bad = 1.0;
+        else {
+            m0 = fmax(m0, e);
+            m1 = fmax(m1, d);
+        }
+    }
+    double v[3] = {m0, m1, bad}, out[3];
+    if (reduceLast<3, true>(v, partials, counter, out) && threadIdx.x == 0) {
+        out3[0] = out[0];
+        out3[1] = out[1];
+        out3[2] = out[2];
+    }
+}
+
+}  // namespace
+
+void KrylovWork::ensure(int n_pad, int64_t nnz_padded, bool mixed) {
+    if (!host_state) PB_CUDA(cudaMallocHost(&host_state, sizeof(KState) + 64));
+    if (n != n_pad || nnz != nnz_padded) {
+        n = n_pad;
+        nnz = nnz_padded;
+        for (auto* b : {&r, &r0, &p, &v, &s, &t, &xs, &dinv, &tmp}) b->alloc(n_pad);
+        As.alloc(nnz_padded);
+        partials.alloc(NUM_SMS * 16 * 4);
+        counter.alloc(1);
+        PB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned int)));
+        scal.alloc(8);
+        state.alloc(1);
+        As32.release();
+        for (auto* b : {&r32, &r032, &p32, &v32, &s32, &t32, &x32}) b->release();
+        // zero vectors once so padded rows stay 0
+        for (auto* b : {&r, &r0, &p, &v, &s, &t, &xs, &dinv, &tmp}) PB_CUDA(cudaMemset(b->p, 0, n_pad * sizeof(double)));
+    }
+    if (mixed && !As32) {
+        As32.alloc(nnz_padded);
+        for (auto* b : {&r32, &r032, &p32, &v32, &s32, &t32, &x32}) {
+            b->alloc(n_pad);
+            PB_CUDA(cudaMemset(b->p, 0, n_pad * sizeof(float)));
+        }
+    }
+}
+KrylovWork::~KrylovWork() {
+    if (host_state) cudaFreeHost(host_state);
+}
+
+void spmv(const SellMatrix& A, const double* x, double* y, cudaStream_t s) {
+    spmv_kernel<double, 0><<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, x, y, nullptr,
+                                                              nullptr, nullptr, nullptr);
+    PB_LAUNCH("spmv_kernel");
+}
+
+namespace {
+
+// ---- sampled SpMV timing (prism_profile_start / prism_profile_stop)
+struct Sample {
+    cudaEvent_t a, b;
+    bool fp32;
+    double bytes;
+};
+struct Profiler {
+    bool on = false;
+    int max_samples = 0;
+    std::vector<Sample> samples;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        PB_CUDA(cudaEventCreate(&e));
+        return e;
+    }
+} g_prof;
+
+template <typename T>
+double spmvBytes(const SellMatrix& A) {
+    return (double)A.nnz_csr * (sizeof(T) + 4) + 4.0 * (A.n + 1) + 2.0 * A.n * sizeof(T);
+}
+template <typename T>
+bool sampleBegin(Sample& smp, const SellMatrix& A, cudaStream_t s) {
+    if (!g_prof.on || (int)g_prof.samples.size() >= g_prof.max_samples) return false;
+    smp.a = g_prof.get();
+    smp.b = g_prof.get();
+    smp.fp32 = sizeof(T) == 4;
+    smp.bytes = spmvBytes<T>(A);
+    PB_CUDA(cudaEventRecord(smp.a, s));
+    return true;
+}
+void sampleEnd(Sample& smp, cudaStream_t s) {
+    PB_CUDA(cudaEventRecord(smp.b, s));
+    g_prof.samples.push_back(smp);
+}
+
+template <typename T>
+struct Vecs {
+    T *x, *r, *r0, *p, *v, *s, *t;
+};
+
+// BiCGSTAB iterations on (M, rhs) from the current x; returns iterations done.
+template <typename T>
+KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, bool from_zero, double tol,
+                      long long maxit, KrylovWork& w, cudaStream_t s) {
+    KrylovOut out;
+    KState* S = w.state.p;
+    KState init{};
+    init.maxit = maxit;
+    PB_CUDA(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, s));
+    const int n = A.n, vg = vecGrid(n), sg = spmvGrid(A.nslices);
+    int restarts = 0;
+    bool zero = from_zero;
+    long long batch = 8;
+    while (true) {
+        if (!zero)
+            spmv_kernel<T, 0><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.x, V.r, nullptr, nullptr, nullptr,
+                                                nullptr);
+        init_kernel<T><<<vg, BS, 0, s>>>(n, V.r, rhs, V.r0, V.p, V.v, zero ? 1 : 0, tol, w.partials.p, w.counter.p, S);
+        PB_LAUNCH("bicgstab init");
+        zero = false;
+        int done = 0;
+        while (true) {
+            for (long long it = 0; it < batch; ++it) {
+                p_kernel<T><<<vg, BS, 0, s>>>(n, V.p, V.r, V.v, S);
+                Sample smp;
+                bool sampled = sampleBegin<T>(smp, A, s);
+                spmv_kernel<T, 1><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.p, V.v, V.r0, w.partials.p,
+                                                    w.counter.p, S);
+                if (sampled) sampleEnd(smp, s);
+                s_kernel<T><<<vg, BS, 0, s>>>(n, V.s, V.r, V.v, S);
+                spmv_kernel<T, 2><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.s, V.t, V.s, w.partials.p,
+                                                    w.counter.p, S);
+                xr_kernel<T><<<vg, BS, 0, s>>>(n, V.x, V.r, V.p, V.s, V.t, V.r0, w.partials.p, w.counter.p, S);
+            }
+            PB_LAUNCH("bicgstab iteration");
+            PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
+            PB_CUDA(cudaStreamSynchronize(s));
+            done = w.host_state->done;
+            if (done != 0) break;
+            batch = std::min<long long>(batch * 2, 64);
+        }
+        out.iterations = w.host_state->iter;
+        if (done == 3) {
+            if (++restarts > 20) {
+                out.status = PRISM_BREAKDOWN;
+                break;
+            }
+            continue;  // restart from the current x (r recomputed from b - A x)
+        }
+        if (done == 2) out.status = PRISM_NOT_CONVERGED;
+        if (done == 5) out.status = PRISM_NONFINITE;
+        break;
+    }
+    return out;
+}
+
+}  // namespace
+
+KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, int precision,
+                   double inner_tol, KrylovWork& w, cudaStream_t s) {
+    const bool mixed = precision == PRISM_PREC_MIXED;
+    w.ensure(A.nslices * 32, A.nnz_padded, mixed);
+    const int n = A.n;
+    const int gn = ceil_div(n, BS);
+    dinv_kernel<<<gn, BS, 0, s>>>(n, A.diag_pos, A.vals, w.dinv.p, x, w.xs.p);
+    int sgrid = std::min<int64_t>((A.nnz_padded + BS - 1) / BS, NUM_SMS * 32);
+    scale_kernel<double><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As.p);
+    PB_LAUNCH("bicgstab scaling");
+    KrylovOut out;
+    if (!mixed) {
+        Vecs<double> V{w.xs.p, w.r.p, w.r0.p, w.p.p, w.v.p, w.s.p, w.t.p};
+        // accurate-residual restarts: the recursive residual drifts from b - A x
+        for (int pass = 0; pass < 4; ++pass) {
+            KrylovOut o = runBicgstab<double>(A, w.As.p, b, V, false, tol, maxit, w, s);
+            out.iterations += o.iterations;
+            out.status = o.status;
+            maxit -= o.iterations;
+            unscale_kernel<<<gn, BS, 0, s>>>(n, w.dinv.p, w.xs.p, x);
+            spmv(A, x, w.tmp.p, s);
+            double rb[2];
+            refine_residual_kernel<<<vecGrid(n), BS, 0, s>>>(n, w.tmp.p, b, reinterpret_cast<float*>(w.s.p),
+                                                             w.partials.p, w.counter.p, w.scal.p);
+            PB_CUDA(cudaMemcpyAsync(rb, w.scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            PB_CUDA(cudaStreamSynchronize(s));
+            out.rel_residual = rb[1] > 0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
+            if (o.status != PRISM_OK || out.rel_residual <= 10 * tol || maxit <= 0 || rb[1] == 0) break;
+        }
+        return out;
+    }
+    // mixed precision: FP32 inner BiCGSTAB on A D^-1, FP64 refinement on A
+    scale_kernel<float><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As32.p);
+    PB_LAUNCH("bicgstab fp32 copy");
+    Vecs<float> V{w.x32.p, w.r32.p, w.r032.p, w.p32.p, w.v32.p, w.s32.p, w.t32.p};
+    float* rhs32 = reinterpret_cast<float*>(w.tmp.p);  // FP32 right-hand side of the correction
+    double rb[2];
+    for (int outer = 0; outer < 60; ++outer) {
+        spmv(A, x, w.r.p, s);
+        refine_residual_kernel<<<vecGrid(n), BS, 0, s>>>(n, w.r.p, b, rhs32, w.partials.p, w.counter.p, w.scal.p);
+        PB_CUDA(cudaMemcpyAsync(rb, w.scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+        if (!std::isfinite(rb[0]) || !std::isfinite(rb[1])) {
+            out.status = PRISM_NONFINITE;
+            break;
+        }
+        out.rel_residual = rb[1] > 0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
+        if (rb[1] == 0.0 || rb[0] <= tol * tol * rb[1] || maxit <= 0) {
+            if (maxit <= 0 && rb[0] > tol * tol * rb[1]) out.status = PRISM_NOT_CONVERGED;
+            break;
+        }
+        fill_zero_f<<<gn, BS, 0, s>>>(n, w.x32.p);
+        KrylovOut o = runBicgstab<float>(A, w.As32.p, rhs32, V, true, inner_tol, maxit, w, s);
+        out.iterations += o.iterations;
+        maxit -= o.iterations;
+        if (o.status == PRISM_NONFINITE) {
+            out.status = o.status;
+            break;
+        }
+        correct_kernel<<<gn, BS, 0, s>>>(n, x, w.dinv.p, w.x32.p);
+        PB_LAUNCH("refinement correction");
+    }
+    return out;
+}
+
+void profileStart(int max_samples) {
+    for (auto& smp : g_prof.samples) {
+        g_prof.pool.push_back(smp.a);
+        g_prof.pool.push_back(smp.b);
+    }
+    g_prof.samples.clear();
+    g_prof.max_samples = max_samples > 0 ? max_samples : 4096;
+    g_prof.on = true;
+}
+
+void profileStop(PrismProfile* out) {
+    std::memset(out, 0, sizeof(*out));
+    g_prof.on = false;
+    for (auto& smp : g_prof.samples) {
+        PB_CUDA(cudaEventSynchronize(smp.b));
+        float ms = 0.f;
+        PB_CUDA(cudaEventElapsedTime(&ms, smp.a, smp.b));
+        if (smp.fp32) {
+            out->fp32_launches++;
+            out->fp32_ms += ms;
+            out->fp32_bytes += smp.bytes;
+        } else {
+            out->fp64_launches++;
+            out->fp64_ms += ms;
+            out->fp64_bytes += smp.bytes;
+        }
+    }
+}
+
+void jacobiStep(const SellMatrix& A, const double* b, double* x, KrylovWork& w, cudaStream_t s) {
+    w.ensure(A.nslices * 32, A.nnz_padded, false);
+    jacobi_kernel<<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x,
+                                                      w.tmp.p);
+    PB_LAUNCH("jacobi_kernel");
+    PB_CUDA(cudaMemcpyAsync(x, w.tmp.p, A.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+}
+
+void explicitUpdate(const SellMatrix& A, const double* b, const double* x, double* xnew, cudaStream_t s) {
+    explicit_kernel<<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x,
+                                                        xnew);
+    PB_LAUNCH("explicit_kernel");
+}
+
+double scaledResidual(const SellMatrix& A, const double* b, const double* x, KrylovWork& w, cudaStream_t s) {
+    w.ensure(A.nslices * 32, A.nnz_padded, false);
+    resid_kernel<<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x,
+                                                     w.partials.p, w.counter.p, w.scal.p);
+    PB_LAUNCH("resid_kernel");
+    double h[3];
+    PB_CUDA(cudaMemcpyAsync(h, w.scal.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    if (h[2] != 0.0) return NAN;
+    return h[0] / (h[1] + EPSILON);
+}
+
+}  // namespace pb

@@ -1,0 +1,67 @@
+// krylov.h -- BiCGSTAB / Jacobi steps and the scaled residual on a SELL-32 matrix.
+#pragma once
+
+#include "common.h"
+
+namespace pb {
+
+// Matrix in SELL-32 layout (see views.h); vals holds the assembled FP64 values.
+struct SellMatrix {
+    int n = 0, nslices = 0;
+    int64_t nnz_padded = 0;
+    const int* sl_off = nullptr;
+    const int* col = nullptr;
+    const int* diag_pos = nullptr;
+    const double* vals = nullptr;
+    int64_t nnz_csr = 0;  // structural entries (for algorithmic byte counts)
+};
+
+// Sampled CUDA-event timing of the BiCGSTAB SpMV launches (v = A p).
+void profileStart(int max_samples);
+void profileStop(PrismProfile* out);
+
+// Device-resident solver state (one per BiCGSTAB run).
+struct KState {
+    double rho, alpha, w, beta;
+    double rr, bb, tol2, r0sq;
+    double ts, tt;
+    long long iter, maxit;
+    int done;  // 0 running, 1 converged, 2 max iterations, 3 restart needed, 4 zero rhs, 5 non-finite
+    int nonfinite;
+};
+
+// Workspace owned by a mesh, sized on first use.
+struct KrylovWork {
+    int n = 0;
+    int64_t nnz = 0;
+    DevBuf<double> r, r0, p, v, s, t, xs, dinv, tmp;
+    DevBuf<double> As;   // column-scaled matrix A D^-1
+    DevBuf<float> As32, r32, r032, p32, v32, s32, t32, x32;
+    DevBuf<double> partials, scal;
+    DevBuf<unsigned int> counter;
+    DevBuf<KState> state;
+    KState* host_state = nullptr;  // pinned
+    void ensure(int n_pad, int64_t nnz_padded, bool mixed);
+    ~KrylovWork();
+};
+
+struct KrylovOut {
+    long long iterations = 0;
+    int status = PRISM_OK;
+    double rel_residual = 0.0;
+};
+
+// x <- BiCGSTAB solve of A x = b from the guess x (Jacobi right preconditioning),
+// stopping at ||b - A x|| <= tol ||b||. precision: PRISM_PREC_FP64 or PRISM_PREC_MIXED.
+KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, int precision,
+                   double inner_tol, KrylovWork& w, cudaStream_t s);
+// x <- x + D^-1 (b - A x)   (numerics/jacobi.cpp:5-9)
+void jacobiStep(const SellMatrix& A, const double* b, double* x, KrylovWork& w, cudaStream_t s);
+// max|A x - b| / (max|diag(A) x| + eps)   (numerics/solver.cpp:8-24); returns NaN if non-finite values met
+double scaledResidual(const SellMatrix& A, const double* b, const double* x, KrylovWork& w, cudaStream_t s);
+// y <- A x (FP64)
+void spmv(const SellMatrix& A, const double* x, double* y, cudaStream_t s);
+// H-operator of the explicit momentum step: x_new = (b - (A x - diag x)) / diag  (PRIME.cpp:39-56)
+void explicitUpdate(const SellMatrix& A, const double* b, const double* x, double* xnew, cudaStream_t s);
+
+}  // namespace pb

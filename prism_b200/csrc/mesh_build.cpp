@@ -1,0 +1,334 @@
+// mesh_build.cpp -- host conversion of a UNV-form mesh to the flattened PMesh.
+//
+// Reproduces the face numbering of UnvToPMeshConverter (mesh/unv.cpp:124-372)
+// and the PMesh face permutation (mesh/pmesh.cpp:51-123):
+//   * faces are created in order of first appearance: boundary elements as they
+//     are read, cell faces in cell order and local face order (unv.cpp:19-58);
+//   * the first cell touching a face owns it, the second is its neighbour;
+//   * boundary faces are ordered by the moment their owner was assigned;
+//   * PMesh orders faces [non-empty boundary | empty boundary | interior].
+// Face and cell geometry follow mesh/face.cpp:5-41 and mesh/cell.cpp:7-41 with
+// the same operation order (host code, no FMA contraction).
+//
+// Faces are matched by sorting 128-bit keys of their sorted vertex ids rather
+// than by the reference's vertex trie: O(N log N), a few seconds for 10^7 cell
+// faces, with identical results.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+
+#include "mesh_build.h"
+
+namespace pb {
+
+namespace {
+
+struct V3 {
+    double x, y, z;
+};
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 scale(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 divs(V3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+inline double dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+
+const int kHexFaces[6][4] = {{1, 2, 6, 5}, {0, 4, 7, 3}, {2, 3, 7, 6}, {0, 1, 5, 4}, {4, 5, 6, 7}, {0, 3, 2, 1}};
+const int kTetFaces[4][3] = {{0, 2, 1}, {1, 2, 3}, {0, 1, 3}, {0, 3, 2}};
+const int kWedgeFaces[5][4] = {{0, 2, 1, -1}, {3, 4, 5, -1}, {0, 1, 4, 3}, {0, 3, 5, 2}, {1, 2, 5, 4}};
+
+int nLocalFaces(int kind) { return kind == PRISM_ELEM_HEX ? 6 : kind == PRISM_ELEM_TETRA ? 4 : 5; }
+
+// vertex ids of local face l of element e (l < 0: the element itself)
+int faceVerts(const PrismUnvMesh* d, int64_t e, int l, int64_t* out) {
+    const int64_t* en = d->elem_nodes + d->elem_offsets[e];
+    int kind = d->elem_kind[e];
+    if (l < 0) {
+        int n = (int)(d->elem_offsets[e + 1] - d->elem_offsets[e]);
+        for (int i = 0; i < n; ++i) out[i] = en[i];
+        return n;
+    }
+    if (kind == PRISM_ELEM_HEX) {
+        for (int i = 0; i < 4; ++i) out[i] = en[kHexFaces[l][i]];
+        return 4;
+    }
+    if (kind == PRISM_ELEM_TETRA) {
+        for (int i = 0; i < 3; ++i) out[i] = en[kTetFaces[l][i]];
+        return 3;
+    }
+    int n = kWedgeFaces[l][3] < 0 ? 3 : 4;
+    for (int i = 0; i < n; ++i) out[i] = en[kWedgeFaces[l][i]];
+    return n;
+}
+
+struct Key {
+    uint64_t hi, lo;
+    bool operator<(const Key& o) const { return hi != o.hi ? hi < o.hi : lo < o.lo; }
+    bool operator==(const Key& o) const { return hi == o.hi && lo == o.lo; }
+};
+Key makeKey(const int64_t* v, int n) {
+    uint64_t s[4] = {~0ull, ~0ull, ~0ull, ~0ull};
+    for (int i = 0; i < n; ++i) s[i] = (uint64_t)v[i];
+    std::sort(s, s + n);
+    return {(s[0] << 32) | (s[1] & 0xffffffffull), (s[2] << 32) | (s[3] & 0xffffffffull)};
+}
+
+// Face::Face (mesh/face.cpp:5-41)
+void faceGeometry(const V3* fv, int n, double& area, V3& normal, V3& center) {
+    V3 gc{0, 0, 0};
+    for (int i = 0; i < n; ++i) gc = add(gc, fv[i]);
+    gc = divs(gc, (double)n);
+    normal = {0, 0, 0};
+    area = 0.0;
+    center = {0, 0, 0};
+    for (int i = 0; i < n; ++i) {
+        V3 v1 = fv[i], v2 = fv[(i + 1) % n], v3 = gc;
+        V3 sc = divs(add(add(v1, v2), v3), 3.0);
+        V3 sn = cross(sub(v2, v1), sub(v3, v1));
+        double sa = std::sqrt(dot(sn, sn)) / 2.0;
+        normal = add(normal, sn);
+        area += sa;
+        center = add(center, scale(sc, sa));
+    }
+    center = divs(center, area);
+    normal = divs(normal, std::sqrt(dot(normal, normal)));
+}
+
+}  // namespace
+
+std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
+    if (!d) fail(PRISM_BAD_ARG, "null mesh description");
+    if (d->n_nodes <= 0) fail(PRISM_INVALID_MESH, "UnvToPMeshConverter(): mesh has zero vertices");
+    if (d->n_nodes >= (int64_t(1) << 32)) fail(PRISM_INVALID_MESH, "too many nodes");
+    const int64_t ne = d->n_elements;
+    std::vector<V3> X(d->n_nodes);
+    for (int64_t i = 0; i < d->n_nodes; ++i) X[i] = {d->xyz[3 * i], d->xyz[3 * i + 1], d->xyz[3 * i + 2]};
+
+    // ---- occurrences of faces in reading order
+    struct Occ {
+        Key key;
+        int64_t elem;
+        int32_t local;  // -1: boundary element
+        int32_t cell;   // -1: boundary element
+    };
+    std::vector<Occ> occ;
+    std::vector<int64_t> cell_elem;
+    std::vector<int64_t> bface_of_elem(ne, -1);  // later: face id of a boundary element
+    int64_t tmp[8];
+    for (int64_t e = 0; e < ne; ++e) {
+        int k = d->elem_kind[e];
+        int64_t nn = d->elem_offsets[e + 1] - d->elem_offsets[e];
+        const int64_t* en = d->elem_nodes + d->elem_offsets[e];
+        for (int64_t i = 0; i < nn; ++i)
+            if (en[i] < 0 || en[i] >= d->n_nodes) fail(PRISM_INVALID_MESH, "element node index out of range");
+        if (k == PRISM_ELEM_LINE) continue;
+        if (k == PRISM_ELEM_TRIANGLE || k == PRISM_ELEM_QUAD) {
+            int n = faceVerts(d, e, -1, tmp);
+            if (n != (k == PRISM_ELEM_QUAD ? 4 : 3)) fail(PRISM_INVALID_MESH, "bad boundary element");
+            occ.push_back({makeKey(tmp, n), e, -1, -1});
+        } else if (k == PRISM_ELEM_HEX || k == PRISM_ELEM_TETRA || k == PRISM_ELEM_WEDGE) {
+            int need = k == PRISM_ELEM_HEX ? 8 : k == PRISM_ELEM_TETRA ? 4 : 6;
+            if (nn != need) fail(PRISM_INVALID_MESH, "cell element with a wrong node count");
+            int32_t c = (int32_t)cell_elem.size();
+            cell_elem.push_back(e);
+            for (int l = 0; l < nLocalFaces(k); ++l) {
+                int n = faceVerts(d, e, l, tmp);
+                occ.push_back({makeKey(tmp, n), e, l, c});
+            }
+        } else {
+            fail(PRISM_INVALID_MESH, "unsupported element type");
+        }
+    }
+    if (cell_elem.empty()) fail(PRISM_INVALID_MESH, "mesh is empty or two dimensional");
+    if (cell_elem.size() >= (size_t(1) << 31)) fail(PRISM_INVALID_MESH, "too many cells");
+
+    // ---- match occurrences: sort by (key, reading order)
+    std::vector<int64_t> ord(occ.size());
+    std::iota(ord.begin(), ord.end(), 0);
+    std::sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) {
+        if (occ[a].key == occ[b].key) return a < b;
+        return occ[a].key < occ[b].key;
+    });
+    struct Run {
+        int64_t first;   // occurrence index of creation
+        int64_t owner_occ;
+        int32_t owner, nbr;
+        bool bface;
+    };
+    std::vector<Run> runs;
+    std::vector<int64_t> run_of_occ(occ.size());
+    for (size_t i = 0; i < ord.size();) {
+        size_t j = i;
+        while (j < ord.size() && occ[ord[j]].key == occ[ord[i]].key) ++j;
+        Run r{ord[i], -1, -1, -1, occ[ord[i]].cell < 0};
+        size_t q = i;
+        if (r.bface) ++q;
+        for (; q < j; ++q) {
+            const Occ& o = occ[ord[q]];
+            if (o.cell < 0) fail(PRISM_INVALID_MESH, "duplicated boundary face element");
+            if (r.owner < 0) { r.owner = o.cell; r.owner_occ = ord[q]; }
+            else if (r.nbr < 0) r.nbr = o.cell;
+            else fail(PRISM_INVALID_MESH, "a face shared by more than two cells");
+        }
+        if (r.bface && r.nbr >= 0) fail(PRISM_INVALID_MESH, "boundary face element between two cells");
+        if (r.bface && r.owner < 0) fail(PRISM_INVALID_MESH, "dangling boundary face (not owned by any cell)");
+        if (!r.bface && r.nbr < 0) fail(PRISM_INVALID_MESH, "cell face on no boundary patch and no neighbour");
+        for (size_t q2 = i; q2 < j; ++q2) run_of_occ[ord[q2]] = (int64_t)runs.size();
+        runs.push_back(r);
+        i = j;
+    }
+    // converter face id = rank of creation
+    std::vector<int64_t> by_creation(runs.size());
+    std::iota(by_creation.begin(), by_creation.end(), 0);
+    std::sort(by_creation.begin(), by_creation.end(), [&](int64_t a, int64_t b) { return runs[a].first < runs[b].first; });
+    std::vector<int64_t> conv_id(runs.size());
+    for (size_t k = 0; k < by_creation.size(); ++k) conv_id[by_creation[k]] = (int64_t)k;
+    const int64_t nf = (int64_t)runs.size();
+
+    // ---- groups -> patches (unv.cpp:298-371, 84-97)
+    std::vector<char> in_group(ne, 0);
+    std::map<std::string, std::vector<int64_t>> name_to_runs;
+    for (int32_t g = 0; g < d->n_groups; ++g) {
+        if (d->group_is_vertex && d->group_is_vertex[g]) continue;
+        std::vector<int64_t> rs;
+        for (int64_t q = d->group_offsets[g]; q < d->group_offsets[g + 1]; ++q) {
+            int64_t e = d->group_elements[q];
+            if (e < 0 || e >= ne || (d->elem_kind[e] != PRISM_ELEM_QUAD && d->elem_kind[e] != PRISM_ELEM_TRIANGLE))
+                fail(PRISM_INVALID_MESH, "group contains non-face elements (cell zones)");
+            in_group[e] = 1;
+            rs.push_back(e);
+        }
+        name_to_runs.insert({d->group_names[g], std::move(rs)});
+    }
+    // element -> run for boundary elements
+    std::vector<int64_t> run_of_elem(ne, -1);
+    for (size_t o = 0; o < occ.size(); ++o)
+        if (occ[o].cell < 0) run_of_elem[occ[o].elem] = run_of_occ[o];
+    int64_t undefined = 0;
+    for (int64_t e = 0; e < ne; ++e)
+        if ((d->elem_kind[e] == PRISM_ELEM_QUAD || d->elem_kind[e] == PRISM_ELEM_TRIANGLE) && !in_group[e]) ++undefined;
+    if (undefined)
+        fail(PRISM_INVALID_MESH, std::to_string(undefined) + " boundary faces are not part of any boundary patch");
+
+    auto hm = std::make_unique<HostMesh>();
+    std::vector<int32_t> run_patch(runs.size(), -1);
+    std::vector<std::vector<int64_t>> patch_runs(d->n_patches);
+    for (int32_t p = 0; p < d->n_patches; ++p) {
+        HostMesh::Patch pa;
+        pa.name = d->patch_names[p];
+        pa.empty = d->patch_is_empty[p] != 0;
+        auto it = name_to_runs.find(pa.name);
+        if (it != name_to_runs.end())
+            for (auto e : it->second) {
+                run_patch[run_of_elem[e]] = p;
+                patch_runs[p].push_back(run_of_elem[e]);
+            }
+        hm->patches.push_back(std::move(pa));
+    }
+
+    // ---- PMesh permutation (pmesh.cpp:51-90)
+    std::vector<int64_t> bruns, iruns;
+    for (size_t r = 0; r < runs.size(); ++r) (runs[r].bface ? bruns : iruns).push_back((int64_t)r);
+    for (auto r : bruns)
+        if (run_patch[r] < 0) fail(PRISM_INVALID_MESH, "boundary face without a patch");
+    std::sort(bruns.begin(), bruns.end(), [&](int64_t a, int64_t b) { return runs[a].owner_occ < runs[b].owner_occ; });
+    std::sort(iruns.begin(), iruns.end(), [&](int64_t a, int64_t b) { return runs[a].first < runs[b].first; });
+    int64_t nb = (int64_t)bruns.size(), nne = 0;
+    for (auto r : bruns)
+        if (!hm->patches[run_patch[r]].empty) ++nne;
+    std::vector<int64_t> new_id(runs.size());
+    int64_t pos_ne = 0, pos_e = nne, pos_i = nb;
+    for (auto r : bruns) new_id[r] = hm->patches[run_patch[r]].empty ? pos_e++ : pos_ne++;
+    for (auto r : iruns) new_id[r] = pos_i++;
+    (void)conv_id;
+
+    // ---- flatten
+    const int64_t nc = (int64_t)cell_elem.size();
+    hm->nc = nc;
+    hm->nf = nf;
+    hm->nb = nb;
+    hm->nne = nne;
+    hm->owner.assign(nf, -1);
+    hm->nbr.assign(nf, -1);
+    hm->patch.assign(nf, -1);
+    hm->area.assign(nf, 0.0);
+    for (int k = 0; k < 3; ++k) {
+        hm->normal[k].assign(nf, 0.0);
+        hm->fc[k].assign(nf, 0.0);
+        hm->cc[k].assign(nc, 0.0);
+    }
+    hm->vol.assign(nc, 0.0);
+    V3 fv[8];
+    for (size_t r = 0; r < runs.size(); ++r) {
+        int64_t f = new_id[r];
+        const Occ& o = occ[runs[r].first];
+        int n = faceVerts(d, o.elem, o.local, tmp);
+        for (int i = 0; i < n; ++i) fv[i] = X[tmp[i]];
+        double a;
+        V3 nrm, ctr;
+        faceGeometry(fv, n, a, nrm, ctr);
+        hm->area[f] = a;
+        hm->normal[0][f] = nrm.x; hm->normal[1][f] = nrm.y; hm->normal[2][f] = nrm.z;
+        hm->fc[0][f] = ctr.x; hm->fc[1][f] = ctr.y; hm->fc[2][f] = ctr.z;
+        hm->owner[f] = runs[r].owner;
+        hm->nbr[f] = runs[r].nbr;
+        hm->patch[f] = run_patch[r];
+    }
+    for (int32_t p = 0; p < d->n_patches; ++p)
+        for (auto r : patch_runs[p]) hm->patches[p].faces.push_back((int32_t)new_id[r]);
+
+    // cell faces in local order (occurrences of a cell are contiguous in reading order)
+    hm->cf_off.assign(nc + 1, 0);
+    for (size_t o = 0; o < occ.size(); ++o)
+        if (occ[o].cell >= 0) hm->cf_off[occ[o].cell + 1]++;
+    for (int64_t c = 0; c < nc; ++c) hm->cf_off[c + 1] += hm->cf_off[c];
+    hm->cf_face.assign(hm->cf_off[nc], -1);
+    {
+        std::vector<int64_t> fill(hm->cf_off.begin(), hm->cf_off.end() - 1);
+        for (size_t o = 0; o < occ.size(); ++o)
+            if (occ[o].cell >= 0) hm->cf_face[fill[occ[o].cell]++] = (int32_t)new_id[run_of_occ[o]];
+    }
+    // Cell::Cell (mesh/cell.cpp:7-41)
+    for (int64_t c = 0; c < nc; ++c) {
+        V3 gc{0, 0, 0};
+        int64_t b = hm->cf_off[c], e = hm->cf_off[c + 1];
+        for (int64_t q = b; q < e; ++q) {
+            int32_t f = hm->cf_face[q];
+            gc = add(gc, V3{hm->fc[0][f], hm->fc[1][f], hm->fc[2][f]});
+        }
+        gc = divs(gc, (double)(e - b));
+        double vol = 0.0;
+        V3 ctr{0, 0, 0};
+        for (int64_t q = b; q < e; ++q) {
+            int32_t f = hm->cf_face[q];
+            V3 fcv{hm->fc[0][f], hm->fc[1][f], hm->fc[2][f]};
+            V3 nrm{hm->normal[0][f], hm->normal[1][f], hm->normal[2][f]};
+            double pv = std::abs(dot(nrm, sub(fcv, gc)) * hm->area[f]) / 3;
+            V3 pc = add(scale(fcv, 0.75), scale(gc, 0.25));
+            vol += pv;
+            ctr = add(ctr, scale(pc, pv));
+        }
+        ctr = divs(ctr, vol);
+        hm->vol[c] = vol;
+        hm->cc[0][c] = ctr.x; hm->cc[1][c] = ctr.y; hm->cc[2][c] = ctr.z;
+    }
+    // geometric weight per interior face (mesh/utilities.cpp:28-40, owner orientation)
+    hm->gc.assign(nf - nb, 0.0);
+    for (int64_t f = nb; f < nf; ++f) {
+        int32_t o = hm->owner[f], n = hm->nbr[f];
+        V3 fcv{hm->fc[0][f], hm->fc[1][f], hm->fc[2][f]};
+        V3 co{hm->cc[0][o], hm->cc[1][o], hm->cc[2][o]};
+        V3 cn{hm->cc[0][n], hm->cc[1][n], hm->cc[2][n]};
+        V3 nrm{hm->normal[0][f], hm->normal[1][f], hm->normal[2][f]};
+        V3 Sf = scale(nrm, hm->area[f]);
+        Sf = V3{hm->area[f] * nrm.x, hm->area[f] * nrm.y, hm->area[f] * nrm.z};
+        V3 ef = divs(Sf, std::sqrt(dot(Sf, Sf)));
+        V3 dCf = sub(fcv, co), dfN = sub(cn, fcv);
+        hm->gc[f - nb] = dot(dCf, ef) / (dot(dCf, ef) + dot(dfN, ef));
+    }
+    return hm;
+}
+
+}  // namespace pb

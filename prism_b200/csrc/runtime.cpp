@@ -1,0 +1,694 @@
+// runtime.cpp -- host side of the sm_100a path: mesh upload, gradient caches,
+// eqn::Transport assembly / relax / solve and the SIMPLE, PRIME and PISO
+// drivers. The control flow follows the reference call by call (file:line
+// cited per function); every cell/face loop is a kernel on the mesh's stream.
+#include "runtime.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "coupling.h"
+#include "gradient.h"
+
+namespace pb {
+
+namespace {
+
+struct H3 {
+    double x, y, z;
+    double operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+inline H3 hsub(H3 a, H3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline double hdot(H3 a, H3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+
+template <typename T>
+void upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
+    d.alloc(h.size());
+    d.upload(h.data(), h.size(), s);
+}
+
+bool scalarHasHandler(int k) {
+    return k == PRISM_BC_FIXED || k == PRISM_BC_NOSLIP || k == PRISM_BC_SYMMETRY || k == PRISM_BC_OUTLET ||
+           k == PRISM_BC_ZERO_GRADIENT;
+}
+bool vectorHasHandler(int k) { return scalarHasHandler(k); }
+bool isDirichlet(int k) { return k == PRISM_BC_FIXED || k == PRISM_BC_NOSLIP; }
+
+[[noreturn]] void noHandler(const Mesh& m, int p, const std::string& who) {
+    fail(PRISM_NO_BC_HANDLER, who + ": no boundary handler for patch '" + m.h->patches[p].name + "'");
+}
+
+// patches whose faces a boundary loop visits
+bool visited(const Mesh& m, int p) { return !m.h->patches[p].empty && !m.h->patches[p].faces.empty(); }
+
+// Scalar::valueAtBoundaryFace would succeed on every visited patch (or on patch `only`)
+void checkScalarValues(const Scalar& s, const std::string& who, int only = -1) {
+    if (s.has_fv) return;
+    const Mesh& m = *s.m;
+    for (int p = 0; p < m.npatch; ++p) {
+        if (!visited(m, p) || (only >= 0 && p != only)) continue;
+        int k = s.bc[p].kind;
+        if (!scalarHasHandler(k)) noHandler(m, p, who + " (field " + s.name + ")");
+        if (isDirichlet(k)) {
+            int want = s.coord >= 0 ? PRISM_BCV_VECTOR : PRISM_BCV_SCALAR;
+            if (s.bc[p].value_kind != want)
+                fail(PRISM_BAD_ARG, "patch '" + m.h->patches[p].name + "' field '" + s.name + "' value kind mismatch");
+        }
+    }
+}
+void checkVectorValues(const Vector& U, const std::string& who, int only = -1) {
+    if (U.has_fd) return;
+    const Mesh& m = *U.m;
+    for (int p = 0; p < m.npatch; ++p) {
+        if (!visited(m, p) || (only >= 0 && p != only)) continue;
+        int k = U.bc[p].kind;
+        if (!vectorHasHandler(k)) noHandler(m, p, who + " (field " + U.name + ")");
+        if (isDirichlet(k) && U.bc[p].value_kind != PRISM_BCV_VECTOR)
+            fail(PRISM_BAD_ARG, "patch '" + m.h->patches[p].name + "' field '" + U.name + "' is not a vector");
+    }
+}
+void checkVectorFlux(const Vector& U, const std::string& who, int only = -1) {
+    if (U.has_ff) return;
+    const Mesh& m = *U.m;
+    for (int p = 0; p < m.npatch; ++p) {
+        if (!visited(m, p) || (only >= 0 && p != only)) continue;
+        int k = U.bc[p].kind;
+        if (k == PRISM_BC_NOSLIP || k == PRISM_BC_SYMMETRY) continue;
+        if (!vectorHasHandler(k)) noHandler(m, p, who + " (field " + U.name + ")");
+    }
+    checkVectorValues(U, who, only);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ mesh
+Mesh::~Mesh() {
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+}
+
+MeshView Mesh::view() const {
+    MeshView v;
+    v.nc = nc;
+    v.nf = nf;
+    v.nb = nb;
+    v.nne = nne;
+    v.npatch = npatch;
+    v.nslices = pat.nslices;
+    v.owner = owner.p;
+    v.nbr = nbr.p;
+    v.bpatch = bpatch.p;
+    v.patch_empty = patch_empty.p;
+    v.area = area.p;
+    v.nx = nx.p;
+    v.ny = ny.p;
+    v.nz = nz.p;
+    v.fx = fx.p;
+    v.fy = fy.p;
+    v.fz = fz.p;
+    v.cx = cx.p;
+    v.cy = cy.p;
+    v.cz = cz.p;
+    v.vol = vol.p;
+    v.gcw = gcw.p;
+    v.cf_off = cf_off.p;
+    v.cf_face = cf_face.p;
+    v.cf_pos = nullptr;
+    v.diag_pos = pat.diag_pos.p;
+    v.sl_off = pat.sl_off.p;
+    v.sl_col = pat.sl_col.p;
+    return v;
+}
+
+SellMatrix Mesh::matrix(const double* vals) const {
+    SellMatrix A;
+    A.n = nc;
+    A.nslices = pat.nslices;
+    A.nnz_padded = pat.sell_nnz;
+    A.sl_off = pat.sl_off.p;
+    A.col = pat.sl_col.p;
+    A.diag_pos = pat.diag_pos.p;
+    A.vals = vals;
+    A.nnz_csr = pat.nnz;
+    return A;
+}
+
+std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d) {
+    auto mesh = std::make_unique<Mesh>();
+    mesh->h = buildHostMesh(d);
+    HostMesh& h = *mesh->h;
+    if (h.nc >= (int64_t(1) << 31) || h.nf >= (int64_t(1) << 31) || (int64_t)h.cf_face.size() >= (int64_t(1) << 31))
+        fail(PRISM_INVALID_MESH, "mesh too large for 32-bit indices");
+    Mesh& m = *mesh;
+    PB_CUDA(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+    cudaStream_t s = m.stream;
+    m.nc = (int)h.nc;
+    m.nf = (int)h.nf;
+    m.nb = (int)h.nb;
+    m.nne = (int)h.nne;
+    m.npatch = (int)h.patches.size();
+    m.n_pad = ceil_div(m.nc, 32) * 32;
+    upload(m.owner, h.owner, s);
+    upload(m.nbr, h.nbr, s);
+    std::vector<int> bp(h.patch.begin(), h.patch.begin() + h.nb), ppos(h.nb, 0);
+    for (auto& pa : h.patches)
+        for (size_t i = 0; i < pa.faces.size(); ++i) ppos[pa.faces[i]] = (int)i;
+    upload(m.bpatch, bp.empty() ? std::vector<int>{0} : bp, s);
+    upload(m.ppos, ppos.empty() ? std::vector<int>{0} : ppos, s);
+    std::vector<unsigned char> pe(std::max(1, m.npatch), 0);
+    for (int p = 0; p < m.npatch; ++p) pe[p] = h.patches[p].empty ? 1 : 0;
+    upload(m.patch_empty, pe, s);
+    upload(m.area, h.area, s);
+    upload(m.nx, h.normal[0], s);
+    upload(m.ny, h.normal[1], s);
+    upload(m.nz, h.normal[2], s);
+    upload(m.fx, h.fc[0], s);
+    upload(m.fy, h.fc[1], s);
+    upload(m.fz, h.fc[2], s);
+    upload(m.cx, h.cc[0], s);
+    upload(m.cy, h.cc[1], s);
+    upload(m.cz, h.cc[2], s);
+    upload(m.vol, h.vol, s);
+    upload(m.gcw, h.gc.empty() ? std::vector<double>{0.0} : h.gc, s);
+    std::vector<int> cfo(h.cf_off.begin(), h.cf_off.end());
+    upload(m.cf_off, cfo, s);
+    upload(m.cf_face, h.cf_face, s);
+
+    PatternInput pin{m.nc, m.nb, m.npatch, (int64_t)h.cf_face.size(), m.cf_off.p, m.cf_face.p,
+                     m.owner.p, m.nbr.p, m.bpatch.p, m.ppos.p};
+    buildPattern(pin, m.pat, s);
+
+    // Green-Gauss schedule: level[c] = 1 + max(level of lower-numbered neighbours)
+    std::vector<int> level(m.nc, 0);
+    int nl = 0;
+    for (int c = 0; c < m.nc; ++c) {
+        int l = 0;
+        for (int64_t q = h.cf_off[c]; q < h.cf_off[c + 1]; ++q) {
+            int f = h.cf_face[q];
+            if (f < m.nb) continue;
+            int o = h.owner[f];
+            int n = (o == c) ? h.nbr[f] : o;
+            if (n < c) l = std::max(l, level[n] + 1);
+        }
+        level[c] = l;
+        nl = std::max(nl, l + 1);
+    }
+    m.level_off.assign(nl + 1, 0);
+    for (int c = 0; c < m.nc; ++c) m.level_off[level[c] + 1]++;
+    for (int l = 0; l < nl; ++l) m.level_off[l + 1] += m.level_off[l];
+    std::vector<int> lc(m.nc), fill(m.level_off.begin(), m.level_off.end() - 1);
+    for (int c = 0; c < m.nc; ++c) lc[fill[level[c]]++] = c;
+    upload(m.level_cells, lc, s);
+    m.scratch.alloc(std::max(3 * m.nf, 1));
+    PB_CUDA(cudaStreamSynchronize(s));
+    return mesh;
+}
+
+// LeastSquares::setPseudoInvMatrices (least_squares.cpp:12-61): pinv = (D^T D)^-1 D^T
+void Mesh::ensureLeastSquares() {
+    if (ls_ready) return;
+    const HostMesh& H = *h;
+    const int64_t nk = (int64_t)H.cf_face.size();
+    std::vector<double> pinv(9 * (size_t)nc), w(3 * (size_t)nk, 0.0);
+    for (int c = 0; c < nc; ++c) {
+        double D[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        H3 xc{H.cc[0][c], H.cc[1][c], H.cc[2][c]};
+        for (int64_t q = H.cf_off[c]; q < H.cf_off[c + 1]; ++q) {
+            int f = H.cf_face[q];
+            H3 r;
+            if (f >= nb) {
+                int o = H.owner[f];
+                int n = (o == c) ? H.nbr[f] : o;
+                r = hsub(H3{H.cc[0][n], H.cc[1][n], H.cc[2][n]}, xc);
+            } else {
+                r = hsub(H3{H.fc[0][f], H.fc[1][f], H.fc[2][f]}, xc);
+            }
+            double wk = 1 / (std::sqrt(hdot(r, r)) + EPSILON);
+            H3 wd{r.x * wk, r.y * wk, r.z * wk};
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) D[i][j] += wd[i] * r[j];
+            w[q] = wd.x;
+            w[nk + q] = wd.y;
+            w[2 * nk + q] = wd.z;
+        }
+        double P[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) P[i][j] = (D[0][i] * D[0][j] + D[1][i] * D[1][j]) + D[2][i] * D[2][j];
+        double c00 = P[1][1] * P[2][2] - P[1][2] * P[2][1];
+        double c10 = P[1][2] * P[2][0] - P[1][0] * P[2][2];
+        double c20 = P[1][0] * P[2][1] - P[1][1] * P[2][0];
+        double det = (P[0][0] * c00 + P[0][1] * c10) + P[0][2] * c20;
+        double I[3][3];
+        I[0][0] = c00 / det;
+        I[1][0] = c10 / det;
+        I[2][0] = c20 / det;
+        I[0][1] = (P[0][2] * P[2][1] - P[0][1] * P[2][2]) / det;
+        I[1][1] = (P[0][0] * P[2][2] - P[0][2] * P[2][0]) / det;
+        I[2][1] = (P[0][1] * P[2][0] - P[0][0] * P[2][1]) / det;
+        I[0][2] = (P[0][1] * P[1][2] - P[0][2] * P[1][1]) / det;
+        I[1][2] = (P[0][2] * P[1][0] - P[0][0] * P[1][2]) / det;
+        I[2][2] = (P[0][0] * P[1][1] - P[0][1] * P[1][0]) / det;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)  // (I * D^T)(i,j) = sum_k I(i,k) D(j,k)
+                pinv[(3 * i + j) * (size_t)nc + c] = (I[i][0] * D[j][0] + I[i][1] * D[j][1]) + I[i][2] * D[j][2];
+    }
+    upload(ls_pinv, pinv, stream);
+    upload(ls_w, w, stream);
+    PB_CUDA(cudaStreamSynchronize(stream));
+    ls_ready = true;
+}
+
+// ------------------------------------------------------------------ fields
+ScalarView Scalar::view() const {
+    ScalarView v;
+    v.v = this->v.p;
+    v.fv = has_fv ? fv.p : nullptr;
+    v.g = grad->g.p;
+    v.gstride = m->n_pad;
+    v.bc_kind = bc_kind.p;
+    v.bc_val = bc_val.p;
+    v.bc_vec = bc_vec.p;
+    return v;
+}
+VectorView Vector::view() const {
+    VectorView v;
+    for (int k = 0; k < 3; ++k) v.c[k] = c[k]->view();
+    v.fd = has_fd ? fd.p : nullptr;
+    v.ff = has_ff ? ff.p : nullptr;
+    v.bc_kind = bc_kind.p;
+    v.bc_vec = bc_vec.p;
+    return v;
+}
+
+// IGradient::computeAllCellGradients (green_gauss.cpp:40-45, least_squares.cpp:71-76)
+void computeGradient(Scalar& s) {
+    Mesh& m = *s.m;
+    checkScalarValues(s, "IGradient::computeAllCellGradients()");
+    if (s.grad->type == PRISM_GRAD_LEAST_SQUARES) {
+        m.ensureLeastSquares();
+        launchLeastSquares(m.view(), s.view(), m.ls_pinv.p, m.ls_w.p, (int64_t)m.h->cf_face.size(), m.stream);
+    } else {
+        launchGreenGauss(m.view(), s.view(), m.level_cells.p, m.level_off, m.stream);
+    }
+    s.grad->computed = s.event;
+}
+// gradAtCell lazy cache by event number (green_gauss.cpp:32-38)
+void ensureGradient(Scalar& s) {
+    if (s.event != s.grad->computed) computeGradient(s);
+}
+
+// ------------------------------------------------------------------ transport
+void Transport::ensure() {
+    Mesh& m = *phi->m;
+    if (!A) {
+        A.alloc(m.pat.sell_nnz);
+        b.alloc(m.n_pad);
+        bconv.alloc(m.n_pad);
+        bdiff.alloc(m.n_pad);
+        A.zero(m.stream);
+        b.zero(m.stream);
+        bconv.zero(m.stream);
+        bdiff.zero(m.stream);
+    }
+}
+
+// Transport::updateCoeffs (transport.cpp:4-21)
+void updateCoeffs(Transport& eq) {
+    Scalar& phi = *eq.phi;
+    Mesh& m = *phi.m;
+    eq.ensure();
+    const bool has_interior = m.nf > m.nb;
+    bool need_grad = false;
+    // boundary handlers of the schemes (convection_boundary.cpp, diffusion_boundary.h)
+    for (int p = 0; p < m.npatch; ++p) {
+        if (!visited(m, p)) continue;
+        const int k = phi.bc[p].kind;
+        if (eq.has_conv) {
+            if (k == PRISM_BC_FIXED) {
+                int want = phi.coord >= 0 ? PRISM_BCV_VECTOR : PRISM_BCV_SCALAR;
+                if (phi.bc[p].value_kind != want)
+                    fail(PRISM_BAD_ARG, "patch '" + m.h->patches[p].name + "' value kind mismatch for " + phi.name);
+                checkVectorFlux(*eq.U, "IConvection Fixed handler", p);
+            } else if (k == PRISM_BC_OUTLET || k == PRISM_BC_ZERO_GRADIENT) {
+                checkVectorValues(*eq.U, "IConvection Outlet handler", p);
+            } else if (k != PRISM_BC_NOSLIP && k != PRISM_BC_SYMMETRY) {
+                noHandler(m, p, "applyBoundary() applied by IConvection");
+            }
+        }
+        if (eq.has_diff) {
+            if (k == PRISM_BC_FIXED || k == PRISM_BC_NOSLIP) {
+                checkScalarValues(phi, "diffusion Fixed handler", p);
+                if (eq.corrected) need_grad = true;
+            } else if (k == PRISM_BC_FIXED_GRADIENT) {
+                if (phi.coord >= 0)
+                    fail(PRISM_BAD_ARG, "patch '" + m.h->patches[p].name + "' does not have a field named '" + phi.name + "'");
+                if (phi.bc[p].value_kind != PRISM_BCV_VECTOR)
+                    fail(PRISM_BAD_ARG, "patch '" + m.h->patches[p].name + "' field is not a vector");
+            } else if (k != PRISM_BC_SYMMETRY && k != PRISM_BC_OUTLET && k != PRISM_BC_ZERO_GRADIENT) {
+                noHandler(m, p, "applyBoundary() applied by a diffusion scheme");
+            }
+        }
+    }
+    if (has_interior && (eq.has_conv || (eq.has_diff && eq.corrected))) need_grad = true;
+    if (need_grad) ensureGradient(phi);
+    if (eq.symmetry && (!eq.has_conv || !eq.has_diff || phi.coord < 0))
+        fail(PRISM_BAD_ARG, "Symmetry<Transport> needs a convection and a diffusion scheme on a vector component");
+    AssembleParams P{};
+    P.m = m.view();
+    P.phi = phi.view();
+    P.phi_coord = phi.coord;
+    P.has_conv = eq.has_conv;
+    P.has_diff = eq.has_diff;
+    P.conv_first = eq.conv_first;
+    P.need_grad = need_grad ? 1 : 0;
+    if (eq.has_conv) {
+        P.conv.scheme = eq.conv_scheme;
+        P.conv.U = eq.U->view();  // interior faces interpolate cell values: no handler needed
+    }
+    if (eq.has_diff) {
+        P.diff.corrected = eq.corrected;
+        P.diff.corrector = eq.corrector;
+        P.diff.kappa_tensor = eq.kt ? 1 : 0;
+        if (eq.ks) P.diff.ks = eq.ks->view();  // kappa is read at cells and interior faces only
+        if (eq.kt) P.diff.kt = eq.kt->view();
+    }
+    if ((int)eq.sources.size() > MAX_SOURCES) fail(PRISM_BAD_ARG, "too many sources");
+    P.nsrc = (int)eq.sources.size();
+    for (size_t i = 0; i < eq.sources.size(); ++i) {
+        Source& src = eq.sources[i];
+        SourceDesc& S = P.src[i];
+        S.kind = src.kind;
+        S.sign = src.sign;
+        S.coord = src.coord;
+        if (src.kind == PRISM_SRC_CONSTANT) {
+            ++src.s->event;  // values() non-const (constant_scalar.h:31)
+            S.s = src.s->view();
+        } else if (src.kind == PRISM_SRC_GRADIENT) {
+            ensureGradient(*src.s);
+            S.s = src.s->view();
+        } else {
+            checkVectorFlux(*src.U, "ops::div()");
+            S.U = src.U->view();
+        }
+    }
+    P.symmetry = eq.symmetry ? 1 : 0;
+    P.accumulate = eq.clean ? 0 : 1;
+    P.ca_off = m.cf_off.p;
+    P.ca_face = m.pat.ca_face.p;
+    P.ca_pos = m.pat.ca_pos.p;
+    P.A = eq.A.p;
+    P.b = eq.b.p;
+    P.bconv = eq.bconv.p;
+    P.bdiff = eq.bdiff.p;
+    launchAssemble(P, m.stream);
+    eq.clean = false;
+}
+
+// Transport::relax (transport.cpp:54-64)
+void relax(Transport& eq) {
+    Mesh& m = *eq.phi->m;
+    eq.ensure();
+    ++eq.phi->event;
+    launchRelax(eq.A.p, eq.b.p, m.pat.diag_pos.p, eq.phi->v.p, eq.urf, m.nc, m.stream);
+}
+
+// Transport::zeroOutCoeffs (transport.cpp:23-36)
+void zeroOutCoeffs(Transport& eq) {
+    Mesh& m = *eq.phi->m;
+    eq.ensure();
+    eq.A.zero(m.stream);
+    eq.b.zero(m.stream);
+    eq.bconv.zero(m.stream);
+    eq.bdiff.zero(m.stream);
+    eq.clean = true;
+}
+
+void solveDefaults(PrismSolveOpts* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->method = PRISM_SOLVER_BICGSTAB;
+    o->precision = PRISM_PREC_FP64;
+    o->n_iter = 10;
+    o->eps = 1e-7;
+    o->ref_cell = -1;
+    o->clear_coeffs = 1;
+}
+
+// ISolver::solve (numerics/solver.cpp:27-82)
+PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
+    Scalar& phi = *eq.phi;
+    Mesh& m = *phi.m;
+    updateCoeffs(eq);
+    relax(eq);
+    if (o.ref_cell >= 0 && o.ref_cell < m.nc) {
+        int pos = 0;
+        PB_CUDA(cudaMemcpyAsync(&pos, m.pat.diag_pos.p + o.ref_cell, sizeof(int), cudaMemcpyDeviceToHost, m.stream));
+        PB_CUDA(cudaStreamSynchronize(m.stream));
+        launchPin(eq.A.p, eq.b.p, pos, (int)o.ref_cell, o.ref_value, m.stream);
+    }
+    SellMatrix A = m.matrix(eq.A.p);
+    const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
+    const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
+    const double itol = o.inner_tol > 0 ? o.inner_tol : 1e-4;
+    PrismSolveResult r{};
+    r.status = PRISM_OK;
+    double init_res = 0.0, cur = 0.0;
+    bool conv = false;
+    int64_t iter = 0;
+    for (; iter < o.n_iter; ++iter) {
+        if (iter == 0) {
+            ++phi.event;
+            init_res = scaledResidual(A, eq.b.p, phi.v.p, m.kw, m.stream);
+        }
+        phi.event += 2;
+        if (o.method == PRISM_SOLVER_JACOBI) {
+            jacobiStep(A, eq.b.p, phi.v.p, m.kw, m.stream);
+        } else {
+            KrylovOut k = bicgstab(A, eq.b.p, phi.v.p, ktol, kmax, o.precision, itol, m.kw, m.stream);
+            r.krylov_iterations += k.iterations;
+            r.krylov_rel_residual = k.rel_residual;
+            if (k.status != PRISM_OK && r.status == PRISM_OK) r.status = k.status;
+        }
+        ++phi.event;
+        cur = scaledResidual(A, eq.b.p, phi.v.p, m.kw, m.stream);
+        if (std::isnan(cur)) r.status = PRISM_NONFINITE;
+        if (cur < o.eps) {
+            conv = true;
+            ++iter;
+            break;
+        }
+    }
+    if (o.clear_coeffs) zeroOutCoeffs(eq);
+    r.iterations = iter;
+    r.initial_residual = init_res;
+    r.final_residual = cur;
+    r.converged = conv ? 1 : 0;
+    return r;
+}
+
+// ------------------------------------------------------------------ SIMPLE / PRIME / PISO
+void simpleDefaults(PrismSIMPLEControls* c) {  // SIMPLEControls, SIMPLE.h:14-43
+    c->momentum_urf = 0.7;
+    c->momentum_max_iter = 3;
+    c->momentum_residual = 1e-7;
+    c->momentum_residual_stop = 1e-5;
+    c->non_ortho_correctors = 2;
+    c->pressure_urf = 0.3;
+    c->pressure_max_iter = 5;
+    c->pressure_residual = 1e-7;
+    c->p_ref_cell = -1;
+    c->p_ref_value = 0.0;
+}
+void pisoDefaults(PrismPISOControls* c) {  // PISOControls, PISO.h:11-49
+    c->outer_iterations = 1;
+    c->momentum_implicit_steps = 1;
+    c->pressure_correction_steps = 2;
+    c->momentum_urf = 1.0;
+    c->momentum_max_iter = 3;
+    c->momentum_residual = 1e-4;
+    c->momentum_residual_stop = 1e-5;
+    c->non_ortho_correctors = 2;
+    c->pressure_urf = 1.0;
+    c->pressure_max_iter = 5;
+    c->pressure_residual = 1e-4;
+    c->p_ref_cell = -1;
+    c->p_ref_value = 0.0;
+}
+
+namespace {
+
+PrismSolveOpts inner(const PrismSolveOpts& so, int64_t n_iter, double eps, int64_t ref, double refv, bool clear) {
+    PrismSolveOpts o = so;
+    o.method = PRISM_SOLVER_BICGSTAB;
+    o.n_iter = n_iter;
+    o.eps = eps;
+    o.ref_cell = ref;
+    o.ref_value = refv;
+    o.clear_coeffs = clear ? 1 : 0;
+    return o;
+}
+
+void setURF(Transport& eq, double f) {  // transport.cpp:38-52: out-of-range values are ignored
+    if (f < 0.0 || f > 1.0) return;
+    eq.urf = f;
+}
+
+// solveImplicitMomentum, SIMPLE.cpp:19-41
+void solveImplicitMomentum(const PrismSIMPLEControls& c, std::vector<Transport*>& mom, const PrismSolveOpts& so,
+                           std::vector<Report>& rep) {
+    for (auto* eq : mom) {
+        setURF(*eq, c.momentum_urf);
+        auto r = solve(*eq, inner(so, c.momentum_max_iter, c.momentum_residual, -1, 0.0, false));
+        rep.push_back({eq->phi->name, r.iterations, r.initial_residual, r.final_residual, r.converged != 0});
+    }
+}
+
+struct PressureResult {
+    std::unique_ptr<Scalar> pp;
+    std::unique_ptr<Tensor> D;
+};
+
+// solvePressureEquation, SIMPLE.cpp:124-196
+PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transport*>& mom, Vector& U, Vector& mdot,
+                                     Scalar& p, const PrismSolveOpts& so, std::vector<Report>& rep) {
+    Mesh& m = *p.m;
+    for (auto* eq : mom) eq->ensure();
+    // pressureEquationCoeffsTensor, SIMPLE.cpp:77-108
+    auto D = std::make_unique<Tensor>();
+    D->m = &m;
+    D->diag = 1;
+    D->d.alloc(3 * (size_t)m.n_pad);
+    D->d.zero(m.stream);
+    launchDTensor(m.nc, m.pat.diag_pos.p, m.vol.p, mom[0]->A.p, mom[1]->A.p, mom.size() == 3 ? mom[2]->A.p : nullptr,
+                  D->d.p, m.n_pad, m.stream);
+    for (auto* eq : mom) zeroOutCoeffs(*eq);
+    // mdot.mapFaceValues(U.valueAtFace); mdot.mapInteriorFaceValues(rhieChowCorrectFace)
+    checkVectorFlux(mdot, "GeneralVector::initFaceData()");
+    checkVectorValues(U, "GeneralVector::valueAtFace()");
+    if (m.nf > m.nb) ensureGradient(p);
+    if (!mdot.fd) mdot.fd.alloc(3 * (size_t)std::max(m.nf, 1));
+    if (!mdot.ff) mdot.ff.alloc(std::max(m.nf, 1));
+    launchRhieChow(m.view(), U.view(), D->view(), p.view(), mdot.fd.p, mdot.ff.p, m.stream);
+    mdot.has_fd = mdot.has_ff = true;
+    // p' named like p, zero valued, with a fresh gradient scheme (scalar.cpp:260-304)
+    auto pp = std::make_unique<Scalar>();
+    pp->m = &m;
+    pp->name = p.name;
+    pp->coord = -1;
+    pp->bc = p.bc;
+    pp->v.alloc(m.n_pad);
+    pp->v.zero(m.stream);
+    pp->bc_kind.alloc(std::max(m.npatch, 1));
+    pp->bc_val.alloc(std::max(m.npatch, 1));
+    pp->bc_vec.alloc(3 * std::max(m.npatch, 1));
+    PB_CUDA(cudaMemcpyAsync(pp->bc_kind.p, p.bc_kind.p, pp->bc_kind.n * sizeof(int), cudaMemcpyDeviceToDevice, m.stream));
+    PB_CUDA(cudaMemcpyAsync(pp->bc_val.p, p.bc_val.p, pp->bc_val.n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    PB_CUDA(cudaMemcpyAsync(pp->bc_vec.p, p.bc_vec.p, pp->bc_vec.n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    pp->grad = std::make_shared<GradState>();
+    pp->grad->type = p.grad->type;
+    pp->grad->g.alloc(3 * (size_t)m.n_pad);
+    pp->grad->g.zero(m.stream);
+    // constrainPPrime, SIMPLE.cpp:43-75: every face value is 0 (Dirichlet/symmetry patches
+    // are zeroed, the others take the owner value of the zero field)
+    for (int q = 0; q < m.npatch; ++q)
+        if (!m.h->patches[q].empty && !scalarHasHandler(pp->bc[q].kind)) noHandler(m, q, "prism::algo::constrainPPrime()");
+    pp->fv.alloc(std::max(m.nf, 1));
+    pp->fv.zero(m.stream);
+    pp->has_fv = true;
+    if (c.p_ref_cell < 0 && needsPressureReference(*pp)) c.p_ref_cell = 0;
+    Transport pEqn;
+    pEqn.phi = pp.get();
+    pEqn.has_diff = 1;
+    pEqn.corrected = 1;
+    pEqn.corrector = PRISM_CORR_OVER_RELAXED;
+    pEqn.kt = D.get();
+    pEqn.sources.push_back({PRISM_SRC_DIVERGENCE, PRISM_SIGN_NEGATIVE, 0, nullptr, &mdot});
+    for (int64_t i = 0; i <= c.non_ortho_correctors; ++i) {
+        auto r = solve(pEqn, inner(so, c.pressure_max_iter, c.pressure_residual, c.p_ref_cell, c.p_ref_value, true));
+        rep.push_back({pp->name + "_corr_" + std::to_string(i), r.iterations, r.initial_residual, r.final_residual,
+                       r.converged != 0});
+    }
+    pp->has_fv = false;  // clearFaceValues
+    return {std::move(pp), std::move(D)};
+}
+
+// correctFields, SIMPLE.cpp:218-241
+void correctFields(Vector& U, Vector& mdot, Scalar& p, const Tensor& D, Scalar& pp, double urf) {
+    Mesh& m = *U.m;
+    ensureGradient(pp);
+    launchCorrectFields(m.view(), U.c[0]->view(), U.c[1]->view(), U.c[2]->view(), D.view(), pp.view(), mdot.fd.p,
+                        mdot.ff.p, p.v.p, urf, m.stream);
+    for (auto& c : U.c) ++c->event;
+    p.event += 2;
+    p.has_fv = false;
+}
+
+// solveExplicitMomentum, PRIME.cpp:39-56
+void solveExplicitMomentum(std::vector<Transport*>& mom) {
+    for (auto* eq : mom) {
+        updateCoeffs(*eq);
+        Mesh& m = *eq->phi->m;
+        m.kw.ensure(m.n_pad, m.pat.sell_nnz, false);
+        explicitUpdate(m.matrix(eq->A.p), eq->b.p, eq->phi->v.p, m.kw.tmp.p, m.stream);
+        PB_CUDA(cudaMemcpyAsync(eq->phi->v.p, m.kw.tmp.p, m.nc * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+        eq->phi->event += 3;
+    }
+}
+
+}  // namespace
+
+bool needsPressureReference(const Scalar& p) {  // SIMPLE.cpp:110-122
+    for (int q = 0; q < p.m->npatch; ++q) {
+        if (p.m->h->patches[q].empty) continue;
+        if (isDirichlet(p.bc[q].kind)) return false;
+    }
+    return true;
+}
+
+void simpleStep(const PrismSIMPLEControls& c, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
+                const PrismSolveOpts& so, std::vector<Report>& rep) {
+    if (mom.size() != 2 && mom.size() != 3) fail(PRISM_BAD_ARG, "SIMPLE expects 2 or 3 momentum predictors");
+    solveImplicitMomentum(c, mom, so, rep);
+    auto r = solvePressureEquation(c, mom, U, mdot, p, so, rep);
+    correctFields(U, mdot, p, *r.D, *r.pp, c.pressure_urf);
+}
+
+void primeStep(const PrismSIMPLEControls& pc, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
+               const PrismSolveOpts& so, std::vector<Report>& rep) {
+    if (mom.size() != 2 && mom.size() != 3) fail(PRISM_BAD_ARG, "PRIME expects 2 or 3 momentum predictors");
+    solveExplicitMomentum(mom);
+    PrismSIMPLEControls c;
+    simpleDefaults(&c);
+    c.non_ortho_correctors = pc.non_ortho_correctors;
+    c.pressure_urf = pc.pressure_urf;
+    c.pressure_max_iter = pc.pressure_max_iter;
+    c.pressure_residual = pc.pressure_residual;
+    c.p_ref_cell = pc.p_ref_cell;
+    c.p_ref_value = pc.p_ref_value;
+    auto r = solvePressureEquation(c, mom, U, mdot, p, so, rep);
+    correctFields(U, mdot, p, *r.D, *r.pp, pc.pressure_urf);
+}
+
+void pisoStep(const PrismPISOControls& pc, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
+              const PrismSolveOpts& so, std::vector<Report>& rep) {
+    PrismSIMPLEControls sc;
+    simpleDefaults(&sc);
+    sc.momentum_urf = pc.momentum_urf;
+    sc.momentum_max_iter = pc.momentum_max_iter;
+    sc.momentum_residual = pc.momentum_residual;
+    sc.momentum_residual_stop = pc.momentum_residual_stop;
+    sc.non_ortho_correctors = pc.non_ortho_correctors;
+    sc.pressure_urf = pc.pressure_urf;
+    sc.pressure_max_iter = pc.pressure_max_iter;
+    sc.pressure_residual = pc.pressure_residual;
+    sc.p_ref_cell = pc.p_ref_cell;
+    sc.p_ref_value = pc.p_ref_value;
+    for (int64_t i = 0; i < pc.outer_iterations; ++i) {
+        for (int64_t j = 0; j < pc.momentum_implicit_steps; ++j) simpleStep(sc, mom, U, mdot, p, so, rep);
+        for (int64_t j = 1; j < pc.pressure_correction_steps; ++j) primeStep(sc, mom, U, mdot, p, so, rep);
+    }
+}
+
+}  // namespace pb

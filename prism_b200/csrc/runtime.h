@@ -1,0 +1,129 @@
+// runtime.h -- host objects behind the C-ABI handles: the device mesh, fields,
+// equations, and the solve / SIMPLE / PRIME / PISO drivers.
+#pragma once
+
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "assemble.h"
+#include "common.h"
+#include "krylov.h"
+#include "mesh_build.h"
+#include "pattern.h"
+#include "views.h"
+
+namespace pb {
+
+struct Mesh {
+    std::unique_ptr<HostMesh> h;
+    cudaStream_t stream = nullptr;
+    int nc = 0, nf = 0, nb = 0, nne = 0, npatch = 0, n_pad = 0;
+    DevBuf<int> owner, nbr, bpatch, ppos, cf_off, cf_face;
+    DevBuf<unsigned char> patch_empty;
+    DevBuf<double> area, nx, ny, nz, fx, fy, fz, cx, cy, cz, vol, gcw;
+    PatternOutput pat;
+    // Green-Gauss sweep schedule: cells grouped by dependency level
+    DevBuf<int> level_cells;
+    std::vector<int> level_off;
+    // least-squares operators (built on first use, shared by every field)
+    DevBuf<double> ls_pinv, ls_w;
+    bool ls_ready = false;
+    KrylovWork kw;
+    DevBuf<double> scratch;  // n_faces doubles for face exports
+
+    ~Mesh();
+    MeshView view() const;
+    SellMatrix matrix(const double* vals) const;
+    void ensureLeastSquares();
+};
+
+std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d);
+
+struct GradState {
+    int type = PRISM_GRAD_LEAST_SQUARES;
+    DevBuf<double> g;  // 3 * n_pad
+    uint64_t computed = std::numeric_limits<uint64_t>::max();
+};
+
+struct Scalar {
+    Mesh* m = nullptr;
+    std::string name;
+    int coord = -1;  // component of a vector field
+    DevBuf<double> v;
+    DevBuf<double> fv;
+    bool has_fv = false;
+    std::vector<PrismBC> bc;
+    DevBuf<int> bc_kind;
+    DevBuf<double> bc_val, bc_vec;
+    std::shared_ptr<GradState> grad;
+    uint64_t event = 0;
+    ScalarView view() const;
+};
+
+struct Vector {
+    Mesh* m = nullptr;
+    std::string name;
+    std::shared_ptr<Scalar> c[3];
+    DevBuf<double> fd, ff;
+    bool has_fd = false, has_ff = false;
+    std::vector<PrismBC> bc;
+    DevBuf<int> bc_kind;
+    DevBuf<double> bc_vec;
+    VectorView view() const;
+};
+
+struct Tensor {
+    Mesh* m = nullptr;
+    DevBuf<double> d;
+    int diag = 0;
+    TensorView view() const { return {d.p, (int64_t)m->n_pad, diag}; }
+};
+
+struct Source {
+    int kind, sign, coord;
+    Scalar* s = nullptr;
+    Vector* U = nullptr;
+};
+
+struct Transport {
+    Scalar* phi = nullptr;
+    int has_conv = 0, conv_scheme = 0, has_diff = 0, corrected = 0, corrector = 0, conv_first = 1;
+    Vector* U = nullptr;
+    Scalar* ks = nullptr;
+    Tensor* kt = nullptr;
+    std::vector<Source> sources;
+    bool symmetry = false;
+    double urf = 1.0;
+    bool clean = true;
+    DevBuf<double> A, b, bconv, bdiff;
+    void ensure();
+};
+
+// operations (mirroring the reference call structure)
+void ensureGradient(Scalar& s);
+void computeGradient(Scalar& s);
+void updateCoeffs(Transport& eq);
+void relax(Transport& eq);
+void zeroOutCoeffs(Transport& eq);
+PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o);
+
+struct Report {
+    std::string name;
+    int64_t n;
+    double init, fin;
+    bool conv;
+};
+void simpleStep(const PrismSIMPLEControls& c, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
+                const PrismSolveOpts& so, std::vector<Report>& rep);
+void primeStep(const PrismSIMPLEControls& c, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
+               const PrismSolveOpts& so, std::vector<Report>& rep);
+void pisoStep(const PrismPISOControls& c, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
+              const PrismSolveOpts& so, std::vector<Report>& rep);
+bool needsPressureReference(const Scalar& p);
+void simpleDefaults(PrismSIMPLEControls* c);
+void pisoDefaults(PrismPISOControls* c);
+void solveDefaults(PrismSolveOpts* o);
+
+}  // namespace pb

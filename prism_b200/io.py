@@ -192,6 +192,20 @@ def read_case(fields_json_path):
     """MeshBoundary (mesh/boundary.cpp:291-319) for a fields.json file."""
     with open(fields_json_path) as fh:
         doc = json.load(fh)
+    base = os.path.dirname(fields_json_path)
+    docs = {}
+    for f in doc.get("fields", []) if isinstance(doc.get("fields"), list) else []:
+        if isinstance(f, dict) and "name" in f:
+            path = os.path.join(base, f["name"] + ".json")
+            if os.path.exists(path):
+                with open(path) as fh:
+                    docs[f["name"]] = json.load(fh)
+    return case_from_docs(doc, docs)
+
+
+def case_from_docs(doc, field_docs):
+    """MeshBoundary from an already parsed fields.json document and the parsed
+    <name>.json documents (name -> document)."""
     if "fields" not in doc or not isinstance(doc["fields"], list):
         raise ValueError("Couldn't find definition for fields in boundary conditions file")
     info = {}
@@ -201,15 +215,12 @@ def read_case(fields_json_path):
             raise ValueError("Field must contain name and type")
         info[f["name"]] = f
         order.append(f["name"])
-    base = os.path.dirname(fields_json_path)
     per_field = {}
     for name in order:
-        path = os.path.join(base, name + ".json")
-        if not os.path.exists(path):
+        if name not in field_docs:
             raise ValueError("Some field defined in `fields.json` file are not present in a "
                              "dedicated boundary conditions file")
-        with open(path) as fh:
-            d = json.load(fh)
+        d = field_docs[name]
         if "patches" not in d or not isinstance(d["patches"], list):
             raise ValueError(f"file `{name}` doesn't contain a `patches` array")
         m = {}

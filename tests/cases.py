@@ -1,0 +1,188 @@
+"""Case builders shared by the tests: the reference's own test cases (from the
+golden fixtures) and the synthetic configurations, built on any library that
+exposes the C-ABI (the sm_100a library or the CPU oracle)."""
+import json
+import os
+
+import numpy as np
+
+from prism_b200 import _abi as A
+from prism_b200 import api, io, meshgen
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+# ---------------------------------------------------------------- golden cases
+def load_golden(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    meta = json.loads(str(z["meta"]))
+    goff = z["group_offsets"]
+    gel = z["group_elements"].astype(np.int64)
+    groups = [(g, bool(z["group_is_vertex"][i]), gel[goff[i]:goff[i + 1]])
+              for i, g in enumerate(meta["groups"])]
+    unv = io.UnvData(z["xyz"], z["elem_kind"].astype(np.int32), z["elem_offsets"].astype(np.int64),
+                     z["elem_nodes"].astype(np.int64), groups)
+    case = io.case_from_docs(meta["fields"], meta["docs"])
+    extra = {k: z[k] for k in z.files if k.startswith("foam_")}
+    return unv, case, extra
+
+
+def load_oracle_results(name):
+    z = np.load(os.path.join(GOLDEN, name + "_oracle.npz"))
+    return {k: z[k] for k in z.files}
+
+
+def rel_l2(x, ref):
+    return float(np.linalg.norm(x - ref) / np.linalg.norm(ref))
+
+
+def poisson_reference(unv, case, lib, solver=None, correctors=5, steps=15):
+    """tests/test_poisson.cpp:24-50: Corrected(c = I, P) + ConstantScalar(S), 5 x solve(15, 1e-20)."""
+    mesh = api.Mesh(unv, case, lib=lib)
+    cc = mesh.export()["cell_center"]
+    P = api.Scalar("P", mesh, 0.0)
+    S = api.Scalar("S", mesh, 2 * np.pi ** 2 * np.sin(np.pi * cc[0]) * np.cos(np.pi * cc[1]))
+    c = api.Tensor("c", mesh, np.eye(3))
+    eqn = api.Transport(api.diffusion.Corrected(c, P), api.source.ConstantScalar(S))
+    solver = solver or api.BiCGSTAB()
+    for _ in range(correctors):
+        solver.solve(eqn, steps, 1e-20)
+    exact = np.sin(np.pi * cc[0]) * np.cos(np.pi * cc[1])
+    x = P.values()
+    return {"P": x, "rel_l2": np.array(rel_l2(x, exact))}
+
+
+def advection_reference(unv, case, lib, solver=None):
+    """tests/test_advection_1d.cpp:24-65: Upwind(U, T) + NonCorrected(0.1, T), 5 x solve(5, 1e-20)."""
+    mesh = api.Mesh(unv, case, lib=lib)
+    cc = mesh.export()["cell_center"]
+    T = api.Scalar("T", mesh, 0.0)
+    pi = case.patch_names.index("Inlet")
+    uin = case.fields["U"][pi].vector
+    U = api.Vector("U", mesh, uin)
+    kappa = api.Scalar("kappa", mesh, 0.1)
+    eqn = api.Transport(api.convection.Upwind(U, T), api.diffusion.NonCorrected(kappa, T))
+    solver = solver or api.BiCGSTAB()
+    for _ in range(5):
+        solver.solve(eqn, 5, 1e-20)
+    u = uin[0]
+    exact = -((np.exp(u * cc[0] / 0.1) - 1) / (np.exp(u / 0.1) - 1)) + 1
+    x = T.values()
+    return {"T": x, "diff_norm": np.array(np.linalg.norm(x - exact))}
+
+
+def simple_fields(mesh, nu=1e-3):
+    """makePressureVelocityFields (tests/test_utils.h:176-195)."""
+    U = api.Vector("U", mesh, (0.0, 0.0, 0.0))
+    p = api.Scalar("P", mesh, 0.0)
+    nuf = api.Scalar("nu", mesh, nu)
+    mdot = U.clone()
+    return U, p, nuf, mdot
+
+
+def momentum_eqns(U, p, nu, mdot, conv="LinearUpwind", symmetry=False, n=2):
+    """MomentumEquations<div, Corrected, Gradient<Negative>> (tests/test_utils.h:197-217)."""
+    eqs = []
+    comps = [U.x(), U.y(), U.z()]
+    for k in range(n):
+        e = api.Transport(getattr(api.convection, conv)(mdot, comps[k]),
+                          api.diffusion.Corrected(nu, comps[k]),
+                          api.source.Gradient(p, k, A.SIGN_NEGATIVE))
+        if symmetry:
+            e.add_symmetry_handler()
+        eqs.append(e)
+    return eqs
+
+
+def simple_reference(unv, case, lib, iters=100, symmetry=False, nu=1e-3, solver=None):
+    """tests/test_simple_coarse_pipe.cpp / test_simple_duct_symmetry.cpp: SIMPLE x iters."""
+    mesh = api.Mesh(unv, case, lib=lib)
+    U, p, nuf, mdot = simple_fields(mesh, nu)
+    eqs = momentum_eqns(U, p, nuf, mdot, symmetry=symmetry)
+    simple = api.IncompressibleSIMPLE(api.SIMPLEControls(), solver=solver)
+    reps = []
+    for _ in range(iters):
+        reps = simple.step(eqs, U, mdot, p)
+    flux = U.face_flux()
+    ex = mesh.export()
+    pfo, pf = ex["patch_face_offsets"], ex["patch_faces"]
+    rates = {}
+    for i, name in enumerate(case.patch_names):
+        rates[name] = float(flux[pf[pfo[i]:pfo[i + 1]]].sum())
+    return {"p": p.values(), "U": U.values(), "mdot_flux": mdot.face_flux(),
+            "rates": np.array([rates[n] for n in case.patch_names]),
+            "needs_ref": np.array(api.needs_pressure_reference(p)),
+            "last_report_iters": np.array([r.n_iterations for r in reps])}
+
+
+def run_reference_test(name, lib, solver=None):
+    unv, case, extra = load_golden(name)
+    if name.startswith("poisson"):
+        return poisson_reference(unv, case, lib, solver)
+    if name == "versteeg_advection_1d":
+        return advection_reference(unv, case, lib, solver)
+    if name == "coarse_pipe":
+        return simple_reference(unv, case, lib, 100, solver=solver)
+    if name == "cavity_hex":
+        return simple_reference(unv, case, lib, 20, nu=0.01, solver=solver)
+    if name == "duct_simple":
+        return simple_reference(unv, case, lib, 100, symmetry=True, solver=solver)
+    raise KeyError(name)
+
+
+# ---------------------------------------------------------------- synthetic configurations
+def box_case(bcs, fields_info=None):
+    """Case over the box patches; bcs: field -> {patch: (kind, value)} (missing -> zero-gradient)."""
+    fields = {}
+    for f, per in bcs.items():
+        fields[f] = {p: per.get(p, ("zero-gradient", None)) for p in meshgen.PATCHES}
+    return io.Case.from_dict(meshgen.PATCHES, fields, fields_info)
+
+
+def poisson_c1(n, lib, nz=1, lengths=(1.0, 1.0, 0.01)):
+    """-div(grad P) = 2 pi^2 sin(pi x) cos(pi y) on an n x n x nz box; Fixed P = exact on the
+    four side walls (face values), symmetry front/back; NonCorrected, kappa = 1."""
+    unv = meshgen.box_hex(n, n, nz, lengths)
+    case = box_case({"P": {"left": ("fixed", 0.0), "right": ("fixed", 0.0), "bottom": ("fixed", 0.0),
+                           "top": ("fixed", 0.0), "back": ("symmetry", None), "front": ("symmetry", None)}})
+    mesh = api.Mesh(unv, case, lib=lib)
+    ex = mesh.export()
+    cc, fc = ex["cell_center"], ex["face_center"]
+    P = api.Scalar("P", mesh, 0.0)
+    P.set_face_values(np.sin(np.pi * fc[0]) * np.cos(np.pi * fc[1]))
+    S = api.Scalar("S", mesh, 2 * np.pi ** 2 * np.sin(np.pi * cc[0]) * np.cos(np.pi * cc[1]))
+    kappa = api.Scalar("kappa", mesh, 1.0)
+    eqn = api.Transport(api.diffusion.NonCorrected(kappa, P), api.source.ConstantScalar(S))
+    return mesh, P, eqn, np.sin(np.pi * cc[0]) * np.cos(np.pi * cc[1])
+
+
+def cavity(n, lib, nu=0.01, conv="Upwind"):
+    """Lid-driven cavity on n x n x 1 hexes: lid (top) fixed [1,0,0], other walls no-slip,
+    front/back empty, P zero-gradient everywhere (auto reference cell 0)."""
+    unv = meshgen.box_hex(n, n, 1, (1.0, 1.0, 1.0 / n))
+    wall = ("no-slip", [0.0, 0.0, 0.0])
+    case = box_case({"U": {"top": ("fixed", [1.0, 0.0, 0.0]), "left": wall, "right": wall, "bottom": wall,
+                           "back": ("empty", None), "front": ("empty", None)},
+                     "P": {"back": ("empty", None), "front": ("empty", None)}})
+    mesh = api.Mesh(unv, case, lib=lib)
+    U, p, nuf, mdot = simple_fields(mesh, nu)
+    eqs = momentum_eqns(U, p, nuf, mdot, conv=conv)
+    return mesh, U, p, nuf, mdot, eqs
+
+
+def transport_c3(n, lib, conv="MUSCL", jitter=0.2, seed=3, kappa=1e-3):
+    """div(U T) - div(kappa grad T) = 0 on a jittered n^3 box, U = (sin pi x cos pi y,
+    -cos pi x sin pi y, 0) at cell centroids; T fixed 1 at x=0 and 0 at x=1, zero-gradient
+    elsewhere; Corrected diffusion; Green-Gauss gradients."""
+    unv = meshgen.box_hex(n, n, n, jitter=jitter, seed=seed)
+    case = box_case({"T": {"left": ("fixed", 1.0), "right": ("fixed", 0.0)}, "U": {}},
+                    {"T": {"gradScheme": "greenGauss"}, "U": {}})
+    mesh = api.Mesh(unv, case, lib=lib)
+    cc = mesh.export()["cell_center"]
+    Uv = np.stack([np.sin(np.pi * cc[0]) * np.cos(np.pi * cc[1]),
+                   -np.cos(np.pi * cc[0]) * np.sin(np.pi * cc[1]), np.zeros(mesh.n_cells)])
+    U = api.Vector("U", mesh, Uv)
+    T = api.Scalar("T", mesh, 0.0)
+    k = api.Scalar("kappa", mesh, kappa)
+    eqn = api.Transport(getattr(api.convection, conv)(U, T), api.diffusion.Corrected(k, T))
+    return mesh, T, U, eqn

@@ -1,0 +1,117 @@
+"""Linear solves and the pressure-velocity drivers on the GPU vs the oracle.
+
+The oracle's step() is Eigen-style ILUT-BiCGSTAB to machine precision; the GPU
+step is Jacobi-preconditioned BiCGSTAB to ||b - Ax|| <= 1e-12 ||b|| (FP64) or
+FP32 inner iterations in FP64 refinement (mixed). Solved fields must agree with
+the oracle within 1e-8 relative L2 (the error is printed)."""
+import numpy as np
+import pytest
+
+from prism_b200 import _abi as A
+from prism_b200 import api
+from tests import cases
+from tests.test_oracle_pins import _tridiag
+
+pytestmark = pytest.mark.gpu
+SOL_TOL = 1e-8
+
+
+@pytest.mark.parametrize("solver", [api.BiCGSTAB, api.Jacobi])
+def test_solver_tridiagonal(gpu, solver):
+    # tests/test_solver.cpp:35-57
+    rp, col, val, b, x_exact = _tridiag()
+    x = np.zeros(10)
+    s = solver()
+    for _ in range(20):
+        x = s.step(gpu, rp, col, val, x, b)
+    assert np.linalg.norm(x - x_exact) / np.linalg.norm(x_exact) < 1e-4
+
+
+def test_jacobi_step_matches_oracle(gpu, orc):
+    rng = np.random.default_rng(1)
+    rp, col, val, b, _ = _tridiag(10)
+    x0 = rng.normal(size=10)
+    xg = api.Jacobi().step(gpu, rp, col, val, x0, b)
+    xo = api.Jacobi().step(orc, rp, col, val, x0, b)
+    np.testing.assert_allclose(xg, xo, rtol=1e-14, atol=1e-14)
+
+
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_poisson_c1_solve(gpu, orc, precision):
+    res = {}
+    for name, lib, solver in (("gpu", gpu, api.BiCGSTAB(precision=precision, krylov_tol=1e-12)),
+                              ("orc", orc, api.BiCGSTAB())):
+        mesh, P, eqn, exact = cases.poisson_c1(32, lib)
+        r = solver.solve(eqn, 3, 1e-10)
+        res[name] = (P.values(), r, exact)
+    err = cases.rel_l2(res["gpu"][0], res["orc"][0])
+    print(f"C1 32x32 precision={precision}: rel L2 vs oracle {err:.3e}, krylov it {res['gpu'][1].krylov_iterations}")
+    assert err < SOL_TOL
+    assert res["gpu"][1].converged
+
+
+@pytest.mark.parametrize("name", ["poisson_hex", "poisson_wedge", "versteeg_advection_1d"])
+def test_reference_cases(gpu, name):
+    ref = cases.load_oracle_results(name)
+    got = cases.run_reference_test(name, gpu)
+    key = {"poisson_hex": "P", "poisson_wedge": "P", "versteeg_advection_1d": "T"}[name]
+    err = cases.rel_l2(got[key], ref[key])
+    print(f"{name}: rel L2 vs oracle {err:.3e}")
+    assert err < SOL_TOL
+    if name == "poisson_hex":
+        assert got["rel_l2"] < 4e-4        # tests/test_poisson.cpp:58-62
+    if name == "poisson_wedge":
+        assert got["rel_l2"] < 0.078       # tests/test_poisson.cpp:52-56
+    if name == "versteeg_advection_1d":
+        assert got["diff_norm"] < 0.25 and np.all(np.diff(got["T"]) <= 0)
+
+
+@pytest.mark.parametrize("name", ["coarse_pipe", "cavity_hex", "duct_simple"])
+def test_simple_reference_cases(gpu, name):
+    unv, case, extra = cases.load_golden(name)
+    ref = cases.load_oracle_results(name)
+    got = cases.run_reference_test(name, gpu)
+    for k in ("p", "U"):
+        err = cases.rel_l2(got[k], ref[k])
+        print(f"{name} {k}: rel L2 vs oracle {err:.3e}")
+        assert err < SOL_TOL
+    assert bool(got["needs_ref"]) == bool(ref["needs_ref"])
+    if name == "coarse_pipe":  # tests/test_simple_coarse_pipe.cpp:36-49
+        assert cases.rel_l2(got["p"], extra["foam_p"]) < 0.005
+        assert cases.rel_l2(got["U"][0], extra["foam_U"][:, 0]) < 0.005
+        assert cases.rel_l2(got["U"][1], extra["foam_U"][:, 1]) < 0.09
+    if name == "duct_simple":  # tests/test_simple_duct_symmetry.cpp:38-53
+        assert cases.rel_l2(got["p"], extra["foam_p"]) < 0.025
+        assert cases.rel_l2(got["U"][0], extra["foam_U"][:, 0]) < 0.07
+        assert cases.rel_l2(got["U"][1], extra["foam_U"][:, 1]) < 0.007
+
+
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_cavity_simple_vs_oracle(gpu, orc, precision):
+    out = {}
+    for name, lib in (("gpu", gpu), ("orc", orc)):
+        mesh, U, p, nu, mdot, eqs = cases.cavity(16, lib)
+        solver = api.BiCGSTAB(precision=precision) if name == "gpu" else api.BiCGSTAB()
+        simple = api.IncompressibleSIMPLE(api.SIMPLEControls(), solver=solver)
+        for _ in range(10):
+            reps = simple.step(eqs, U, mdot, p)
+        out[name] = (U.values(), p.values(), mdot.face_flux(), reps)
+    for i, k in enumerate(("U", "p", "mdot")):
+        err = cases.rel_l2(out["gpu"][i], out["orc"][i])
+        print(f"cavity 16x16 precision={precision} {k}: rel L2 vs oracle {err:.3e}")
+        assert err < SOL_TOL
+    assert [r.field_name for r in out["gpu"][3]] == [r.field_name for r in out["orc"][3]]
+
+
+def test_piso_vs_oracle(gpu, orc):
+    out = {}
+    for name, lib in (("gpu", gpu), ("orc", orc)):
+        mesh, U, p, nu, mdot, eqs = cases.cavity(12, lib, conv="LinearUpwind")
+        piso = api.PISO(api.PISOControls(momentum_urf=0.7, pressure_urf=0.3))
+        for _ in range(3):
+            piso.step(eqs, U, mdot, p)
+        out[name] = (U.values(), p.values())
+    for i, k in enumerate(("U", "p")):
+        err = cases.rel_l2(out["gpu"][i], out["orc"][i])
+        print(f"PISO cavity {k}: rel L2 vs oracle {err:.3e}")
+        assert err < SOL_TOL
