@@ -339,6 +339,7 @@ typedef struct {
     int64_t fp32_launches;
     double fp32_ms;
     double fp32_bytes;
+    int64_t kernel_launches; /* every kernel this library launched in the window */
 } PrismProfile;
 int prism_profile_start(int32_t max_samples);
 int prism_profile_stop(PrismProfile* out);

@@ -102,7 +102,8 @@ class Report(C.Structure):
 
 class Profile(C.Structure):
     _fields_ = [("fp64_launches", i64), ("fp64_ms", f64), ("fp64_bytes", f64),
-                ("fp32_launches", i64), ("fp32_ms", f64), ("fp32_bytes", f64)]
+                ("fp32_launches", i64), ("fp32_ms", f64), ("fp32_bytes", f64),
+                ("kernel_launches", i64)]
 
 
 PP = C.POINTER(P)

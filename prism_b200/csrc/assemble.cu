@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(256) assemble_kernel(const AssembleParams P) {
 
 void launchAssemble(const AssembleParams& P, cudaStream_t s) {
     if (P.m.nc == 0) return;
-    assemble_kernel<<<ceil_div(P.m.nc, 256), 256, 0, s>>>(P);
+    assemble_kernel<<<ceil_div(P.m.nc, 256), 256, 0, s>>>(P); countLaunch();
     PB_LAUNCH("assemble_kernel");
 }
 
@@ -299,7 +299,7 @@ __global__ void relax_kernel(double* A, double* b, const int* diag_pos, const do
 }
 void launchRelax(double* A, double* b, const int* diag_pos, const double* phi, double alpha, int n, cudaStream_t s) {
     if (n == 0) return;
-    relax_kernel<<<ceil_div(n, 256), 256, 0, s>>>(A, b, diag_pos, phi, alpha, n);
+    relax_kernel<<<ceil_div(n, 256), 256, 0, s>>>(A, b, diag_pos, phi, alpha, n); countLaunch();
     PB_LAUNCH("relax_kernel");
 }
 
@@ -310,7 +310,7 @@ __global__ void pin_kernel(double* A, double* b, int pos, int row, double ref_va
     b[row] += diag * ref_value;
 }
 void launchPin(double* A, double* b, int pos, int row, double ref_value, cudaStream_t s) {
-    pin_kernel<<<1, 1, 0, s>>>(A, b, pos, row, ref_value);
+    pin_kernel<<<1, 1, 0, s>>>(A, b, pos, row, ref_value); countLaunch();
     PB_LAUNCH("pin_kernel");
 }
 

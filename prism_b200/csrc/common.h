@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -75,6 +76,13 @@ struct DevBuf {
     }
     explicit operator bool() const { return p != nullptr; }
 };
+
+// Number of kernels this library has launched (read by the profiling window).
+inline std::atomic<long long>& launchCounter() {
+    static std::atomic<long long> c{0};
+    return c;
+}
+inline void countLaunch() { launchCounter().fetch_add(1, std::memory_order_relaxed); }
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 

@@ -25,7 +25,7 @@ __global__ void d_tensor_kernel(int n, const int* diag_pos, const double* vol, c
 void launchDTensor(int n, const int* diag_pos, const double* vol, const double* Au, const double* Av,
                    const double* Aw, double* D, int64_t stride, cudaStream_t s) {
     if (n == 0) return;
-    d_tensor_kernel<<<ceil_div(n, 256), 256, 0, s>>>(n, diag_pos, vol, Au, Av, Aw, D, stride);
+    d_tensor_kernel<<<ceil_div(n, 256), 256, 0, s>>>(n, diag_pos, vol, Au, Av, Aw, D, stride); countLaunch();
     PB_LAUNCH("d_tensor_kernel");
 }
 
@@ -64,7 +64,7 @@ __global__ void rhie_chow_kernel(const MeshView m, const VectorView U, const Ten
 void launchRhieChow(const MeshView& m, const VectorView& U, const TensorView& D, const ScalarView& P, double* fd,
                     double* ff, cudaStream_t s) {
     if (m.nf == 0) return;
-    rhie_chow_kernel<<<ceil_div(m.nf, 256), 256, 0, s>>>(m, U, D, P, fd, ff);
+    rhie_chow_kernel<<<ceil_div(m.nf, 256), 256, 0, s>>>(m, U, D, P, fd, ff); countLaunch();
     PB_LAUNCH("rhie_chow_kernel");
 }
 
@@ -99,15 +99,15 @@ void launchCorrectFields(const MeshView& m, const ScalarView& ux, const ScalarVi
                          const TensorView& D, const ScalarView& pp, double* fd, double* ff, double* p, double urf,
                          cudaStream_t s) {
     if (m.nc) {
-        correct_u_kernel<<<ceil_div(m.nc, 256), 256, 0, s>>>(m.nc, ux, uy, uz, D, pp);
+        correct_u_kernel<<<ceil_div(m.nc, 256), 256, 0, s>>>(m.nc, ux, uy, uz, D, pp); countLaunch();
         PB_LAUNCH("correct_u_kernel");
     }
     if (m.nf > m.nb) {
-        correct_mdot_kernel<<<ceil_div(m.nf - m.nb, 256), 256, 0, s>>>(m, D, pp, fd, ff);
+        correct_mdot_kernel<<<ceil_div(m.nf - m.nb, 256), 256, 0, s>>>(m, D, pp, fd, ff); countLaunch();
         PB_LAUNCH("correct_mdot_kernel");
     }
     if (m.nc) {
-        correct_p_kernel<<<ceil_div(m.nc, 256), 256, 0, s>>>(m.nc, p, pp.v, urf);
+        correct_p_kernel<<<ceil_div(m.nc, 256), 256, 0, s>>>(m.nc, p, pp.v, urf); countLaunch();
         PB_LAUNCH("correct_p_kernel");
     }
 }

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) gg_level_kernel(const MeshView m, ScalarV
 void launchLeastSquares(const MeshView& m, const ScalarView& s, const double* pinv, const double* w, int64_t nk,
                         cudaStream_t st) {
     if (m.nc == 0) return;
-    ls_grad_kernel<<<ceil_div(m.nc, 256), 256, 0, st>>>(m, s, pinv, w, nk);
+    ls_grad_kernel<<<ceil_div(m.nc, 256), 256, 0, st>>>(m, s, pinv, w, nk); countLaunch();
     PB_LAUNCH("ls_grad_kernel");
 }
 
@@ -89,7 +89,7 @@ void launchGreenGauss(const MeshView& m, const ScalarView& s, const int* level_c
     for (size_t l = 0; l + 1 < level_off.size(); ++l) {
         int count = level_off[l + 1] - level_off[l];
         if (count == 0) continue;
-        gg_level_kernel<<<ceil_div(count, 256), 256, 0, st>>>(m, s, level_cells + level_off[l], count);
+        gg_level_kernel<<<ceil_div(count, 256), 256, 0, st>>>(m, s, level_cells + level_off[l], count); countLaunch();
     }
     PB_LAUNCH("gg_level_kernel");
 }
@@ -107,12 +107,12 @@ __global__ void vector_flux_kernel(const MeshView m, VectorView U, double* out) 
 }
 void launchScalarFaces(const MeshView& m, const ScalarView& s, double* out, cudaStream_t st) {
     if (m.nf == 0) return;
-    scalar_faces_kernel<<<ceil_div(m.nf, 256), 256, 0, st>>>(m, s, out);
+    scalar_faces_kernel<<<ceil_div(m.nf, 256), 256, 0, st>>>(m, s, out); countLaunch();
     PB_LAUNCH("scalar_faces_kernel");
 }
 void launchVectorFlux(const MeshView& m, const VectorView& U, double* out, cudaStream_t st) {
     if (m.nf == 0) return;
-    vector_flux_kernel<<<ceil_div(m.nf, 256), 256, 0, st>>>(m, U, out);
+    vector_flux_kernel<<<ceil_div(m.nf, 256), 256, 0, st>>>(m, U, out); countLaunch();
     PB_LAUNCH("vector_flux_kernel");
 }
 

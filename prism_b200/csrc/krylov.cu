@@ -358,7 +358,7 @@ KrylovWork::~KrylovWork() {
 
 void spmv(const SellMatrix& A, const double* x, double* y, cudaStream_t s) {
     spmv_kernel<double, 0><<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, x, y, nullptr,
-                                                              nullptr, nullptr, nullptr);
+                                                              nullptr, nullptr, nullptr); countLaunch();
     PB_LAUNCH("spmv_kernel");
 }
 
@@ -372,6 +372,7 @@ struct Sample {
 };
 struct Profiler {
     bool on = false;
+    long long launches0 = 0;
     int max_samples = 0;
     std::vector<Sample> samples;
     std::vector<cudaEvent_t> pool;
@@ -427,23 +428,23 @@ KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, 
     while (true) {
         if (!zero)
             spmv_kernel<T, 0><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.x, V.r, nullptr, nullptr, nullptr,
-                                                nullptr);
-        init_kernel<T><<<vg, BS, 0, s>>>(n, V.r, rhs, V.r0, V.p, V.v, zero ? 1 : 0, tol, w.partials.p, w.counter.p, S);
+                                                nullptr); countLaunch();
+        init_kernel<T><<<vg, BS, 0, s>>>(n, V.r, rhs, V.r0, V.p, V.v, zero ? 1 : 0, tol, w.partials.p, w.counter.p, S); countLaunch();
         PB_LAUNCH("bicgstab init");
         zero = false;
         int done = 0;
         while (true) {
             for (long long it = 0; it < batch; ++it) {
-                p_kernel<T><<<vg, BS, 0, s>>>(n, V.p, V.r, V.v, S);
+                p_kernel<T><<<vg, BS, 0, s>>>(n, V.p, V.r, V.v, S); countLaunch();
                 Sample smp;
                 bool sampled = sampleBegin<T>(smp, A, s);
                 spmv_kernel<T, 1><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.p, V.v, V.r0, w.partials.p,
-                                                    w.counter.p, S);
+                                                    w.counter.p, S); countLaunch();
                 if (sampled) sampleEnd(smp, s);
-                s_kernel<T><<<vg, BS, 0, s>>>(n, V.s, V.r, V.v, S);
+                s_kernel<T><<<vg, BS, 0, s>>>(n, V.s, V.r, V.v, S); countLaunch();
                 spmv_kernel<T, 2><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.s, V.t, V.s, w.partials.p,
-                                                    w.counter.p, S);
-                xr_kernel<T><<<vg, BS, 0, s>>>(n, V.x, V.r, V.p, V.s, V.t, V.r0, w.partials.p, w.counter.p, S);
+                                                    w.counter.p, S); countLaunch();
+                xr_kernel<T><<<vg, BS, 0, s>>>(n, V.x, V.r, V.p, V.s, V.t, V.r0, w.partials.p, w.counter.p, S); countLaunch();
             }
             PB_LAUNCH("bicgstab iteration");
             PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
@@ -475,9 +476,9 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
     w.ensure(A.nslices * 32, A.nnz_padded, mixed);
     const int n = A.n;
     const int gn = ceil_div(n, BS);
-    dinv_kernel<<<gn, BS, 0, s>>>(n, A.diag_pos, A.vals, w.dinv.p, x, w.xs.p);
+    dinv_kernel<<<gn, BS, 0, s>>>(n, A.diag_pos, A.vals, w.dinv.p, x, w.xs.p); countLaunch();
     int sgrid = std::min<int64_t>((A.nnz_padded + BS - 1) / BS, NUM_SMS * 32);
-    scale_kernel<double><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As.p);
+    scale_kernel<double><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As.p); countLaunch();
     PB_LAUNCH("bicgstab scaling");
     KrylovOut out;
     if (!mixed) {
@@ -488,11 +489,11 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
             out.iterations += o.iterations;
             out.status = o.status;
             maxit -= o.iterations;
-            unscale_kernel<<<gn, BS, 0, s>>>(n, w.dinv.p, w.xs.p, x);
+            unscale_kernel<<<gn, BS, 0, s>>>(n, w.dinv.p, w.xs.p, x); countLaunch();
             spmv(A, x, w.tmp.p, s);
             double rb[2];
             refine_residual_kernel<<<vecGrid(n), BS, 0, s>>>(n, w.tmp.p, b, reinterpret_cast<float*>(w.s.p),
-                                                             w.partials.p, w.counter.p, w.scal.p);
+                                                             w.partials.p, w.counter.p, w.scal.p); countLaunch();
             PB_CUDA(cudaMemcpyAsync(rb, w.scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
             PB_CUDA(cudaStreamSynchronize(s));
             out.rel_residual = rb[1] > 0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
@@ -501,14 +502,14 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
         return out;
     }
     // mixed precision: FP32 inner BiCGSTAB on A D^-1, FP64 refinement on A
-    scale_kernel<float><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As32.p);
+    scale_kernel<float><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As32.p); countLaunch();
     PB_LAUNCH("bicgstab fp32 copy");
     Vecs<float> V{w.x32.p, w.r32.p, w.r032.p, w.p32.p, w.v32.p, w.s32.p, w.t32.p};
     float* rhs32 = reinterpret_cast<float*>(w.tmp.p);  // FP32 right-hand side of the correction
     double rb[2];
     for (int outer = 0; outer < 60; ++outer) {
         spmv(A, x, w.r.p, s);
-        refine_residual_kernel<<<vecGrid(n), BS, 0, s>>>(n, w.r.p, b, rhs32, w.partials.p, w.counter.p, w.scal.p);
+        refine_residual_kernel<<<vecGrid(n), BS, 0, s>>>(n, w.r.p, b, rhs32, w.partials.p, w.counter.p, w.scal.p); countLaunch();
         PB_CUDA(cudaMemcpyAsync(rb, w.scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
         PB_CUDA(cudaStreamSynchronize(s));
         if (!std::isfinite(rb[0]) || !std::isfinite(rb[1])) {
@@ -520,7 +521,7 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
             if (maxit <= 0 && rb[0] > tol * tol * rb[1]) out.status = PRISM_NOT_CONVERGED;
             break;
         }
-        fill_zero_f<<<gn, BS, 0, s>>>(n, w.x32.p);
+        fill_zero_f<<<gn, BS, 0, s>>>(n, w.x32.p); countLaunch();
         KrylovOut o = runBicgstab<float>(A, w.As32.p, rhs32, V, true, inner_tol, maxit, w, s);
         out.iterations += o.iterations;
         maxit -= o.iterations;
@@ -528,7 +529,7 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
             out.status = o.status;
             break;
         }
-        correct_kernel<<<gn, BS, 0, s>>>(n, x, w.dinv.p, w.x32.p);
+        correct_kernel<<<gn, BS, 0, s>>>(n, x, w.dinv.p, w.x32.p); countLaunch();
         PB_LAUNCH("refinement correction");
     }
     return out;
@@ -541,12 +542,14 @@ void profileStart(int max_samples) {
     }
     g_prof.samples.clear();
     g_prof.max_samples = max_samples > 0 ? max_samples : 4096;
+    g_prof.launches0 = launchCounter().load();
     g_prof.on = true;
 }
 
 void profileStop(PrismProfile* out) {
     std::memset(out, 0, sizeof(*out));
     g_prof.on = false;
+    out->kernel_launches = launchCounter().load() - g_prof.launches0;
     for (auto& smp : g_prof.samples) {
         PB_CUDA(cudaEventSynchronize(smp.b));
         float ms = 0.f;
@@ -566,21 +569,21 @@ void profileStop(PrismProfile* out) {
 void jacobiStep(const SellMatrix& A, const double* b, double* x, KrylovWork& w, cudaStream_t s) {
     w.ensure(A.nslices * 32, A.nnz_padded, false);
     jacobi_kernel<<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x,
-                                                      w.tmp.p);
+                                                      w.tmp.p); countLaunch();
     PB_LAUNCH("jacobi_kernel");
     PB_CUDA(cudaMemcpyAsync(x, w.tmp.p, A.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
 }
 
 void explicitUpdate(const SellMatrix& A, const double* b, const double* x, double* xnew, cudaStream_t s) {
     explicit_kernel<<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x,
-                                                        xnew);
+                                                        xnew); countLaunch();
     PB_LAUNCH("explicit_kernel");
 }
 
 double scaledResidual(const SellMatrix& A, const double* b, const double* x, KrylovWork& w, cudaStream_t s) {
     w.ensure(A.nslices * 32, A.nnz_padded, false);
     resid_kernel<<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x,
-                                                     w.partials.p, w.counter.p, w.scal.p);
+                                                     w.partials.p, w.counter.p, w.scal.p); countLaunch();
     PB_LAUNCH("resid_kernel");
     double h[3];
     PB_CUDA(cudaMemcpyAsync(h, w.scal.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -133,8 +133,8 @@ void buildPattern(const PatternInput& in, PatternOutput& out, cudaStream_t s) {
     PB_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
     PB_CUDA(cudaMemsetAsync(rowlen.p + nc, 0, sizeof(int), s));
     PB_CUDA(cudaMemsetAsync(slice_entries.p + nslices, 0, sizeof(int), s));
-    row_kernel<<<ceil_div(nc, 256), 256, 0, s>>>(nc, in.cf_off, in.cf_face, in.owner, in.nbr, in.nb, rowlen.p, bad.p);
-    slice_kernel<<<ceil_div(nslices, 256), 256, 0, s>>>(nc, nslices, rowlen.p, slice_entries.p);
+    row_kernel<<<ceil_div(nc, 256), 256, 0, s>>>(nc, in.cf_off, in.cf_face, in.owner, in.nbr, in.nb, rowlen.p, bad.p); countLaunch();
+    slice_kernel<<<ceil_div(nslices, 256), 256, 0, s>>>(nc, nslices, rowlen.p, slice_entries.p); countLaunch();
     PB_LAUNCH("pattern row/slice kernels");
     out.rowptr.alloc(nc + 1);
     out.sl_off.alloc(nslices + 1);
@@ -161,7 +161,7 @@ void buildPattern(const PatternInput& in, PatternOutput& out, cudaStream_t s) {
     out.ca_pos.alloc(in.ncf);
     fill_kernel<<<ceil_div((int64_t)nslices * 32, 256), 256, 0, s>>>(
         nc, nslices, in.cf_off, in.cf_face, in.owner, in.nbr, in.nb, in.npatch, in.bpatch, in.ppos, out.rowptr.p,
-        out.sl_off.p, out.col.p, out.sl_col.p, out.diag_pos.p, out.ca_face.p, out.ca_pos.p);
+        out.sl_off.p, out.col.p, out.sl_col.p, out.diag_pos.p, out.ca_face.p, out.ca_pos.p); countLaunch();
     PB_LAUNCH("pattern fill_kernel");
     PB_CUDA(cudaStreamSynchronize(s));
 }
