@@ -344,6 +344,33 @@ typedef struct {
 int prism_profile_start(int32_t max_samples);
 int prism_profile_stop(PrismProfile* out);
 
+/* ---- allocation-free Jacobi sweep ------------------------------------------ */
+/* For callers that cannot allocate device memory when they need a solver step
+ * (work recorded into a CUDA graph, where allocating during stream capture is an
+ * error; host applications that own a fixed device-memory budget; time loops
+ * that must not synchronize on cudaMalloc/cudaFree). No counterpart in the
+ * reference.
+ *
+ * One Jacobi sweep x <- x + D^-1 (b - A x) on an n x n CSR matrix whose arrays
+ * the caller already holds in device memory: rowptr (n+1) and col (nnz) int32,
+ * values (nnz), b and x (n) FP64; all are device pointers and x is updated in
+ * place. The work is enqueued on `stream` (a cudaStream_t; NULL = the default
+ * stream) and the call returns without waiting for it.
+ *
+ * Nothing is allocated: the out-of-place sweep uses a fixed scratch vector of
+ * PRISM_NOALLOC_MAX_ROWS doubles (8 MiB) that every GPU loading the library
+ * holds until the process exits; n above that limit is rejected with
+ * PRISM_BAD_ARG. The first call on a device, with that device current, looks up
+ * the scratch's device address (cudaGetSymbolAddress): make that first call
+ * before any stream capture. All calls share the one scratch vector, so calls
+ * whose work overlaps on the GPU (different streams, or different host threads)
+ * race; serialize them. Every scratch entry a call reads is written earlier in
+ * the same call, so nothing has to be cleared between calls. A row without a
+ * diagonal entry yields NaN. */
+#define PRISM_NOALLOC_MAX_ROWS 1048576
+int prism_jacobi_step_noalloc(int64_t n, const int32_t* rowptr, const int32_t* col, const double* values,
+                              const double* b, double* x, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -157,6 +157,7 @@ SIGNATURES = {
     "needs_pressure_reference": (C.c_int, [P, pi32]),
     "profile_start": (C.c_int, [i32]),
     "profile_stop": (C.c_int, [C.POINTER(Profile)]),
+    "jacobi_step_noalloc": (C.c_int, [i64, P, P, P, P, P, P]),
 }
 
 
@@ -169,7 +170,7 @@ class PrismError(RuntimeError):
         self.status = status
 
 
-GPU_ONLY = {"profile_start", "profile_stop"}
+GPU_ONLY = {"profile_start", "profile_stop", "jacobi_step_noalloc"}
 
 
 class Bound:

@@ -717,3 +717,9 @@ API int prism_profile_stop(PrismProfile* out) {
         profileStop(out);
     });
 }
+
+// ---- allocation-free Jacobi sweep (see include/prism_b200.h)
+API int prism_jacobi_step_noalloc(int64_t n, const int32_t* rowptr, const int32_t* col, const double* values,
+                                  const double* b, double* x, void* stream) {
+    return guard([&] { jacobiStepNoAlloc(n, rowptr, col, values, b, x, static_cast<cudaStream_t>(stream)); });
+}

@@ -16,6 +16,10 @@ struct SellMatrix {
     int64_t nnz_csr = 0;  // structural entries (for algorithmic byte counts)
 };
 
+// prism_jacobi_step_noalloc: Jacobi sweep on a device CSR matrix using only static scratch
+void jacobiStepNoAlloc(int64_t n, const int32_t* rowptr, const int32_t* col, const double* values, const double* b,
+                       double* x, cudaStream_t stream);
+
 // Sampled CUDA-event timing of the BiCGSTAB SpMV launches (v = A p).
 void profileStart(int max_samples);
 void profileStop(PrismProfile* out);
