@@ -205,7 +205,7 @@ def transport_time_to_tol(mesh, precision, ref, tol=1e-8):
     last = None
     for e in np.arange(8.0, 14.01, 0.5):
         ktol = 10.0 ** (-e)
-        solver = api.BiCGSTAB(precision=precision, krylov_tol=ktol, krylov_max_iter=100000, inner_tol=1e-4)
+        solver = api.BiCGSTAB(precision=precision, krylov_tol=ktol, krylov_max_iter=100000)
         for rep in range(2):
             T, keep, eqn = transport_eqn(mesh)
             torch.cuda.synchronize()

@@ -251,7 +251,7 @@ typedef struct {
     int32_t clear_coeffs;
     double krylov_tol;      /* BiCGSTAB step: stop at ||b-Ax||/||b|| <= krylov_tol (0: default 1e-12) */
     int64_t krylov_max_iter; /* 0: default 2*n_cells */
-    double inner_tol;        /* mixed precision: FP32 inner relative tolerance (0: default 1e-4) */
+    double inner_tol;        /* mixed precision: residual reduction between FP64 reliable updates (0: default 0.1) */
 } PrismSolveOpts;
 
 typedef struct {

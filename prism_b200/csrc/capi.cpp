@@ -641,7 +641,7 @@ API int prism_solve_csr(int64_t n, const int64_t* rowptr, const int64_t* col, co
         } else {
             k = bicgstab(A, d_b.p, d_x.p, o->krylov_tol > 0 ? o->krylov_tol : 1e-12,
                          o->krylov_max_iter > 0 ? o->krylov_max_iter : 2 * n, o->precision,
-                         o->inner_tol > 0 ? o->inner_tol : 1e-4, kw, s);
+                         o->inner_tol > 0 ? o->inner_tol : 0.1, kw, s);
         }
         double res = scaledResidual(A, d_b.p, d_x.p, kw, s);
         d_x.download(x, n, s);

@@ -17,8 +17,13 @@
 // iterations and reads the state once per batch; kernels after convergence
 // return immediately, so a batch never changes a converged result.
 //
-// Mixed precision: FP32 matrix/vectors in the inner BiCGSTAB (dot products
-// accumulated in FP64) inside FP64 iterative refinement on the true residual.
+// Mixed precision: the same BiCGSTAB with an FP32 copy of A' and FP32 vectors
+// (dot products accumulated in FP64), with reliable updates (Sleijpen and van
+// der Vorst 1996): the solution correction is accumulated in FP32 and flushed
+// into the FP64 solution whenever the iterated residual has dropped by a factor
+// delta (default 0.1) since the last flush; the FP64 true residual b - A'x' then
+// replaces the FP32 one and the recurrences continue with the Krylov space kept.
+// Convergence is only declared on an FP64 true residual.
 #include <cmath>
 #include <cstring>
 
@@ -91,9 +96,37 @@ __device__ bool reduceLast(double (&v)[NV], double* partials, unsigned int* coun
 
 inline int vecGrid(int n) { return std::max(1, std::min(ceil_div(n, BS), MAX_GRID)); }
 inline int spmvGrid(int nslices) { return std::max(1, std::min(ceil_div(nslices, WARPS), NUM_SMS * 16)); }
+inline int sliceGrid(int nslices) { return std::max(1, std::min(ceil_div(nslices, WARPS), NUM_SMS * 16)); }
 
-// y = A x for a SELL-32 matrix; one warp per 32-row slice, coalesced loads.
+// y = A x for a SELL-32 matrix: a warp walks 32-row slices (one row per lane),
+// coalesced loads. For slices up to 8 entries wide every column index and value
+// of the slice is loaded before the x gathers, so a warp keeps 16 independent
+// loads in flight instead of a chain of dependent pairs; the matrix is read with
+// evict-first (streaming) loads so that L2 keeps the gathered x.
 // STAGE 0: plain; 1: alpha = rho / (u.y); 2: w = (u.y)/(y.y)
+template <typename T>
+__device__ __forceinline__ T sliceRow(const int* __restrict__ col, const T* __restrict__ val,
+                                      const T* __restrict__ x, int b, int width, int lane) {
+    T sum = 0;
+    if (width <= 8) {
+        int c[8];
+        T v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (j < width) {
+                c[j] = __ldcs(col + b + 32 * j + lane);
+                v[j] = __ldcs(val + b + 32 * j + lane);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j < width) sum += v[j] * x[c[j]];
+    } else {
+        for (int j = 0; j < width; ++j) sum += __ldcs(val + b + 32 * j + lane) * x[__ldcs(col + b + 32 * j + lane)];
+    }
+    return sum;
+}
+
 template <typename T, int STAGE>
 __global__ void __launch_bounds__(BS) spmv_kernel(int nslices, int n, const int* __restrict__ sl_off,
                                                   const int* __restrict__ col, const T* __restrict__ val,
@@ -106,10 +139,7 @@ __global__ void __launch_bounds__(BS) spmv_kernel(int nslices, int n, const int*
     for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
         const int b = sl_off[sl];
         const int width = (sl_off[sl + 1] - b) >> 5;
-        const int* cp = col + b + lane;
-        const T* vp = val + b + lane;
-        T sum = 0;
-        for (int j = 0; j < width; ++j) sum += vp[32 * j] * x[cp[32 * j]];
+        const T sum = sliceRow<T>(col, val, x, b, width, lane);
         const int r = sl * 32 + lane;
         y[r] = sum;
         if (STAGE != 0 && r < n) {
@@ -171,6 +201,7 @@ __global__ void __launch_bounds__(BS) xr_kernel(int n, T* __restrict__ x, T* __r
         S->iter += 1;
         const double rho_new = out[0];
         if (!isfinite(out[0]) || !isfinite(out[1])) S->done = 5;
+        else if (S->reliable && (out[1] <= S->tol2 || out[1] < S->delta2 * S->rr_update)) S->done = 6;
         else if (out[1] <= S->tol2) S->done = 1;
         else if (S->iter >= S->maxit) S->done = 2;
         else if (w == 0.0 || fabs(rho_new) < EPSILON * EPSILON * S->r0sq) S->done = 3;
@@ -250,13 +281,71 @@ __global__ void __launch_bounds__(BS) refine_residual_kernel(int n, const double
         out2[1] = out[1];
     }
 }
-__global__ void correct_kernel(int n, double* x, const double* dinv, const float* d32) {
-    int i = blockIdx.x * BS + threadIdx.x;
-    if (i < n) x[i] += dinv[i] * (double)d32[i];
-}
 __global__ void fill_zero_f(int n, float* x) {
     int i = blockIdx.x * BS + threadIdx.x;
     if (i < n) x[i] = 0.0f;
+}
+
+// Reliable update, part 1: xs += y (FP32 correction flushed into the FP64 solution), y = 0.
+__global__ void flush_kernel(int n, double* __restrict__ xs, float* __restrict__ y) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) {
+        xs[i] += (double)y[i];
+        y[i] = 0.0f;
+    }
+}
+// Reliable update, part 2 (Ax = A' xs already in `ax`): r64 = b - ax, r32 = (float) r64,
+// rr = r64.r64, rho = r0.r32; continue the recurrence or declare convergence.
+// first != 0: (re)start -- r0 = r32, p = v = 0, fresh recurrence scalars.
+__global__ void __launch_bounds__(BS) reliable_kernel(int n, const double* __restrict__ ax, const double* __restrict__ b,
+                                                      double* __restrict__ r64, float* __restrict__ r32,
+                                                      float* __restrict__ r032, float* __restrict__ p32,
+                                                      float* __restrict__ v32, int first, double tol,
+                                                      double* partials, unsigned int* counter, KState* S) {
+    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS) {
+        double ri = b[i] - ax[i];
+        float rf = (float)ri;
+        r64[i] = ri;
+        r32[i] = rf;
+        if (first) {
+            r032[i] = rf;
+            p32[i] = 0.0f;
+            v32[i] = 0.0f;
+        }
+        d0 += ri * ri;
+        d1 += (double)(first ? rf : r032[i]) * (double)rf;
+        d2 += b[i] * b[i];
+    }
+    double v[3] = {d0, d1, d2}, out[3];
+    if (reduceLast<3, false>(v, partials, counter, out) && threadIdx.x == 0) {
+        S->rr = out[0];
+        S->rr_update = out[0];
+        if (first) {
+            S->bb = out[2];
+            S->tol2 = tol * tol * out[2];
+            S->r0sq = out[1];
+            S->rho = out[1];
+            S->beta = out[1];
+            S->alpha = 1.0;
+            S->w = 1.0;
+        }
+        if (!isfinite(out[0]) || !isfinite(out[1])) S->done = 5;
+        else if (out[2] == 0.0) S->done = 4;
+        else if (out[0] <= S->tol2) S->done = 1;
+        else if (S->iter >= S->maxit) S->done = 2;
+        else {
+            if (!first) {
+                if (S->w == 0.0 || fabs(out[1]) < EPSILON * EPSILON * S->r0sq) {
+                    S->done = 3;
+                    return;
+                }
+                S->beta = (out[1] / S->rho) * (S->alpha / S->w);
+                S->rho = out[1];
+            }
+            S->done = 0;
+        }
+    }
 }
 
 // Jacobi: out = x + dinv (b - A x)
@@ -334,7 +423,7 @@ void KrylovWork::ensure(int n_pad, int64_t nnz_padded, bool mixed) {
         nnz = nnz_padded;
         for (auto* b : {&r, &r0, &p, &v, &s, &t, &xs, &dinv, &tmp}) b->alloc(n_pad);
         As.alloc(nnz_padded);
-        partials.alloc(NUM_SMS * 16 * 4);
+        partials.alloc((size_t)std::max(sliceGrid(n_pad / 32), NUM_SMS * 16) * 4);
         counter.alloc(1);
         PB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned int)));
         scal.alloc(8);
@@ -346,6 +435,8 @@ void KrylovWork::ensure(int n_pad, int64_t nnz_padded, bool mixed) {
     }
     if (mixed && !As32) {
         As32.alloc(nnz_padded);
+        r64.alloc(n_pad);
+        PB_CUDA(cudaMemset(r64.p, 0, n_pad * sizeof(double)));
         for (auto* b : {&r32, &r032, &p32, &v32, &s32, &t32, &x32}) {
             b->alloc(n_pad);
             PB_CUDA(cudaMemset(b->p, 0, n_pad * sizeof(float)));
@@ -357,7 +448,7 @@ KrylovWork::~KrylovWork() {
 }
 
 void spmv(const SellMatrix& A, const double* x, double* y, cudaStream_t s) {
-    spmv_kernel<double, 0><<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, x, y, nullptr,
+    spmv_kernel<double, 0><<<sliceGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, x, y, nullptr,
                                                               nullptr, nullptr, nullptr); countLaunch();
     PB_LAUNCH("spmv_kernel");
 }
@@ -421,7 +512,7 @@ KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, 
     KState init{};
     init.maxit = maxit;
     PB_CUDA(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, s));
-    const int n = A.n, vg = vecGrid(n), sg = spmvGrid(A.nslices);
+    const int n = A.n, vg = vecGrid(n), sg = sliceGrid(A.nslices);
     int restarts = 0;
     bool zero = from_zero;
     long long batch = 8;
@@ -486,6 +577,7 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
         // accurate-residual restarts: the recursive residual drifts from b - A x
         for (int pass = 0; pass < 4; ++pass) {
             KrylovOut o = runBicgstab<double>(A, w.As.p, b, V, false, tol, maxit, w, s);
+            if (w.host_state->done == 4) PB_CUDA(cudaMemsetAsync(w.xs.p, 0, n * sizeof(double), s));  // b = 0: x = 0
             out.iterations += o.iterations;
             out.status = o.status;
             maxit -= o.iterations;
@@ -501,37 +593,80 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
         }
         return out;
     }
-    // mixed precision: FP32 inner BiCGSTAB on A D^-1, FP64 refinement on A
+    // mixed precision: FP32 BiCGSTAB on A' with FP64 reliable updates of x' and r
     scale_kernel<float><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As32.p); countLaunch();
     PB_LAUNCH("bicgstab fp32 copy");
-    Vecs<float> V{w.x32.p, w.r32.p, w.r032.p, w.p32.p, w.v32.p, w.s32.p, w.t32.p};
-    float* rhs32 = reinterpret_cast<float*>(w.tmp.p);  // FP32 right-hand side of the correction
-    double rb[2];
-    for (int outer = 0; outer < 60; ++outer) {
-        spmv(A, x, w.r.p, s);
-        refine_residual_kernel<<<vecGrid(n), BS, 0, s>>>(n, w.r.p, b, rhs32, w.partials.p, w.counter.p, w.scal.p); countLaunch();
-        PB_CUDA(cudaMemcpyAsync(rb, w.scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    const double delta = (inner_tol > 0.0 && inner_tol < 1.0) ? inner_tol : 0.1;
+    KState* S = w.state.p;
+    KState init{};
+    init.maxit = maxit;
+    init.reliable = 1;
+    init.delta2 = delta * delta;
+    PB_CUDA(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, s));
+    SellMatrix As = A;
+    As.vals = w.As.p;
+    const int vg = vecGrid(n), sg = sliceGrid(A.nslices);
+    auto reliable = [&](int first) {
+        if (!first) {
+            flush_kernel<<<gn, BS, 0, s>>>(n, w.xs.p, w.x32.p); countLaunch();
+        }
+        spmv(As, w.xs.p, w.tmp.p, s);
+        reliable_kernel<<<vg, BS, 0, s>>>(n, w.tmp.p, b, w.r64.p, w.r32.p, w.r032.p, w.p32.p, w.v32.p, first, tol,
+                                          w.partials.p, w.counter.p, S); countLaunch();
+        PB_LAUNCH("reliable update");
+        PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
         PB_CUDA(cudaStreamSynchronize(s));
-        if (!std::isfinite(rb[0]) || !std::isfinite(rb[1])) {
-            out.status = PRISM_NONFINITE;
-            break;
+        return w.host_state->done;
+    };
+    fill_zero_f<<<gn, BS, 0, s>>>(n, w.x32.p); countLaunch();
+    int done = reliable(1);
+    int restarts = 0;
+    long long batch = 8;
+    while (done == 0) {
+        for (long long it = 0; it < batch; ++it) {
+            p_kernel<float><<<vg, BS, 0, s>>>(n, w.p32.p, w.r32.p, w.v32.p, S); countLaunch();
+            Sample smp;
+            bool sampled = sampleBegin<float>(smp, A, s);
+            spmv_kernel<float, 1><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, w.As32.p, w.p32.p, w.v32.p,
+                                                    w.r032.p, w.partials.p, w.counter.p, S); countLaunch();
+            if (sampled) sampleEnd(smp, s);
+            s_kernel<float><<<vg, BS, 0, s>>>(n, w.s32.p, w.r32.p, w.v32.p, S); countLaunch();
+            spmv_kernel<float, 2><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, w.As32.p, w.s32.p, w.t32.p,
+                                                    w.s32.p, w.partials.p, w.counter.p, S); countLaunch();
+            xr_kernel<float><<<vg, BS, 0, s>>>(n, w.x32.p, w.r32.p, w.p32.p, w.s32.p, w.t32.p, w.r032.p,
+                                               w.partials.p, w.counter.p, S); countLaunch();
         }
-        out.rel_residual = rb[1] > 0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
-        if (rb[1] == 0.0 || rb[0] <= tol * tol * rb[1] || maxit <= 0) {
-            if (maxit <= 0 && rb[0] > tol * tol * rb[1]) out.status = PRISM_NOT_CONVERGED;
-            break;
+        PB_LAUNCH("bicgstab fp32 iteration");
+        PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
+        PB_CUDA(cudaStreamSynchronize(s));
+        done = w.host_state->done;
+        if (done == 0) {
+            batch = std::min<long long>(batch * 2, 64);
+            continue;
         }
-        fill_zero_f<<<gn, BS, 0, s>>>(n, w.x32.p); countLaunch();
-        KrylovOut o = runBicgstab<float>(A, w.As32.p, rhs32, V, true, inner_tol, maxit, w, s);
-        out.iterations += o.iterations;
-        maxit -= o.iterations;
-        if (o.status == PRISM_NONFINITE) {
-            out.status = o.status;
-            break;
+        if (done == 6) {
+            done = reliable(0);
+            continue;
         }
-        correct_kernel<<<gn, BS, 0, s>>>(n, x, w.dinv.p, w.x32.p); countLaunch();
-        PB_LAUNCH("refinement correction");
+        if (done == 3) {  // breakdown of the recurrence: flush and restart from the current x
+            if (++restarts > 20) break;
+            flush_kernel<<<gn, BS, 0, s>>>(n, w.xs.p, w.x32.p); countLaunch();
+            done = reliable(1);
+            continue;
+        }
     }
+    if (done == 2 || done == 3 || done == 5) {
+        flush_kernel<<<gn, BS, 0, s>>>(n, w.xs.p, w.x32.p); countLaunch();
+    }
+    out.iterations = w.host_state->iter;
+    out.status = done == 1 || done == 4 ? PRISM_OK
+                 : done == 2           ? PRISM_NOT_CONVERGED
+                 : done == 5           ? PRISM_NONFINITE
+                                       : PRISM_BREAKDOWN;
+    out.rel_residual = w.host_state->bb > 0 ? std::sqrt(w.host_state->rr / w.host_state->bb) : 0.0;
+    if (done == 4) PB_CUDA(cudaMemsetAsync(w.xs.p, 0, n * sizeof(double), s));
+    unscale_kernel<<<gn, BS, 0, s>>>(n, w.dinv.p, w.xs.p, x); countLaunch();
+    PB_LAUNCH("bicgstab unscale");
     return out;
 }
 

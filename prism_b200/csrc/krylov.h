@@ -29,9 +29,11 @@ struct KState {
     double rho, alpha, w, beta;
     double rr, bb, tol2, r0sq;
     double ts, tt;
+    double rr_update, delta2;  // mixed precision: |r|^2 at the last reliable update, trigger factor^2
     long long iter, maxit;
-    int done;  // 0 running, 1 converged, 2 max iterations, 3 restart needed, 4 zero rhs, 5 non-finite
-    int nonfinite;
+    int done;  // 0 running, 1 converged, 2 max iterations, 3 restart needed, 4 zero rhs, 5 non-finite,
+               // 6 reliable update due (mixed precision)
+    int reliable;
 };
 
 // Workspace owned by a mesh, sized on first use.
@@ -41,6 +43,7 @@ struct KrylovWork {
     DevBuf<double> r, r0, p, v, s, t, xs, dinv, tmp;
     DevBuf<double> As;   // column-scaled matrix A D^-1
     DevBuf<float> As32, r32, r032, p32, v32, s32, t32, x32;
+    DevBuf<double> r64;  // mixed precision: FP64 true residual at reliable updates
     DevBuf<double> partials, scal;
     DevBuf<unsigned int> counter;
     DevBuf<KState> state;

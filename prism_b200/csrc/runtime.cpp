@@ -451,7 +451,7 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
     SellMatrix A = m.matrix(eq.A.p);
     const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
     const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
-    const double itol = o.inner_tol > 0 ? o.inner_tol : 1e-4;
+    const double itol = o.inner_tol > 0 ? o.inner_tol : 0.1;
     PrismSolveResult r{};
     r.status = PRISM_OK;
     double init_res = 0.0, cur = 0.0;

@@ -115,3 +115,18 @@ def test_piso_vs_oracle(gpu, orc):
         err = cases.rel_l2(out["gpu"][i], out["orc"][i])
         print(f"PISO cavity {k}: rel L2 vs oracle {err:.3e}")
         assert err < SOL_TOL
+
+
+@pytest.mark.parametrize("precision", [A.PREC_FP64, A.PREC_MIXED])
+def test_transport_linear_upwind_solve(gpu, orc, precision):
+    # the nonsymmetric C3-type system (jittered hexes, LinearUpwind + Corrected)
+    out = {}
+    for name, lib in (("gpu", gpu), ("orc", orc)):
+        mesh, T, U, eqn = cases.transport_c3(16, lib, conv="LinearUpwind")
+        solver = api.BiCGSTAB(precision=precision, krylov_tol=1e-12) if name == "gpu" else api.BiCGSTAB()
+        r = solver.solve(eqn, 1, 0.0)
+        out[name] = (T.values(), r)
+    err = cases.rel_l2(out["gpu"][0], out["orc"][0])
+    print(f"transport 16^3 precision={precision}: rel L2 vs oracle {err:.3e}, "
+          f"krylov it {out['gpu'][1].krylov_iterations}, status {out['gpu'][1].status}")
+    assert err < SOL_TOL
