@@ -190,11 +190,11 @@ def transport_exact(mesh):
     """x* of the system assembled at T = 0: FP64 BiCGSTAB to ||b - Ax|| <= 1e-14 ||b||."""
     from prism_b200 import api
     T, keep, eqn = transport_eqn(mesh)
-    api.BiCGSTAB(krylov_tol=1e-14, krylov_max_iter=100000).solve(eqn, 1, 0.0)
+    api.BiCGSTAB(krylov_tol=1e-14, krylov_max_iter=100000, preconditioner="jacobi").solve(eqn, 1, 0.0)
     return T.values()
 
 
-def transport_time_to_tol(mesh, precision, ref, tol=1e-8):
+def transport_time_to_tol(mesh, precision, ref, tol=1e-8, preconditioner="auto"):
     """Seconds (CUDA events) for one solve() step from T = 0 (assembly included) to reach
     ||T - x*|| / ||x*|| <= tol: the loosest Krylov tolerance of a 10^-0.5 ladder that meets
     the error is timed (second of two identical runs)."""
@@ -205,7 +205,8 @@ def transport_time_to_tol(mesh, precision, ref, tol=1e-8):
     last = None
     for e in np.arange(8.0, 14.01, 0.5):
         ktol = 10.0 ** (-e)
-        solver = api.BiCGSTAB(precision=precision, krylov_tol=ktol, krylov_max_iter=100000)
+        solver = api.BiCGSTAB(precision=precision, krylov_tol=ktol, krylov_max_iter=100000,
+                              preconditioner=preconditioner)
         for rep in range(2):
             T, keep, eqn = transport_eqn(mesh)
             torch.cuda.synchronize()

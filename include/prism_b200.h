@@ -109,7 +109,12 @@ extern "C" {
 #define PRISM_SOLVER_JACOBI 1
 
 #define PRISM_PREC_FP64 0  /* FP64 Krylov */
-#define PRISM_PREC_MIXED 1 /* FP32 inner BiCGSTAB (FP64 dots) in FP64 iterative refinement */
+#define PRISM_PREC_MIXED 1 /* FP32 BiCGSTAB (FP64 dots) with FP64 reliable updates */
+
+#define PRISM_PC_AUTO 0   /* library choice: AMG from PRISM_PC_AUTO_MIN_ROWS rows, Jacobi below */
+#define PRISM_PC_JACOBI 1 /* diagonal (column scaling), the cheapest iteration */
+#define PRISM_PC_AMG 2    /* aggregation AMG V-cycle; hierarchy kept per equation, values refreshed per solve */
+#define PRISM_PC_AUTO_MIN_ROWS 32768
 
 /* ---- handles ------------------------------------------------------------ */
 typedef struct PrismMesh PrismMesh;
@@ -252,6 +257,7 @@ typedef struct {
     double krylov_tol;      /* BiCGSTAB step: stop at ||b-Ax||/||b|| <= krylov_tol (0: default 1e-12) */
     int64_t krylov_max_iter; /* 0: default 2*n_cells */
     double inner_tol;        /* mixed precision: residual reduction between FP64 reliable updates (0: default 0.1) */
+    int32_t preconditioner;  /* PRISM_PC_* (BiCGSTAB only) */
 } PrismSolveOpts;
 
 typedef struct {

@@ -29,6 +29,9 @@ SRC_CONSTANT, SRC_DIVERGENCE, SRC_GRADIENT = 0, 1, 2
 SIGN_POSITIVE, SIGN_NEGATIVE = 0, 1
 SOLVER_BICGSTAB, SOLVER_JACOBI = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+PC_AUTO, PC_JACOBI, PC_AMG = 0, 1, 2
+PC_AUTO_MIN_ROWS = 32768
+PRECONDITIONERS = {"auto": PC_AUTO, "jacobi": PC_JACOBI, "amg": PC_AMG}
 
 STATUS_NAMES = {
     0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "NONFINITE", 4: "BAD_ARG", 5: "CUDA_ERROR",
@@ -70,7 +73,8 @@ class BC(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("method", i32), ("precision", i32), ("n_iter", i64), ("eps", f64),
                 ("ref_cell", i64), ("ref_value", f64), ("clear_coeffs", i32),
-                ("krylov_tol", f64), ("krylov_max_iter", i64), ("inner_tol", f64)]
+                ("krylov_tol", f64), ("krylov_max_iter", i64), ("inner_tol", f64),
+                ("preconditioner", i32)]
 
 
 class SolveResult(C.Structure):

@@ -379,7 +379,7 @@ class SolverResult:
 
 
 def _solve_opts(lib, method, precision, n_iter, eps, ref_cell, ref_value, clear, krylov_tol,
-                krylov_max_iter, inner_tol):
+                krylov_max_iter, inner_tol, preconditioner=A.PC_AUTO):
     o = A.SolveOpts()
     lib.solve_opts_default(C.byref(o))
     o.method, o.precision, o.n_iter, o.eps = method, precision, n_iter, eps
@@ -391,19 +391,25 @@ def _solve_opts(lib, method, precision, n_iter, eps, ref_cell, ref_value, clear,
         o.krylov_max_iter = krylov_max_iter
     if inner_tol:
         o.inner_tol = inner_tol
+    o.preconditioner = preconditioner
     return o
 
 
 class _Solver:
     method = A.SOLVER_BICGSTAB
 
-    def __init__(self, precision=A.PREC_FP64, krylov_tol=0.0, krylov_max_iter=0, inner_tol=0.0):
+    def __init__(self, precision=A.PREC_FP64, krylov_tol=0.0, krylov_max_iter=0, inner_tol=0.0,
+                 preconditioner="auto"):
         self.precision, self.krylov_tol = precision, krylov_tol
         self.krylov_max_iter, self.inner_tol = krylov_max_iter, inner_tol
+        if isinstance(preconditioner, str):
+            preconditioner = A.PRECONDITIONERS[preconditioner]
+        self.preconditioner = preconditioner
 
     def opts(self, lib, n_iter=10, eps=1e-7, ref_cell=None, ref_value=0.0, clear_coeffs=True):
         return _solve_opts(lib, self.method, self.precision, n_iter, eps, ref_cell, ref_value,
-                           clear_coeffs, self.krylov_tol, self.krylov_max_iter, self.inner_tol)
+                           clear_coeffs, self.krylov_tol, self.krylov_max_iter, self.inner_tol,
+                           self.preconditioner)
 
     def solve(self, eqn: Transport, n_iter=10, eps=1e-7, ref_cell=None, ref_value=0.0,
               clear_coeffs=True) -> SolverResult:

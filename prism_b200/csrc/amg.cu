@@ -1,0 +1,777 @@
+// amg.cu -- aggregation algebraic multigrid, used as the BiCGSTAB preconditioner.
+//
+// The reference preconditions every BiCGSTAB step with Eigen's IncompleteLUT
+// (numerics/bicgstab.h:12). A strong preconditioner is what keeps the
+// iteration count of the pressure-correction and transport solves small; on a
+// GPU the parallel equivalent is algebraic multigrid:
+//   * coarsening: double pairwise aggregation (two matching passes per level,
+//     ~5x fewer rows per level). Each pass is a handshake matching on the
+//     strong edges (w_ij = (|a_ij|+|a_ji|)/sqrt(|a_ii a_jj|) >= 0.5 of the best
+//     edge of both rows), taking for every row its strong edge of highest
+//     symmetric hash priority; an edge chosen by both ends is matched. After
+//     ten rounds an unmatched row joins the aggregate of its strongest matched
+//     strong neighbour, or stays single. Deterministic (no atomics, no races).
+//   * prolongation: piecewise constant; Galerkin coarse operator A_c = P^T A P
+//     built by sorting the fine entries by (aggregate row, aggregate column)
+//     once, after which refreshing the values for a new matrix is one
+//     segmented sum per coarse entry in a fixed order;
+//   * cycle: V(1,1), damped Jacobi (omega = 0.67) smoothing, coarse correction
+//     scaled by 1.5 (unsmoothed aggregation under-corrects), dense inverse
+//     (single-block Gauss-Jordan with partial pivoting) on the coarsest level.
+// The hierarchy's structure is built once per matrix pattern and reused; every
+// solve refreshes the values from the current matrix.
+#include <cub/cub.cuh>
+
+#include <chrono>
+#include <cmath>
+
+#include "amg.h"
+
+namespace pb {
+
+namespace {
+
+constexpr int BS = 256;
+constexpr int WARPS = BS / 32;
+constexpr int COARSE_MAX = 128;   // stop coarsening at this many rows
+constexpr int DENSE_MAX = 160;    // dense inverse of the coarsest level up to this many rows (fits shared memory)
+constexpr int MAX_LEVELS = 20;
+constexpr int MATCH_ROUNDS = 10;
+
+inline int grid(int64_t n) { return std::max(1, ceil_div(n, BS)); }
+inline int sgrid(int nslices) { return std::max(1, std::min(ceil_div(nslices, WARPS), NUM_SMS * 16)); }
+
+__device__ __forceinline__ unsigned long long edgeHash(int i, int j) {
+    unsigned long long a = (unsigned long long)min(i, j), b = (unsigned long long)max(i, j);
+    unsigned long long h = (a * 0x9E3779B97F4A7C15ull) ^ (b + 0x632BE59BD9B4E019ull);
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    return h;
+}
+
+// ---------------------------------------------------------------- setup kernels
+__global__ void weights_kernel(int n, const int* rowptr, const int* col, const int* csr_pos, const int* diag_pos,
+                               const double* vals, double* w, double* wmax) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i >= n) return;
+    double aii = fabs(vals[diag_pos[i]]);
+    double best = 0.0;
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+        int j = col[k];
+        if (j == i) {
+            w[k] = 0.0;
+            continue;
+        }
+        double aij = fabs(vals[csr_pos[k]]), aji = 0.0;
+        for (int q = rowptr[j]; q < rowptr[j + 1]; ++q)
+            if (col[q] == i) aji = fabs(vals[csr_pos[q]]);
+        double ajj = fabs(vals[diag_pos[j]]);
+        double d = aii * ajj;
+        double wk = d > 0.0 ? (aij + aji) / sqrt(d) : (aij + aji);
+        w[k] = wk;
+        best = fmax(best, wk);
+    }
+    wmax[i] = best;
+}
+
+__global__ void propose_kernel(int n, const int* rowptr, const int* col, const double* w, const double* wmax,
+                               const int* label, int* cand) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i >= n) return;
+    if (label[i] >= 0) {
+        cand[i] = -1;
+        return;
+    }
+    int best = -1;
+    unsigned long long bp = 0;
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+        int j = col[k];
+        if (j == i || label[j] >= 0) continue;
+        double wk = w[k];
+        if (!(wk > 0.0) || wk < 0.5 * wmax[i] || wk < 0.5 * wmax[j]) continue;
+        unsigned long long h = edgeHash(i, j);
+        if (best < 0 || h > bp || (h == bp && j < best)) {
+            best = j;
+            bp = h;
+        }
+    }
+    cand[i] = best;
+}
+
+__global__ void accept_kernel(int n, const int* cand, int* label) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i >= n) return;
+    int j = cand[i];
+    if (j >= 0 && cand[j] == i) label[i] = min(i, j);
+}
+
+// After the handshake rounds: an unmatched row joins the aggregate of its
+// strongest matched strong neighbour (ties: lower index), else stays single.
+// Reads the round labels, writes the final ones (no order dependence).
+__global__ void finish_label_kernel(int n, const int* rowptr, const int* col, const double* w, const double* wmax,
+                                    const int* label, int* out, int* root) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i >= n) return;
+    int l = label[i];
+    if (l < 0) {
+        int best = -1;
+        double bw = 0.0;
+        for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            int j = col[k];
+            if (j == i || label[j] < 0) continue;
+            double wk = w[k];
+            if (!(wk > 0.0) || wk < 0.5 * wmax[i] || wk < 0.5 * wmax[j]) continue;
+            if (best < 0 || wk > bw || (wk == bw && j < best)) {
+                best = j;
+                bw = wk;
+            }
+        }
+        l = best >= 0 ? label[best] : i;
+    }
+    out[i] = l;
+    root[i] = (l == i) ? 1 : 0;
+}
+
+__global__ void agg_kernel(int n, const int* label, const int* rootid, int* agg) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) agg[i] = rootid[label[i]];
+}
+
+__global__ void compose_kernel(int n, const int* agg1, const int* agg2, int* agg) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) agg[i] = agg2[agg1[i]];
+}
+
+__global__ void keys_kernel(int n, const int* rowptr, const int* col, const int* agg, long long nc, long long* keys,
+                            int* idx) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i >= n) return;
+    long long ai = agg[i];
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+        keys[k] = ai * nc + agg[col[k]];
+        idx[k] = k;
+    }
+}
+
+__global__ void heads_kernel(int64_t m, const long long* keys, int* head) {
+    int64_t q = blockIdx.x * (int64_t)BS + threadIdx.x;
+    if (q < m) head[q] = (q == 0 || keys[q] != keys[q - 1]) ? 1 : 0;
+}
+
+// coarse CSR from sorted keys: seg start, column, row starts; src = fine SELL position
+__global__ void coarse_csr_kernel(int64_t m, const long long* keys, const int* head, const int* mid,
+                                  const int* idx_sorted, const int* fine_csr_pos, long long nc, int* seg, int* ccol,
+                                  int* crowptr, int* src) {
+    int64_t q = blockIdx.x * (int64_t)BS + threadIdx.x;
+    if (q >= m) return;
+    src[q] = fine_csr_pos[idx_sorted[q]];
+    if (!head[q]) return;
+    int e = mid[q];
+    seg[e] = (int)q;
+    long long key = keys[q];
+    int r = (int)(key / nc);
+    ccol[e] = (int)(key % nc);
+    if (q == 0 || keys[q - 1] / nc != r) crowptr[r] = e;
+}
+
+__global__ void rowlen_slice_kernel(int n, int nslices, const int* rowptr, int* slice_entries) {
+    int s = blockIdx.x * BS + threadIdx.x;
+    if (s >= nslices) return;
+    int w = 0;
+    for (int l = 0; l < 32; ++l) {
+        int r = s * 32 + l;
+        if (r < n) w = max(w, rowptr[r + 1] - rowptr[r]);
+    }
+    slice_entries[s] = 32 * w;
+}
+
+__global__ void sell_fill_kernel(int n, int nslices, const int* rowptr, const int* col, const int* sl_off,
+                                 int* sl_col, int* csr_pos, int* diag_pos) {
+    int r = blockIdx.x * BS + threadIdx.x;
+    if (r >= nslices * 32) return;
+    int s = r >> 5, lane = r & 31;
+    int base = sl_off[s], width = (sl_off[s + 1] - base) >> 5;
+    if (r >= n) {
+        for (int j = 0; j < width; ++j) sl_col[base + 32 * j + lane] = 0;
+        return;
+    }
+    int len = rowptr[r + 1] - rowptr[r];
+    for (int j = 0; j < width; ++j) {
+        int pos = base + 32 * j + lane;
+        if (j < len) {
+            int c = col[rowptr[r] + j];
+            sl_col[pos] = c;
+            csr_pos[rowptr[r] + j] = pos;
+            if (c == r) diag_pos[r] = pos;
+        } else {
+            sl_col[pos] = r;
+        }
+    }
+}
+
+__global__ void member_heads_kernel(int n, const int* agg_sorted, int* m_off) {
+    int q = blockIdx.x * BS + threadIdx.x;
+    if (q >= n) return;
+    if (q == 0 || agg_sorted[q] != agg_sorted[q - 1]) m_off[agg_sorted[q]] = q;
+}
+
+// SELL position of every CSR entry (entry j of row r sits in slot j of the row)
+__global__ void csr_pos_kernel(int n, const int* rowptr, const int* sl_off, int* csr_pos) {
+    int r = blockIdx.x * BS + threadIdx.x;
+    if (r >= n) return;
+    const int base = sl_off[r >> 5] + (r & 31);
+    for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) csr_pos[k] = base + 32 * (k - rowptr[r]);
+}
+
+__global__ void iota_kernel(int n, int* v) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+// coarse values: sum of the sorted fine entries of each coarse entry, in order
+__global__ void galerkin_values_kernel(int nnz_c, const int* seg, const int* src, const double* fine_vals,
+                                       const int* coarse_csr_pos, double* coarse_vals) {
+    int m = blockIdx.x * BS + threadIdx.x;
+    if (m >= nnz_c) return;
+    double sum = 0.0;
+    for (int q = seg[m]; q < seg[m + 1]; ++q) sum += fine_vals[src[q]];
+    coarse_vals[coarse_csr_pos[m]] = sum;
+}
+
+__global__ void dinv_kernel(int n, const int* diag_pos, const double* vals, double* dinv, float* dinv32) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i >= n) return;
+    double d = vals[diag_pos[i]];
+    double di = d != 0.0 ? 1.0 / d : 0.0;
+    dinv[i] = di;
+    if (dinv32) dinv32[i] = (float)di;
+}
+
+__global__ void to_float_kernel(int64_t m, const double* a, float* b) {
+    for (int64_t k = blockIdx.x * (int64_t)BS + threadIdx.x; k < m; k += (int64_t)gridDim.x * BS) b[k] = (float)a[k];
+}
+
+__global__ void dense_fill_kernel(int n, const int* rowptr, const int* col, const int* csr_pos, const double* vals,
+                                  double* M) {
+    int r = blockIdx.x * BS + threadIdx.x;
+    if (r >= n) return;
+    for (int j = 0; j < n; ++j) M[(size_t)r * n + j] = 0.0;
+    for (int k = rowptr[r]; k < rowptr[r + 1]; ++k) M[(size_t)r * n + col[k]] += vals[csr_pos[k]];
+}
+
+// In-place Gauss-Jordan inversion (partial pivoting) of the n x n row-major
+// matrix M in shared memory, one block of 32 warps. A pivot below 1e-12 of the
+// largest diagonal entry marks a singular direction (e.g. the constant vector
+// of an all-Neumann Laplacian): its row and column are zeroed, which yields the
+// solution of a consistent system with that unknown set to zero.
+__global__ void __launch_bounds__(1024) gauss_jordan_kernel(int n, const double* __restrict__ M,
+                                                            double* __restrict__ inv, float* __restrict__ inv32,
+                                                            int* __restrict__ nsing) {
+    extern __shared__ double a[];
+    __shared__ double fac[DENSE_MAX];
+    __shared__ int perm[DENSE_MAX];
+    __shared__ double red_v[32];
+    __shared__ int red_i[32];
+    __shared__ double amax;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int e = t; e < n * n; e += blockDim.x) a[e] = M[e];
+    __syncthreads();
+    if (t == 0) {
+        double m = 0.0;
+        for (int i = 0; i < n; ++i) m = fmax(m, fabs(a[i * n + i]));
+        amax = m;
+        *nsing = 0;
+    }
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        if (warp == 0) {
+            double bv = -1.0;
+            int bi = k;
+            for (int i = k + lane; i < n; i += 32) {
+                double v = fabs(a[i * n + k]);
+                if (v > bv) {
+                    bv = v;
+                    bi = i;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                double ov = __shfl_down_sync(0xffffffffu, bv, o);
+                int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ov > bv || (ov == bv && oi < bi)) {
+                    bv = ov;
+                    bi = oi;
+                }
+            }
+            if (lane == 0) {
+                red_v[0] = bv;
+                red_i[0] = bi;
+                perm[k] = bi;
+            }
+        }
+        __syncthreads();
+        const int p = red_i[0];
+        if (p != k)
+            for (int j = t; j < n; j += blockDim.x) {
+                double x = a[k * n + j];
+                a[k * n + j] = a[p * n + j];
+                a[p * n + j] = x;
+            }
+        __syncthreads();
+        const double piv = a[k * n + k];
+        if (!(fabs(piv) > 1e-12 * amax)) {
+            for (int j = t; j < n; j += blockDim.x) {
+                a[k * n + j] = 0.0;
+                a[j * n + k] = 0.0;
+            }
+            if (t == 0) *nsing += 1;
+            __syncthreads();
+            continue;
+        }
+        for (int i = t; i < n; i += blockDim.x) fac[i] = (i == k) ? 0.0 : a[i * n + k];
+        __syncthreads();
+        for (int j = t; j < n; j += blockDim.x) a[k * n + j] = (j == k ? 1.0 : a[k * n + j]) / piv;
+        __syncthreads();
+        for (int i = warp; i < n; i += 32) {
+            if (i == k) continue;
+            const double f = fac[i];
+            for (int j = lane; j < n; j += 32) a[i * n + j] = (j == k ? 0.0 : a[i * n + j]) - f * a[k * n + j];
+        }
+        __syncthreads();
+    }
+    for (int k = n - 1; k >= 0; --k) {
+        const int p = perm[k];
+        if (p != k)
+            for (int i = t; i < n; i += blockDim.x) {
+                double x = a[i * n + k];
+                a[i * n + k] = a[i * n + p];
+                a[i * n + p] = x;
+            }
+        __syncthreads();
+    }
+    for (int e = t; e < n * n; e += blockDim.x) {
+        inv[e] = a[e];
+        if (inv32) inv32[e] = (float)a[e];
+    }
+}
+
+// ---------------------------------------------------------------- cycle kernels
+template <typename T>
+__global__ void smooth0_kernel(int n, T* x, const T* b, const T* dinv, T omega, const KState* S) {
+    if (S && S->done) return;
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) x[i] = omega * dinv[i] * b[i];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BS) residual_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                      const int* __restrict__ col, const T* __restrict__ val,
+                                                      const T* __restrict__ b, const T* __restrict__ x,
+                                                      T* __restrict__ res, const KState* S) {
+    if (S && S->done) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
+        const int r = sl * 32 + lane;
+        T sum = 0;
+        for (int j = 0; j < width; ++j) sum += val[bo + 32 * j + lane] * x[col[bo + 32 * j + lane]];
+        if (r < n) res[r] = b[r] - sum;
+    }
+}
+
+template <typename T>
+__global__ void restrict_kernel(int nc, const int* m_off, const int* m_idx, const T* res, T* bc, const KState* S) {
+    if (S && S->done) return;
+    int c = blockIdx.x * BS + threadIdx.x;
+    if (c >= nc) return;
+    T sum = 0;
+    for (int q = m_off[c]; q < m_off[c + 1]; ++q) sum += res[m_idx[q]];
+    bc[c] = sum;
+}
+
+// out = xp + omega dinv (b - A xp), xp = x + scale * xc[agg]
+template <typename T>
+__global__ void __launch_bounds__(BS) post_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                  const int* __restrict__ col, const T* __restrict__ val,
+                                                  const T* __restrict__ b, const T* __restrict__ x,
+                                                  const T* __restrict__ xc, const int* __restrict__ agg, T scale,
+                                                  const T* __restrict__ dinv, T omega, T* __restrict__ out,
+                                                  const KState* S) {
+    if (S && S->done) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
+        const int r = sl * 32 + lane;
+        T sum = 0;
+        for (int j = 0; j < width; ++j) {
+            int c = col[bo + 32 * j + lane];
+            sum += val[bo + 32 * j + lane] * (x[c] + scale * xc[agg[c]]);
+        }
+        if (r < n) {
+            T xp = x[r] + scale * xc[agg[r]];
+            out[r] = xp + omega * dinv[r] * (b[r] - sum);
+        }
+    }
+}
+
+// x = Inv b on the coarsest level (one warp per row)
+template <typename T>
+__global__ void coarse_solve_kernel(int n, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x,
+                                    const KState* S) {
+    if (S && S->done) return;
+    int row = (blockIdx.x * BS + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= n) return;
+    T sum = 0;
+    for (int c = lane; c < n; c += 32) sum += inv[(size_t)row * n + c] * b[c];
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+    if (lane == 0) x[row] = sum;
+}
+
+// coarsest level too large for a dense inverse: a few damped Jacobi sweeps
+template <typename T>
+__global__ void __launch_bounds__(BS) jacobi_sweep_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                          const int* __restrict__ col, const T* __restrict__ val,
+                                                          const T* __restrict__ b, const T* __restrict__ x,
+                                                          const T* __restrict__ dinv, T omega, T* __restrict__ out,
+                                                          const KState* S) {
+    if (S && S->done) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
+        const int r = sl * 32 + lane;
+        T sum = 0;
+        for (int j = 0; j < width; ++j) sum += val[bo + 32 * j + lane] * x[col[bo + 32 * j + lane]];
+        if (r < n) out[r] = x[r] + omega * dinv[r] * (b[r] - sum);
+    }
+}
+
+// ---------------------------------------------------------------- structure builders
+// Handshake pairwise matching on level L: writes the aggregate of every row
+// into agg (n entries) and returns the number of aggregates.
+int matchPairs(const AmgLevel& L, int* agg, cudaStream_t s) {
+    const int n = L.n;
+    TmpBuf<double> w(std::max<int64_t>(L.nnz, 1), s), wmax(n, s);
+    TmpBuf<int> label(n, s), cand(n, s), root(n + 1, s), rootid(n + 1, s);
+    weights_kernel<<<grid(n), BS, 0, s>>>(n, L.rowptr, L.col, L.csr_pos, L.diag_pos, L.vals, w.p, wmax.p); countLaunch();
+    PB_CUDA(cudaMemsetAsync(label.p, 0xff, n * sizeof(int), s));
+    for (int round = 0; round < MATCH_ROUNDS; ++round) {
+        propose_kernel<<<grid(n), BS, 0, s>>>(n, L.rowptr, L.col, w.p, wmax.p, label.p, cand.p); countLaunch();
+        accept_kernel<<<grid(n), BS, 0, s>>>(n, cand.p, label.p); countLaunch();
+    }
+    finish_label_kernel<<<grid(n), BS, 0, s>>>(n, L.rowptr, L.col, w.p, wmax.p, label.p, cand.p, root.p); countLaunch();
+    PB_CUDA(cudaMemsetAsync(root.p + n, 0, sizeof(int), s));
+    size_t tb = 0;
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, root.p, rootid.p, n + 1, s));
+    TmpBuf<unsigned char> tmp(std::max<size_t>(tb, 1), s);
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, tb, root.p, rootid.p, n + 1, s));
+    agg_kernel<<<grid(n), BS, 0, s>>>(n, cand.p, rootid.p, agg); countLaunch();
+    int nc = 0;
+    PB_CUDA(cudaMemcpyAsync(&nc, rootid.p + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    PB_LAUNCH("amg matching");
+    return nc;
+}
+
+// Galerkin structure of P^T A P for the aggregate map `agg` (nc aggregates):
+// fills the restriction data of L and creates the coarse level C (pattern + SELL).
+void galerkinStructure(AmgLevel& L, const int* agg, int nc, AmgLevel& C, cudaStream_t s) {
+    const int n = L.n;
+    const int64_t m = L.nnz;
+    TmpBuf<long long> keys(m, s), keys_s(m, s);
+    TmpBuf<int> idx(m, s), idx_s(m, s), head(m + 1, s), mid(m + 1, s);
+    keys_kernel<<<grid(n), BS, 0, s>>>(n, L.rowptr, L.col, agg, nc, keys.p, idx.p); countLaunch();
+    int end_bit = 1;
+    while (end_bit < 63 && ((long long)1 << end_bit) < (long long)nc * nc) ++end_bit;
+    size_t tb = 0;
+    PB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.p, keys_s.p, idx.p, idx_s.p, m, 0, end_bit, s));
+    TmpBuf<unsigned char> tmp(std::max<size_t>(tb, 1), s);
+    PB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, keys.p, keys_s.p, idx.p, idx_s.p, m, 0, end_bit, s));
+    heads_kernel<<<grid(m), BS, 0, s>>>(m, keys_s.p, head.p); countLaunch();
+    PB_CUDA(cudaMemsetAsync(head.p + m, 0, sizeof(int), s));
+    size_t tb2 = 0;
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb2, head.p, mid.p, m + 1, s));
+    TmpBuf<unsigned char> tmp2(std::max<size_t>(tb2, 1), s);
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(tmp2.p, tb2, head.p, mid.p, m + 1, s));
+    int nnz_c = 0;
+    PB_CUDA(cudaMemcpyAsync(&nnz_c, mid.p + m, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    // restriction data + coarse CSR
+    L.gal_seg.alloc(nnz_c + 1);
+    L.gal_src.alloc(m);
+    C.n = nc;
+    C.nnz = nnz_c;
+    C.o_rowptr.alloc(nc + 1);
+    C.o_col.alloc(nnz_c);
+    coarse_csr_kernel<<<grid(m), BS, 0, s>>>(m, keys_s.p, head.p, mid.p, idx_s.p, L.csr_pos, nc, L.gal_seg.p,
+                                             C.o_col.p, C.o_rowptr.p, L.gal_src.p); countLaunch();
+    int hm = (int)m;
+    PB_CUDA(cudaMemcpyAsync(L.gal_seg.p + nnz_c, &hm, sizeof(int), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(C.o_rowptr.p + nc, &nnz_c, sizeof(int), cudaMemcpyHostToDevice, s));
+    // coarse SELL
+    C.nslices = ceil_div(nc, 32);
+    TmpBuf<int> se(C.nslices + 1, s);
+    PB_CUDA(cudaMemsetAsync(se.p + C.nslices, 0, sizeof(int), s));
+    rowlen_slice_kernel<<<grid(C.nslices), BS, 0, s>>>(nc, C.nslices, C.o_rowptr.p, se.p); countLaunch();
+    C.o_sl_off.alloc(C.nslices + 1);
+    size_t tb3 = 0;
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb3, se.p, C.o_sl_off.p, C.nslices + 1, s));
+    TmpBuf<unsigned char> tmp3(std::max<size_t>(tb3, 1), s);
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(tmp3.p, tb3, se.p, C.o_sl_off.p, C.nslices + 1, s));
+    int sell = 0;
+    PB_CUDA(cudaMemcpyAsync(&sell, C.o_sl_off.p + C.nslices, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    C.sell_nnz = sell;
+    C.o_sl_col.alloc(std::max(sell, 1));
+    C.o_csr_pos.alloc(std::max(nnz_c, 1));
+    C.o_diag_pos.alloc(nc);
+    sell_fill_kernel<<<grid((int64_t)C.nslices * 32), BS, 0, s>>>(nc, C.nslices, C.o_rowptr.p, C.o_col.p,
+                                                                   C.o_sl_off.p, C.o_sl_col.p, C.o_csr_pos.p,
+                                                                   C.o_diag_pos.p); countLaunch();
+    C.rowptr = C.o_rowptr.p;
+    C.col = C.o_col.p;
+    C.csr_pos = C.o_csr_pos.p;
+    C.sl_off = C.o_sl_off.p;
+    C.sl_col = C.o_sl_col.p;
+    C.diag_pos = C.o_diag_pos.p;
+    C.o_vals.alloc(std::max(sell, 1));
+    C.o_vals.zero(s);
+    C.vals = C.o_vals.p;
+    PB_LAUNCH("amg galerkin structure");
+}
+
+void galerkinValues(const AmgLevel& L, AmgLevel& C, cudaStream_t s) {
+    galerkin_values_kernel<<<grid(C.nnz), BS, 0, s>>>((int)C.nnz, L.gal_seg.p, L.gal_src.p, L.vals, C.csr_pos,
+                                                       C.o_vals.p); countLaunch();
+}
+
+// aggregate -> member rows (rows sorted by aggregate, stable)
+void members(AmgLevel& L, int nc, cudaStream_t s) {
+    const int n = L.n;
+    TmpBuf<int> rows(n, s), agg_s(n, s);
+    iota_kernel<<<grid(n), BS, 0, s>>>(n, rows.p); countLaunch();
+    L.m_idx.alloc(n);
+    int end_bit = 1;
+    while (end_bit < 31 && (1 << end_bit) < nc) ++end_bit;
+    size_t tb = 0;
+    PB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, L.agg.p, agg_s.p, rows.p, L.m_idx.p, n, 0, end_bit, s));
+    TmpBuf<unsigned char> tmp(std::max<size_t>(tb, 1), s);
+    PB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, L.agg.p, agg_s.p, rows.p, L.m_idx.p, n, 0, end_bit, s));
+    L.m_off.alloc(nc + 1);
+    member_heads_kernel<<<grid(n), BS, 0, s>>>(n, agg_s.p, L.m_off.p); countLaunch();
+    PB_CUDA(cudaMemcpyAsync(L.m_off.p + nc, &n, sizeof(int), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    PB_LAUNCH("amg members");
+}
+
+// returns true if a buffer was allocated
+bool allocCycle(AmgLevel& L, bool mixed, cudaStream_t s) {
+    bool fresh = false;
+    int np = L.nslices * 32;
+    for (auto* b : {&L.b, &L.x, &L.x2, &L.res, &L.dinv})
+        if (!b->p) {
+            b->alloc(np);
+            b->zero(s);
+            fresh = true;
+        }
+    if (mixed) {
+        for (auto* b : {&L.b32, &L.x32, &L.x232, &L.res32, &L.dinv32})
+            if (!b->p) {
+                b->alloc(np);
+                b->zero(s);
+                fresh = true;
+            }
+        if (!L.vals32.p) {
+            L.vals32.alloc(std::max<int64_t>(L.sell_nnz, 1));
+            L.vals32.zero(s);
+            fresh = true;
+        }
+    }
+    return fresh;
+}
+
+}  // namespace
+
+void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mixed, cudaStream_t s) {
+    if (!built || levels.empty() || levels[0]->n != A.n || levels[0]->sl_off != A.sl_off) {
+        levels.clear();
+        coarse_a.release();
+        coarse_inv.release();
+        coarse_inv32.release();
+        coarse_bad.release();
+        auto L0 = std::make_unique<AmgLevel>();
+        L0->n = A.n;
+        L0->nslices = A.nslices;
+        L0->nnz = A.nnz_csr;
+        L0->sell_nnz = A.nnz_padded;
+        L0->rowptr = rowptr;
+        L0->col = col;
+        L0->o_csr_pos.alloc(std::max<int64_t>(A.nnz_csr, 1));
+        csr_pos_kernel<<<grid(A.n), BS, 0, s>>>(A.n, rowptr, A.sl_off, L0->o_csr_pos.p); countLaunch();
+        L0->csr_pos = L0->o_csr_pos.p;
+        L0->sl_off = A.sl_off;
+        L0->sl_col = A.col;
+        L0->diag_pos = A.diag_pos;
+        L0->vals = A.vals;
+        levels.push_back(std::move(L0));
+        // PRISM_VERBOSE: host time of the setup phases (stream drained around each)
+        double t_match = 0.0, t_gal = 0.0, t_mem = 0.0;
+        auto timed = [&](double& acc, auto&& f) {
+            if (!verbose()) return f();
+            PB_CUDA(cudaStreamSynchronize(s));
+            auto t0 = std::chrono::steady_clock::now();
+            auto r = f();
+            PB_CUDA(cudaStreamSynchronize(s));
+            acc += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return r;
+        };
+        while ((int)levels.size() < MAX_LEVELS) {
+            AmgLevel& L = *levels.back();
+            if (L.n <= COARSE_MAX) break;
+            // pass 1
+            TmpBuf<int> agg1(L.n, s);
+            int n1 = timed(t_match, [&] { return matchPairs(L, agg1.p, s); });
+            if (n1 > (int)(0.9 * L.n)) break;
+            AmgLevel T;
+            timed(t_gal, [&] {
+                galerkinStructure(L, agg1.p, n1, T, s);
+                galerkinValues(L, T, s);
+                return 0;
+            });
+            // pass 2 on the pass-1 operator
+            TmpBuf<int> agg2(n1, s);
+            int n2 = timed(t_match, [&] { return matchPairs(T, agg2.p, s); });
+            L.agg.alloc(L.n);
+            compose_kernel<<<grid(L.n), BS, 0, s>>>(L.n, agg1.p, agg2.p, L.agg.p); countLaunch();
+            auto C = std::make_unique<AmgLevel>();
+            timed(t_gal, [&] {
+                galerkinStructure(L, L.agg.p, n2, *C, s);
+                galerkinValues(L, *C, s);
+                return 0;
+            });
+            timed(t_mem, [&] {
+                members(L, n2, s);
+                return 0;
+            });
+            levels.push_back(std::move(C));
+        }
+        coarse_n = levels.back()->n;
+        if (verbose()) {
+            std::fprintf(stderr, "[prism amg] hierarchy:");
+            for (auto& L : levels) std::fprintf(stderr, " %d/%lld", L->n, (long long)L->nnz);
+            std::fprintf(stderr, " (rows/entries), coarsest %s; matching %.1f ms, galerkin %.1f ms, members %.1f ms\n",
+                         coarse_n <= DENSE_MAX ? "dense" : "Jacobi", t_match, t_gal, t_mem);
+        }
+        trimScratch(s);
+        if (coarse_n <= DENSE_MAX) {
+            coarse_a.alloc((size_t)coarse_n * coarse_n);
+            coarse_inv.alloc((size_t)coarse_n * coarse_n);
+            coarse_bad.alloc(1);
+            PB_CUDA(cudaFuncSetAttribute(gauss_jordan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         DENSE_MAX * DENSE_MAX * (int)sizeof(double)));
+        }
+        built = true;
+        ++generation;
+    } else if (levels[0]->vals != A.vals) {
+        levels[0]->vals = A.vals;
+        ++generation;
+    }
+    for (auto& L : levels)
+        if (allocCycle(*L, mixed, s)) ++generation;
+    if (mixed && coarse_inv.p && !coarse_inv32.p) {
+        coarse_inv32.alloc(coarse_inv.n);
+        ++generation;
+    }
+    has32 = mixed;
+    // values of every level from the current matrix
+    for (size_t l = 0; l + 1 < levels.size(); ++l) galerkinValues(*levels[l], *levels[l + 1], s);
+    for (auto& L : levels) {
+        dinv_kernel<<<grid(L->n), BS, 0, s>>>(L->n, L->diag_pos, L->vals, L->dinv.p, mixed ? L->dinv32.p : nullptr); countLaunch();
+        if (mixed) {
+            to_float_kernel<<<std::min<int64_t>(grid(L->sell_nnz), NUM_SMS * 32), BS, 0, s>>>(L->sell_nnz, L->vals,
+                                                                                               L->vals32.p); countLaunch();
+        }
+    }
+    if (coarse_inv.p) {
+        const AmgLevel& C = *levels.back();
+        const int n = coarse_n;
+        dense_fill_kernel<<<grid(n), BS, 0, s>>>(n, C.rowptr, C.col, C.csr_pos, C.vals, coarse_a.p); countLaunch();
+        gauss_jordan_kernel<<<1, 1024, (size_t)n * n * sizeof(double), s>>>(n, coarse_a.p, coarse_inv.p,
+                                                                            mixed ? coarse_inv32.p : nullptr,
+                                                                            coarse_bad.p); countLaunch();
+        if (verbose()) {
+            int ns = 0;
+            PB_CUDA(cudaMemcpyAsync(&ns, coarse_bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            PB_CUDA(cudaStreamSynchronize(s));
+            if (ns) std::fprintf(stderr, "[prism amg] coarsest level: %d singular pivot(s) dropped\n", ns);
+        }
+    }
+    PB_LAUNCH("amg setup");
+}
+
+namespace {
+
+template <typename T>
+struct CycleData {
+    static const T* vals(const AmgLevel& L);
+};
+template <>
+const double* CycleData<double>::vals(const AmgLevel& L) { return L.vals; }
+template <>
+const float* CycleData<float>::vals(const AmgLevel& L) { return L.vals32.p; }
+
+template <typename T>
+struct Bufs {
+    T *b, *x, *x2, *res;
+    const T* dinv;
+};
+Bufs<double> bufs64(AmgLevel& L) { return {L.b.p, L.x.p, L.x2.p, L.res.p, L.dinv.p}; }
+Bufs<float> bufs32(AmgLevel& L) { return {L.b32.p, L.x32.p, L.x232.p, L.res32.p, L.dinv32.p}; }
+
+template <typename T>
+void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s) {
+    AmgLevel& L = *A.levels[l];
+    auto B = [&](AmgLevel& X) {
+        if constexpr (sizeof(T) == 8) return bufs64(X);
+        else return bufs32(X);
+    };
+    Bufs<T> lb = B(L);
+    const T omega = (T)A.omega;
+    if (l + 1 == A.levels.size()) {
+        if (A.coarse_inv.p) {
+            const T* inv;
+            if constexpr (sizeof(T) == 8) inv = A.coarse_inv.p;
+            else inv = A.coarse_inv32.p;
+            coarse_solve_kernel<T><<<grid((int64_t)L.n * 32), BS, 0, s>>>(L.n, inv, b, out, S); countLaunch();
+        } else {
+            // ping-pong between x and res (out is this level's x2 or a caller vector)
+            smooth0_kernel<T><<<grid(L.n), BS, 0, s>>>(L.n, lb.x, b, lb.dinv, omega, S); countLaunch();
+            T* cur = lb.x;
+            T* nxt = lb.res;
+            for (int k = 0; k < 8; ++k) {
+                T* dst = (k == 7) ? out : nxt;
+                jacobi_sweep_kernel<T><<<sgrid(L.nslices), BS, 0, s>>>(L.nslices, L.n, L.sl_off, L.sl_col,
+                                                                       CycleData<T>::vals(L), b, cur, lb.dinv, omega,
+                                                                       dst, S); countLaunch();
+                nxt = cur;
+                cur = dst;
+            }
+        }
+        return;
+    }
+    AmgLevel& N = *A.levels[l + 1];
+    Bufs<T> nb = B(N);
+    smooth0_kernel<T><<<grid(L.n), BS, 0, s>>>(L.n, lb.x, b, lb.dinv, omega, S); countLaunch();
+    residual_kernel<T><<<sgrid(L.nslices), BS, 0, s>>>(L.nslices, L.n, L.sl_off, L.sl_col, CycleData<T>::vals(L), b,
+                                                       lb.x, lb.res, S); countLaunch();
+    restrict_kernel<T><<<grid(N.n), BS, 0, s>>>(N.n, L.m_off.p, L.m_idx.p, lb.res, nb.b, S); countLaunch();
+    vcycle<T>(A, l + 1, nb.b, nb.x2, S, s);
+    post_kernel<T><<<sgrid(L.nslices), BS, 0, s>>>(L.nslices, L.n, L.sl_off, L.sl_col, CycleData<T>::vals(L), b, lb.x,
+                                                   nb.x2, L.agg.p, (T)A.scale, lb.dinv, omega, out, S); countLaunch();
+}
+
+}  // namespace
+
+void Amg::apply(const double* r, double* z, const KState* S, cudaStream_t s) { vcycle<double>(*this, 0, r, z, S, s); }
+void Amg::apply32(const float* r, float* z, const KState* S, cudaStream_t s) { vcycle<float>(*this, 0, r, z, S, s); }
+
+}  // namespace pb

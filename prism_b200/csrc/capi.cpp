@@ -579,6 +579,8 @@ API int prism_solve_csr(int64_t n, const int64_t* rowptr, const int64_t* col, co
     return guard([&] {
         ARG(n > 0 && rowptr && col && values && b && x && o, "bad argument");
         ARG(n < (int64_t(1) << 31), "matrix too large");
+        ARG(rowptr[0] == 0 && rowptr[n] < (int64_t(1) << 31), "bad row pointers");
+        for (int64_t i = 0; i < n; ++i) ARG(rowptr[i + 1] >= rowptr[i], "bad row pointers");
         // host-side SELL-32 layout of the caller's CSR matrix
         int nslices = ceil_div(n, 32);
         std::vector<int> slo(nslices + 1, 0), dpos(n, -1);
@@ -639,9 +641,17 @@ API int prism_solve_csr(int64_t n, const int64_t* rowptr, const int64_t* col, co
         if (o->method == PRISM_SOLVER_JACOBI) {
             jacobiStep(A, d_b.p, d_x.p, kw, s);
         } else {
+            Amg amg;
+            DevBuf<int> d_rp, d_col;
+            const bool use_amg = choosePreconditioner(o->preconditioner, n) == PRISM_PC_AMG;
+            if (use_amg) {
+                std::vector<int> rp32(rowptr, rowptr + n + 1), col32(col, col + rowptr[n]);
+                d_rp.upload(rp32, s);
+                d_col.upload(col32, s);
+            }
             k = bicgstab(A, d_b.p, d_x.p, o->krylov_tol > 0 ? o->krylov_tol : 1e-12,
                          o->krylov_max_iter > 0 ? o->krylov_max_iter : 2 * n, o->precision,
-                         o->inner_tol > 0 ? o->inner_tol : 0.1, kw, s);
+                         o->inner_tol > 0 ? o->inner_tol : 0.1, kw, s, use_amg ? &amg : nullptr, d_rp.p, d_col.p);
         }
         double res = scaledResidual(A, d_b.p, d_x.p, kw, s);
         d_x.download(x, n, s);

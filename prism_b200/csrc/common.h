@@ -7,6 +7,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -77,6 +78,47 @@ struct DevBuf {
     explicit operator bool() const { return p != nullptr; }
 };
 
+// Library-owned stream-ordered memory pool of the current device, for
+// temporaries of setup phases: freed blocks are reused by later temporaries
+// without a device synchronisation; trimScratch() returns them to the device.
+inline cudaMemPool_t scratchPool() {
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    PB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) fail(PRISM_INTERNAL, "device index out of range");
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        PB_CUDA(cudaMemPoolCreate(&pools[dev], &props));
+        uint64_t keep = ~0ull;
+        PB_CUDA(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return pools[dev];
+}
+inline void trimScratch(cudaStream_t s) {
+    PB_CUDA(cudaStreamSynchronize(s));
+    PB_CUDA(cudaMemPoolTrimTo(scratchPool(), 0));
+}
+
+// Temporary device buffer in stream order on stream s (scratchPool()).
+template <typename T>
+struct TmpBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    TmpBuf(size_t count, cudaStream_t st) : n(count), s(st) {
+        if (count)
+            PB_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), count * sizeof(T), scratchPool(), s));
+    }
+    TmpBuf(const TmpBuf&) = delete;
+    TmpBuf& operator=(const TmpBuf&) = delete;
+    ~TmpBuf() {
+        if (p) cudaFreeAsync(p, s);
+    }
+};
+
 // Number of kernels this library has launched (read by the profiling window).
 inline std::atomic<long long>& launchCounter() {
     static std::atomic<long long> c{0};
@@ -85,6 +127,16 @@ inline std::atomic<long long>& launchCounter() {
 inline void countLaunch() { launchCounter().fetch_add(1, std::memory_order_relaxed); }
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// PRISM_VERBOSE=1 in the environment: solver diagnostics on stderr
+// (hierarchy sizes, per-solve timings and iteration counts).
+inline bool verbose() {
+    static const bool v = [] {
+        const char* e = std::getenv("PRISM_VERBOSE");
+        return e && e[0] && e[0] != '0';
+    }();
+    return v;
+}
 
 constexpr double EPSILON = 2.220446049250313080847263336181640625e-16; // std::numeric_limits<double>::epsilon()
 constexpr int SLICE = 32;  // SELL slice height: one warp of rows

@@ -25,9 +25,11 @@
 // replaces the FP32 one and the recurrences continue with the Krylov space kept.
 // Convergence is only declared on an FP64 true residual.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "krylov.h"
+#include "amg.h"
 
 namespace pb {
 
@@ -178,17 +180,18 @@ __global__ void __launch_bounds__(BS) s_kernel(int n, T* __restrict__ s, const T
         s[i] = (T)((double)r[i] - alpha * (double)v[i]);
 }
 
+// x += alpha p + w q ; r = s - w t  (q = s without a preconditioner pass, else q = M^-1 s, p = M^-1 p)
 template <typename T>
 __global__ void __launch_bounds__(BS) xr_kernel(int n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
-                                                const T* __restrict__ s, const T* __restrict__ t,
-                                                const T* __restrict__ r0, double* partials, unsigned int* counter,
-                                                KState* S) {
+                                                const T* __restrict__ q, const T* __restrict__ s,
+                                                const T* __restrict__ t, const T* __restrict__ r0, double* partials,
+                                                unsigned int* counter, KState* S) {
     if (S->done) return;
     const double alpha = S->alpha, w = S->w;
     double d0 = 0.0, d1 = 0.0;
     for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS) {
         double si = (double)s[i];
-        double xi = (double)x[i] + alpha * (double)p[i] + w * si;
+        double xi = (double)x[i] + alpha * (double)p[i] + w * (double)q[i];
         T ri = (T)(si - w * (double)t[i]);
         x[i] = (T)xi;
         r[i] = ri;
@@ -416,9 +419,14 @@ __global__ void __launch_bounds__(BS) resid_kernel(int nslices, int n, const int
 
 }  // namespace
 
+// Fresh buffers are zeroed with cudaMemset on the legacy stream, then that
+// stream is drained so the zeros land before any kernel of the (non-blocking)
+// solve stream reads them.
 void KrylovWork::ensure(int n_pad, int64_t nnz_padded, bool mixed) {
     if (!host_state) PB_CUDA(cudaMallocHost(&host_state, sizeof(KState) + 64));
+    bool fresh = false;
     if (n != n_pad || nnz != nnz_padded) {
+        fresh = true;
         n = n_pad;
         nnz = nnz_padded;
         for (auto* b : {&r, &r0, &p, &v, &s, &t, &xs, &dinv, &tmp}) b->alloc(n_pad);
@@ -434,6 +442,7 @@ void KrylovWork::ensure(int n_pad, int64_t nnz_padded, bool mixed) {
         for (auto* b : {&r, &r0, &p, &v, &s, &t, &xs, &dinv, &tmp}) PB_CUDA(cudaMemset(b->p, 0, n_pad * sizeof(double)));
     }
     if (mixed && !As32) {
+        fresh = true;
         As32.alloc(nnz_padded);
         r64.alloc(n_pad);
         PB_CUDA(cudaMemset(r64.p, 0, n_pad * sizeof(double)));
@@ -442,8 +451,31 @@ void KrylovWork::ensure(int n_pad, int64_t nnz_padded, bool mixed) {
             PB_CUDA(cudaMemset(b->p, 0, n_pad * sizeof(float)));
         }
     }
+    if (fresh) PB_CUDA(cudaStreamSynchronize(nullptr));
+}
+void KrylovWork::ensurePrec(bool mixed) {
+    bool fresh = false;
+    if (y.n != (size_t)n) {
+        fresh = true;
+        y.alloc(n);
+        z.alloc(n);
+        PB_CUDA(cudaMemset(y.p, 0, n * sizeof(double)));
+        PB_CUDA(cudaMemset(z.p, 0, n * sizeof(double)));
+        y32.release();
+        z32.release();
+    }
+    if (mixed && !y32) {
+        fresh = true;
+        y32.alloc(n);
+        z32.alloc(n);
+        PB_CUDA(cudaMemset(y32.p, 0, n * sizeof(float)));
+        PB_CUDA(cudaMemset(z32.p, 0, n * sizeof(float)));
+    }
+    if (fresh) PB_CUDA(cudaStreamSynchronize(nullptr));
 }
 KrylovWork::~KrylovWork() {
+    for (auto& g : graph)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     if (host_state) cudaFreeHost(host_state);
 }
 
@@ -503,10 +535,125 @@ struct Vecs {
     T *x, *r, *r0, *p, *v, *s, *t;
 };
 
+// PRISM_VERBOSE: device time of a scope on stream s, printed to stderr at its end
+struct VerboseTimer {
+    const char* what;
+    cudaStream_t s;
+    cudaEvent_t a = nullptr, b = nullptr;
+    VerboseTimer(const char* w, cudaStream_t st) : what(w), s(st) {
+        if (!verbose()) return;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    ~VerboseTimer() {
+        if (!a) return;
+        float ms = 0.f;
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        std::fprintf(stderr, "[prism] %s: %.3f ms\n", what, ms);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+// z = M^-1 r by one AMG V-cycle (FP64 or FP32 hierarchy)
+inline void precApply(Amg* amg, const double* r, double* z, const KState* S, cudaStream_t s) { amg->apply(r, z, S, s); }
+inline void precApply(Amg* amg, const float* r, float* z, const KState* S, cudaStream_t s) { amg->apply32(r, z, S, s); }
+
+// `count` BiCGSTAB iterations on the operator M (SELL values), launched one
+// kernel at a time. With amg: right-preconditioned, y = M^-1 p and z = M^-1 s.
+template <typename T>
+void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, long long count, bool sample,
+                  KrylovWork& w, cudaStream_t s) {
+    KState* S = w.state.p;
+    const int n = A.n, vg = vecGrid(n), sg = sliceGrid(A.nslices);
+    for (long long it = 0; it < count; ++it) {
+        p_kernel<T><<<vg, BS, 0, s>>>(n, V.p, V.r, V.v, S); countLaunch();
+        const T* dp = V.p;
+        if (amg) {
+            precApply(amg, V.p, y, S, s);
+            dp = y;
+        }
+        Sample smp;
+        bool sampled = sample && sampleBegin<T>(smp, A, s);
+        spmv_kernel<T, 1><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, dp, V.v, V.r0, w.partials.p,
+                                            w.counter.p, S); countLaunch();
+        if (sampled) sampleEnd(smp, s);
+        s_kernel<T><<<vg, BS, 0, s>>>(n, V.s, V.r, V.v, S); countLaunch();
+        const T* ds = V.s;
+        if (amg) {
+            precApply(amg, V.s, z, S, s);
+            ds = z;
+        }
+        spmv_kernel<T, 2><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, ds, V.t, V.s, w.partials.p,
+                                            w.counter.p, S); countLaunch();
+        xr_kernel<T><<<vg, BS, 0, s>>>(n, V.x, V.r, dp, ds, V.s, V.t, V.r0, w.partials.p, w.counter.p, S); countLaunch();
+    }
+}
+
+// PRISM_NO_GRAPHS=1: launch every iteration kernel by kernel (diagnostics)
+bool graphsEnabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("PRISM_NO_GRAPHS");
+        return !(e && e[0] && e[0] != '0');
+    }();
+    return on;
+}
+
+// A batch of iterations. The first batch of a solve runs kernel by kernel (and
+// feeds the SpMV timing samples); later batches replay one iteration captured
+// as a CUDA graph (~90 kernels with an AMG V-cycle on each side), re-captured
+// only when an operand changes. Kernels after convergence return at once, so
+// replays past the end of a batch change nothing.
+template <typename T>
+void iterate(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, long long batch, bool first,
+             KrylovWork& w, cudaStream_t s) {
+    if (first || !graphsEnabled()) {
+        iterateEager<T>(A, M, V, amg, y, z, batch, true, w, s);
+        return;
+    }
+    auto& g = w.graph[sizeof(T) == 4 ? 1 : 0];
+    std::vector<uintptr_t> key = {(uintptr_t)A.sl_off, (uintptr_t)A.col, (uintptr_t)A.nslices, (uintptr_t)A.n,
+                                  (uintptr_t)M, (uintptr_t)V.x, (uintptr_t)V.r, (uintptr_t)V.r0, (uintptr_t)V.p,
+                                  (uintptr_t)V.v, (uintptr_t)V.s, (uintptr_t)V.t, (uintptr_t)amg,
+                                  (uintptr_t)(amg ? amg->generation : 0), (uintptr_t)y, (uintptr_t)z,
+                                  (uintptr_t)w.state.p, (uintptr_t)w.partials.p, (uintptr_t)w.counter.p};
+    if (!g.exec || g.key != key) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+        const long long c0 = launchCounter().load();
+        PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t graph = nullptr;
+        try {
+            iterateEager<T>(A, M, V, amg, y, z, 1, false, w, s);
+        } catch (...) {
+            cudaStreamEndCapture(s, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            throw;
+        }
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        const long long k = launchCounter().load() - c0;
+        launchCounter().fetch_sub(k);
+        PB_CUDA(e);
+        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        PB_CUDA(e);
+        g.key = key;
+        g.kernels = k;
+    }
+    for (long long it = 0; it < batch; ++it) PB_CUDA(cudaGraphLaunch(g.exec, s));
+    launchCounter().fetch_add(g.kernels * batch);
+}
+
 // BiCGSTAB iterations on (M, rhs) from the current x; returns iterations done.
 template <typename T>
 KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, bool from_zero, double tol,
-                      long long maxit, KrylovWork& w, cudaStream_t s) {
+                      long long maxit, KrylovWork& w, cudaStream_t s, Amg* amg, T* y, T* z) {
     KrylovOut out;
     KState* S = w.state.p;
     KState init{};
@@ -524,19 +671,10 @@ KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, 
         PB_LAUNCH("bicgstab init");
         zero = false;
         int done = 0;
+        bool first = true;
         while (true) {
-            for (long long it = 0; it < batch; ++it) {
-                p_kernel<T><<<vg, BS, 0, s>>>(n, V.p, V.r, V.v, S); countLaunch();
-                Sample smp;
-                bool sampled = sampleBegin<T>(smp, A, s);
-                spmv_kernel<T, 1><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.p, V.v, V.r0, w.partials.p,
-                                                    w.counter.p, S); countLaunch();
-                if (sampled) sampleEnd(smp, s);
-                s_kernel<T><<<vg, BS, 0, s>>>(n, V.s, V.r, V.v, S); countLaunch();
-                spmv_kernel<T, 2><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.s, V.t, V.s, w.partials.p,
-                                                    w.counter.p, S); countLaunch();
-                xr_kernel<T><<<vg, BS, 0, s>>>(n, V.x, V.r, V.p, V.s, V.t, V.r0, w.partials.p, w.counter.p, S); countLaunch();
-            }
+            iterate<T>(A, M, V, amg, y, z, batch, first, w, s);
+            first = false;
             PB_LAUNCH("bicgstab iteration");
             PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
             PB_CUDA(cudaStreamSynchronize(s));
@@ -562,26 +700,53 @@ KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, 
 }  // namespace
 
 KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, int precision,
-                   double inner_tol, KrylovWork& w, cudaStream_t s) {
+                   double inner_tol, KrylovWork& w, cudaStream_t s, Amg* amg, const int* rowptr, const int* col) {
     const bool mixed = precision == PRISM_PREC_MIXED;
     w.ensure(A.nslices * 32, A.nnz_padded, mixed);
     const int n = A.n;
     const int gn = ceil_div(n, BS);
-    dinv_kernel<<<gn, BS, 0, s>>>(n, A.diag_pos, A.vals, w.dinv.p, x, w.xs.p); countLaunch();
-    int sgrid = std::min<int64_t>((A.nnz_padded + BS - 1) / BS, NUM_SMS * 32);
-    scale_kernel<double><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As.p); countLaunch();
-    PB_LAUNCH("bicgstab scaling");
+    // The iteration runs on A64 (FP64) / M32 (FP32) for the unknown X:
+    // Jacobi: A' = A D^-1, X = D x (unscaled at the end); AMG: A itself, X = x.
+    const bool scaled = amg == nullptr;
+    SellMatrix A64 = A;
+    double* X = x;
+    const float* M32 = nullptr;
+    if (scaled) {
+        dinv_kernel<<<gn, BS, 0, s>>>(n, A.diag_pos, A.vals, w.dinv.p, x, w.xs.p); countLaunch();
+        int sgrid = std::min<int64_t>((A.nnz_padded + BS - 1) / BS, NUM_SMS * 32);
+        scale_kernel<double><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As.p); countLaunch();
+        if (mixed) {
+            scale_kernel<float><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As32.p); countLaunch();
+        }
+        PB_LAUNCH("bicgstab scaling");
+        A64.vals = w.As.p;
+        X = w.xs.p;
+        M32 = w.As32.p;
+    } else {
+        if (!rowptr || !col) fail(PRISM_INTERNAL, "AMG preconditioner without a CSR pattern");
+        w.ensurePrec(mixed);
+        VerboseTimer vt("amg setup", s);
+        amg->setup(A, rowptr, col, mixed, s);
+        M32 = amg->vals32();
+    }
+    VerboseTimer vt_solve(mixed ? "bicgstab fp32+fp64" : "bicgstab fp64", s);
+    auto finish = [&] {
+        if (scaled) {
+            unscale_kernel<<<gn, BS, 0, s>>>(n, w.dinv.p, w.xs.p, x); countLaunch();
+            PB_LAUNCH("bicgstab unscale");
+        }
+    };
     KrylovOut out;
     if (!mixed) {
-        Vecs<double> V{w.xs.p, w.r.p, w.r0.p, w.p.p, w.v.p, w.s.p, w.t.p};
+        Vecs<double> V{X, w.r.p, w.r0.p, w.p.p, w.v.p, w.s.p, w.t.p};
         // accurate-residual restarts: the recursive residual drifts from b - A x
         for (int pass = 0; pass < 4; ++pass) {
-            KrylovOut o = runBicgstab<double>(A, w.As.p, b, V, false, tol, maxit, w, s);
-            if (w.host_state->done == 4) PB_CUDA(cudaMemsetAsync(w.xs.p, 0, n * sizeof(double), s));  // b = 0: x = 0
+            KrylovOut o = runBicgstab<double>(A, A64.vals, b, V, false, tol, maxit, w, s, amg, w.y.p, w.z.p);
+            if (w.host_state->done == 4) PB_CUDA(cudaMemsetAsync(X, 0, n * sizeof(double), s));  // b = 0: x = 0
             out.iterations += o.iterations;
             out.status = o.status;
             maxit -= o.iterations;
-            unscale_kernel<<<gn, BS, 0, s>>>(n, w.dinv.p, w.xs.p, x); countLaunch();
+            finish();
             spmv(A, x, w.tmp.p, s);
             double rb[2];
             refine_residual_kernel<<<vecGrid(n), BS, 0, s>>>(n, w.tmp.p, b, reinterpret_cast<float*>(w.s.p),
@@ -591,11 +756,12 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
             out.rel_residual = rb[1] > 0 ? std::sqrt(rb[0] / rb[1]) : 0.0;
             if (o.status != PRISM_OK || out.rel_residual <= 10 * tol || maxit <= 0 || rb[1] == 0) break;
         }
+        if (verbose())
+            std::fprintf(stderr, "[prism] bicgstab fp64 n=%d: %lld iterations, rel residual %.3e, status %d\n", n,
+                         out.iterations, out.rel_residual, out.status);
         return out;
     }
-    // mixed precision: FP32 BiCGSTAB on A' with FP64 reliable updates of x' and r
-    scale_kernel<float><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As32.p); countLaunch();
-    PB_LAUNCH("bicgstab fp32 copy");
+    // mixed precision: FP32 BiCGSTAB with FP64 reliable updates of X and r
     const double delta = (inner_tol > 0.0 && inner_tol < 1.0) ? inner_tol : 0.1;
     KState* S = w.state.p;
     KState init{};
@@ -603,14 +769,12 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
     init.reliable = 1;
     init.delta2 = delta * delta;
     PB_CUDA(cudaMemcpyAsync(S, &init, sizeof(KState), cudaMemcpyHostToDevice, s));
-    SellMatrix As = A;
-    As.vals = w.As.p;
-    const int vg = vecGrid(n), sg = sliceGrid(A.nslices);
+    const int vg = vecGrid(n);
     auto reliable = [&](int first) {
         if (!first) {
-            flush_kernel<<<gn, BS, 0, s>>>(n, w.xs.p, w.x32.p); countLaunch();
+            flush_kernel<<<gn, BS, 0, s>>>(n, X, w.x32.p); countLaunch();
         }
-        spmv(As, w.xs.p, w.tmp.p, s);
+        spmv(A64, X, w.tmp.p, s);
         reliable_kernel<<<vg, BS, 0, s>>>(n, w.tmp.p, b, w.r64.p, w.r32.p, w.r032.p, w.p32.p, w.v32.p, first, tol,
                                           w.partials.p, w.counter.p, S); countLaunch();
         PB_LAUNCH("reliable update");
@@ -620,22 +784,13 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
     };
     fill_zero_f<<<gn, BS, 0, s>>>(n, w.x32.p); countLaunch();
     int done = reliable(1);
-    int restarts = 0;
+    int restarts = 0, n_reliable = 0;
     long long batch = 8;
+    Vecs<float> V32{w.x32.p, w.r32.p, w.r032.p, w.p32.p, w.v32.p, w.s32.p, w.t32.p};
+    bool first = true;
     while (done == 0) {
-        for (long long it = 0; it < batch; ++it) {
-            p_kernel<float><<<vg, BS, 0, s>>>(n, w.p32.p, w.r32.p, w.v32.p, S); countLaunch();
-            Sample smp;
-            bool sampled = sampleBegin<float>(smp, A, s);
-            spmv_kernel<float, 1><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, w.As32.p, w.p32.p, w.v32.p,
-                                                    w.r032.p, w.partials.p, w.counter.p, S); countLaunch();
-            if (sampled) sampleEnd(smp, s);
-            s_kernel<float><<<vg, BS, 0, s>>>(n, w.s32.p, w.r32.p, w.v32.p, S); countLaunch();
-            spmv_kernel<float, 2><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, w.As32.p, w.s32.p, w.t32.p,
-                                                    w.s32.p, w.partials.p, w.counter.p, S); countLaunch();
-            xr_kernel<float><<<vg, BS, 0, s>>>(n, w.x32.p, w.r32.p, w.p32.p, w.s32.p, w.t32.p, w.r032.p,
-                                               w.partials.p, w.counter.p, S); countLaunch();
-        }
+        iterate<float>(A, M32, V32, amg, w.y32.p, w.z32.p, batch, first, w, s);
+        first = false;
         PB_LAUNCH("bicgstab fp32 iteration");
         PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
         PB_CUDA(cudaStreamSynchronize(s));
@@ -645,18 +800,19 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
             continue;
         }
         if (done == 6) {
+            ++n_reliable;
             done = reliable(0);
             continue;
         }
         if (done == 3) {  // breakdown of the recurrence: flush and restart from the current x
             if (++restarts > 20) break;
-            flush_kernel<<<gn, BS, 0, s>>>(n, w.xs.p, w.x32.p); countLaunch();
+            flush_kernel<<<gn, BS, 0, s>>>(n, X, w.x32.p); countLaunch();
             done = reliable(1);
             continue;
         }
     }
     if (done == 2 || done == 3 || done == 5) {
-        flush_kernel<<<gn, BS, 0, s>>>(n, w.xs.p, w.x32.p); countLaunch();
+        flush_kernel<<<gn, BS, 0, s>>>(n, X, w.x32.p); countLaunch();
     }
     out.iterations = w.host_state->iter;
     out.status = done == 1 || done == 4 ? PRISM_OK
@@ -664,9 +820,12 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
                  : done == 5           ? PRISM_NONFINITE
                                        : PRISM_BREAKDOWN;
     out.rel_residual = w.host_state->bb > 0 ? std::sqrt(w.host_state->rr / w.host_state->bb) : 0.0;
-    if (done == 4) PB_CUDA(cudaMemsetAsync(w.xs.p, 0, n * sizeof(double), s));
-    unscale_kernel<<<gn, BS, 0, s>>>(n, w.dinv.p, w.xs.p, x); countLaunch();
-    PB_LAUNCH("bicgstab unscale");
+    if (done == 4) PB_CUDA(cudaMemsetAsync(X, 0, n * sizeof(double), s));
+    finish();
+    if (verbose())
+        std::fprintf(stderr, "[prism] bicgstab fp32+fp64 n=%d: %lld iterations, %d reliable updates, %d restarts, "
+                     "rel residual %.3e, status %d\n", n, out.iterations, n_reliable, restarts, out.rel_residual,
+                     out.status);
     return out;
 }
 

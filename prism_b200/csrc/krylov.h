@@ -24,6 +24,8 @@ void jacobiStepNoAlloc(int64_t n, const int32_t* rowptr, const int32_t* col, con
 void profileStart(int max_samples);
 void profileStop(PrismProfile* out);
 
+struct Amg;
+
 // Device-resident solver state (one per BiCGSTAB run).
 struct KState {
     double rho, alpha, w, beta;
@@ -44,10 +46,20 @@ struct KrylovWork {
     DevBuf<double> As;   // column-scaled matrix A D^-1
     DevBuf<float> As32, r32, r032, p32, v32, s32, t32, x32;
     DevBuf<double> r64;  // mixed precision: FP64 true residual at reliable updates
+    DevBuf<double> y, z;       // preconditioned directions M^-1 p, M^-1 s (AMG)
+    DevBuf<float> y32, z32;
+    void ensurePrec(bool mixed);
     DevBuf<double> partials, scal;
     DevBuf<unsigned int> counter;
     DevBuf<KState> state;
     KState* host_state = nullptr;  // pinned
+    // one BiCGSTAB iteration captured as a CUDA graph, per precision ([0] FP64, [1] FP32),
+    // reused while the operands (key) stay the same
+    struct IterGraph {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uintptr_t> key;
+        long long kernels = 0;  // kernel nodes per launch
+    } graph[2];
     void ensure(int n_pad, int64_t nnz_padded, bool mixed);
     ~KrylovWork();
 };
@@ -58,10 +70,14 @@ struct KrylovOut {
     double rel_residual = 0.0;
 };
 
-// x <- BiCGSTAB solve of A x = b from the guess x (Jacobi right preconditioning),
-// stopping at ||b - A x|| <= tol ||b||. precision: PRISM_PREC_FP64 or PRISM_PREC_MIXED.
+// x <- BiCGSTAB solve of A x = b from the guess x, stopping at ||b - A x|| <= tol ||b||.
+// precision: PRISM_PREC_FP64 or PRISM_PREC_MIXED. Right preconditioning: Jacobi
+// (column scaling) when amg is null, else one V-cycle of amg, whose hierarchy is
+// built on first use from the device CSR pattern (rowptr, col) of A and refreshed
+// with A's values on every call.
 KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, int precision,
-                   double inner_tol, KrylovWork& w, cudaStream_t s);
+                   double inner_tol, KrylovWork& w, cudaStream_t s, Amg* amg = nullptr, const int* rowptr = nullptr,
+                   const int* col = nullptr);
 // x <- x + D^-1 (b - A x)   (numerics/jacobi.cpp:5-9)
 void jacobiStep(const SellMatrix& A, const double* b, double* x, KrylovWork& w, cudaStream_t s);
 // max|A x - b| / (max|diag(A) x| + eps)   (numerics/solver.cpp:8-24); returns NaN if non-finite values met

@@ -436,6 +436,12 @@ void solveDefaults(PrismSolveOpts* o) {
     o->clear_coeffs = 1;
 }
 
+int choosePreconditioner(int pc, int64_t n) {
+    if (pc == PRISM_PC_AUTO) return n >= PRISM_PC_AUTO_MIN_ROWS ? PRISM_PC_AMG : PRISM_PC_JACOBI;
+    if (pc != PRISM_PC_JACOBI && pc != PRISM_PC_AMG) fail(PRISM_BAD_ARG, "unknown preconditioner");
+    return pc;
+}
+
 // ISolver::solve (numerics/solver.cpp:27-82)
 PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
     Scalar& phi = *eq.phi;
@@ -452,6 +458,11 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
     const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
     const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
     const double itol = o.inner_tol > 0 ? o.inner_tol : 0.1;
+    Amg* amg = nullptr;
+    if (o.method != PRISM_SOLVER_JACOBI && choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
+        if (!eq.amg) eq.amg = std::make_shared<Amg>();
+        amg = eq.amg.get();
+    }
     PrismSolveResult r{};
     r.status = PRISM_OK;
     double init_res = 0.0, cur = 0.0;
@@ -466,7 +477,8 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
         if (o.method == PRISM_SOLVER_JACOBI) {
             jacobiStep(A, eq.b.p, phi.v.p, m.kw, m.stream);
         } else {
-            KrylovOut k = bicgstab(A, eq.b.p, phi.v.p, ktol, kmax, o.precision, itol, m.kw, m.stream);
+            KrylovOut k = bicgstab(A, eq.b.p, phi.v.p, ktol, kmax, o.precision, itol, m.kw, m.stream, amg,
+                                   m.pat.rowptr.p, m.pat.col.p);
             r.krylov_iterations += k.iterations;
             r.krylov_rel_residual = k.rel_residual;
             if (k.status != PRISM_OK && r.status == PRISM_OK) r.status = k.status;
@@ -605,6 +617,8 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
     pEqn.corrector = PRISM_CORR_OVER_RELAXED;
     pEqn.kt = D.get();
     pEqn.sources.push_back({PRISM_SRC_DIVERGENCE, PRISM_SIGN_NEGATIVE, 0, nullptr, &mdot});
+    if (!m.p_amg) m.p_amg = std::make_shared<Amg>();
+    pEqn.amg = m.p_amg;
     for (int64_t i = 0; i <= c.non_ortho_correctors; ++i) {
         auto r = solve(pEqn, inner(so, c.pressure_max_iter, c.pressure_residual, c.p_ref_cell, c.p_ref_value, true));
         rep.push_back({pp->name + "_corr_" + std::to_string(i), r.iterations, r.initial_residual, r.final_residual,

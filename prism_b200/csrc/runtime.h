@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "amg.h"
 #include "assemble.h"
 #include "common.h"
 #include "krylov.h"
@@ -31,6 +32,7 @@ struct Mesh {
     DevBuf<double> ls_pinv, ls_w;
     bool ls_ready = false;
     KrylovWork kw;
+    std::shared_ptr<Amg> p_amg;  // AMG hierarchy of the pressure-correction equation (SIMPLE/PRIME/PISO)
     DevBuf<double> scratch;  // n_faces doubles for face exports
 
     ~Mesh();
@@ -98,6 +100,7 @@ struct Transport {
     double urf = 1.0;
     bool clean = true;
     DevBuf<double> A, b, bconv, bdiff;
+    std::shared_ptr<Amg> amg;  // AMG hierarchy (PRISM_PC_AMG), built on the first solve
     void ensure();
 };
 
@@ -125,5 +128,7 @@ bool needsPressureReference(const Scalar& p);
 void simpleDefaults(PrismSIMPLEControls* c);
 void pisoDefaults(PrismPISOControls* c);
 void solveDefaults(PrismSolveOpts* o);
+// PRISM_PC_AUTO resolved for an n-row system
+int choosePreconditioner(int pc, int64_t n);
 
 }  // namespace pb

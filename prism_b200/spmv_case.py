@@ -6,7 +6,11 @@ assembles it and runs one BiCGSTAB step capped at a few iterations, so that a
 profiler can capture individual SELL-32 SpMV launches with few launches before
 them. Prints the Krylov iteration count.
 
-    python -m prism_b200.spmv_case [--n 128] [--iters 3] [--mixed]
+    python -m prism_b200.spmv_case [--n 128] [--iters 3] [--mixed] [--preconditioner jacobi|amg]
+                                   [--tol 1e-12]
+
+With --preconditioner amg the step also builds the AMG hierarchy (setup) and
+runs V-cycles around every SpMV; --iters 0 runs the step to --tol.
 """
 import argparse
 
@@ -38,10 +42,13 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--mixed", action="store_true")
+    ap.add_argument("--preconditioner", default="jacobi", choices=["jacobi", "amg"])
+    ap.add_argument("--tol", type=float, default=1e-12)
     a = ap.parse_args()
     mesh, T, U, k, eqn = build(a.n, lib())
     prec = A.PREC_MIXED if a.mixed else A.PREC_FP64
-    r = api.BiCGSTAB(precision=prec, krylov_tol=1e-12, krylov_max_iter=a.iters).solve(eqn, 1, 0.0)
+    r = api.BiCGSTAB(precision=prec, krylov_tol=a.tol, krylov_max_iter=a.iters if a.iters > 0 else 100000,
+                     preconditioner=a.preconditioner).solve(eqn, 1, 0.0)
     print(f"cells {mesh.n_cells} nnz {mesh.info.nnz} krylov iterations {r.krylov_iterations} status {r.status}")
 
 
