@@ -24,6 +24,7 @@
 
 #include <chrono>
 #include <cmath>
+#include <type_traits>
 
 #include "amg.h"
 
@@ -39,7 +40,6 @@ constexpr int MAX_LEVELS = 20;
 constexpr int MATCH_ROUNDS = 10;
 
 inline int grid(int64_t n) { return std::max(1, ceil_div(n, BS)); }
-inline int sgrid(int nslices) { return std::max(1, std::min(ceil_div(nslices, WARPS), NUM_SMS * 16)); }
 
 __device__ __forceinline__ unsigned long long edgeHash(int i, int j) {
     unsigned long long a = (unsigned long long)min(i, j), b = (unsigned long long)max(i, j);
@@ -356,26 +356,46 @@ __global__ void __launch_bounds__(1024) gauss_jordan_kernel(int n, const double*
 }
 
 // ---------------------------------------------------------------- cycle kernels
-template <typename T>
-__global__ void smooth0_kernel(int n, T* x, const T* b, const T* dinv, T omega, const KState* S) {
-    if (S && S->done) return;
-    int i = blockIdx.x * BS + threadIdx.x;
-    if (i < n) x[i] = omega * dinv[i] * b[i];
+// Row-parallel SELL kernels with LPR lanes per row (LPR divides 32; the lanes
+// of a row are adjacent and split its slots round-robin). Coarse levels have
+// few, long rows: more lanes per row keep enough loads in flight.
+
+// sum_j A[row, c_j] * xf(c_j); the result is valid in every lane of the row's group
+template <typename T, int LPR, typename F>
+__device__ __forceinline__ T rowSum(const int* __restrict__ sl_off, const int* __restrict__ col,
+                                    const T* __restrict__ val, int row, bool valid, int sub, F xf) {
+    T sum = 0;
+    if (valid) {
+        const int s0 = sl_off[row >> 5];
+        const int width = (sl_off[(row >> 5) + 1] - s0) >> 5;
+        const int bo = s0 + (row & 31);
+        for (int j = sub; j < width; j += LPR) {
+            const int p = bo + 32 * j;
+            sum += val[p] * xf(col[p]);
+        }
+    }
+    if constexpr (LPR > 1) {
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    }
+    return sum;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(BS) residual_kernel(int nslices, int n, const int* __restrict__ sl_off,
-                                                      const int* __restrict__ col, const T* __restrict__ val,
-                                                      const T* __restrict__ b, const T* __restrict__ x,
-                                                      T* __restrict__ res, const KState* S) {
+// pre-smoothing from zero and residual: x = omega D^-1 b ; res = b - A x
+// (x at the neighbours formed on the fly, so no separate smoothing pass)
+template <typename T, int LPR>
+__global__ void __launch_bounds__(BS) pre_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
+                                                 const T* __restrict__ val, const T* __restrict__ b,
+                                                 const T* __restrict__ dinv, T omega, T* __restrict__ x,
+                                                 T* __restrict__ res, const KState* S) {
     if (S && S->done) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
-        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
-        const int r = sl * 32 + lane;
-        T sum = 0;
-        for (int j = 0; j < width; ++j) sum += val[bo + 32 * j + lane] * x[col[bo + 32 * j + lane]];
-        if (r < n) res[r] = b[r] - sum;
+    const int gt = blockIdx.x * BS + threadIdx.x;
+    const int row = gt / LPR, sub = gt % LPR;
+    const bool valid = row < n;
+    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, [&](int c) { return omega * dinv[c] * b[c]; });
+    if (valid && sub == 0) {
+        x[row] = omega * dinv[row] * b[row];
+        res[row] = b[row] - sum;
     }
 }
 
@@ -389,29 +409,66 @@ __global__ void restrict_kernel(int nc, const int* m_off, const int* m_idx, cons
     bc[c] = sum;
 }
 
-// out = xp + omega dinv (b - A xp), xp = x + scale * xc[agg]
-template <typename T>
-__global__ void __launch_bounds__(BS) post_kernel(int nslices, int n, const int* __restrict__ sl_off,
-                                                  const int* __restrict__ col, const T* __restrict__ val,
-                                                  const T* __restrict__ b, const T* __restrict__ x,
-                                                  const T* __restrict__ xc, const int* __restrict__ agg, T scale,
-                                                  const T* __restrict__ dinv, T omega, T* __restrict__ out,
-                                                  const KState* S) {
+// prolongation and post-smoothing: out = xp + omega D^-1 (b - A xp), xp = x + scale * xc[agg]
+template <typename T, int LPR>
+__global__ void __launch_bounds__(BS) post_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
+                                                  const T* __restrict__ val, const T* __restrict__ b,
+                                                  const T* __restrict__ x, const T* __restrict__ xc,
+                                                  const int* __restrict__ agg, T scale, const T* __restrict__ dinv,
+                                                  T omega, T* __restrict__ out, const KState* S) {
     if (S && S->done) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
-        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
-        const int r = sl * 32 + lane;
-        T sum = 0;
-        for (int j = 0; j < width; ++j) {
-            int c = col[bo + 32 * j + lane];
-            sum += val[bo + 32 * j + lane] * (x[c] + scale * xc[agg[c]]);
-        }
-        if (r < n) {
-            T xp = x[r] + scale * xc[agg[r]];
-            out[r] = xp + omega * dinv[r] * (b[r] - sum);
-        }
+    const int gt = blockIdx.x * BS + threadIdx.x;
+    const int row = gt / LPR, sub = gt % LPR;
+    const bool valid = row < n;
+    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub,
+                                 [&](int c) { return x[c] + scale * xc[agg[c]]; });
+    if (valid && sub == 0) {
+        const T xp = x[row] + scale * xc[agg[row]];
+        out[row] = xp + omega * dinv[row] * (b[row] - sum);
     }
+}
+
+// damped Jacobi sweep (coarsest level without a dense inverse): out = x + omega D^-1 (b - A x)
+template <typename T>
+__global__ void smooth0_kernel(int n, T* x, const T* b, const T* dinv, T omega, const KState* S) {
+    if (S && S->done) return;
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) x[i] = omega * dinv[i] * b[i];
+}
+template <typename T, int LPR>
+__global__ void __launch_bounds__(BS) jacobi_sweep_kernel(int n, const int* __restrict__ sl_off,
+                                                          const int* __restrict__ col, const T* __restrict__ val,
+                                                          const T* __restrict__ b, const T* __restrict__ x,
+                                                          const T* __restrict__ dinv, T omega, T* __restrict__ out,
+                                                          const KState* S) {
+    if (S && S->done) return;
+    const int gt = blockIdx.x * BS + threadIdx.x;
+    const int row = gt / LPR, sub = gt % LPR;
+    const bool valid = row < n;
+    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, [&](int c) { return x[c]; });
+    if (valid && sub == 0) out[row] = x[row] + omega * dinv[row] * (b[row] - sum);
+}
+
+// Calls f(std::integral_constant<int, LPR>) for the level's lanes per row.
+template <typename F>
+void withLpr(int lpr, F&& f) {
+    switch (lpr) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 16: f(std::integral_constant<int, 16>{}); break;
+        default: f(std::integral_constant<int, 32>{}); break;
+    }
+}
+
+// lanes per row: enough threads to fill the GPU once, at most the mean row length
+int lanesPerRow(int n, int64_t nnz) {
+    const int64_t target = (int64_t)NUM_SMS * 2048;
+    const double mean = n > 0 ? (double)nnz / n : 1.0;
+    int l = 1;
+    while (l < 32 && (int64_t)n * l * 2 <= target && l < mean) l *= 2;
+    return l;
 }
 
 // x = Inv b on the coarsest level (one warp per row)
@@ -655,10 +712,11 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
             levels.push_back(std::move(C));
         }
         coarse_n = levels.back()->n;
+        for (auto& L : levels) L->lpr = lanesPerRow(L->n, L->nnz);
         if (verbose()) {
             std::fprintf(stderr, "[prism amg] hierarchy:");
-            for (auto& L : levels) std::fprintf(stderr, " %d/%lld", L->n, (long long)L->nnz);
-            std::fprintf(stderr, " (rows/entries), coarsest %s; matching %.1f ms, galerkin %.1f ms, members %.1f ms\n",
+            for (auto& L : levels) std::fprintf(stderr, " %d/%lld/%d", L->n, (long long)L->nnz, L->lpr);
+            std::fprintf(stderr, " (rows/entries/lanes per row), coarsest %s; matching %.1f ms, galerkin %.1f ms, members %.1f ms\n",
                          coarse_n <= DENSE_MAX ? "dense" : "Jacobi", t_match, t_gal, t_mem);
         }
         trimScratch(s);
@@ -736,6 +794,7 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
     };
     Bufs<T> lb = B(L);
     const T omega = (T)A.omega;
+    const T* vals = CycleData<T>::vals(L);
     if (l + 1 == A.levels.size()) {
         if (A.coarse_inv.p) {
             const T* inv;
@@ -749,9 +808,12 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
             T* nxt = lb.res;
             for (int k = 0; k < 8; ++k) {
                 T* dst = (k == 7) ? out : nxt;
-                jacobi_sweep_kernel<T><<<sgrid(L.nslices), BS, 0, s>>>(L.nslices, L.n, L.sl_off, L.sl_col,
-                                                                       CycleData<T>::vals(L), b, cur, lb.dinv, omega,
-                                                                       dst, S); countLaunch();
+                withLpr(L.lpr, [&](auto c) {
+                    constexpr int P = decltype(c)::value;
+                    jacobi_sweep_kernel<T, P><<<grid((int64_t)L.n * P), BS, 0, s>>>(L.n, L.sl_off, L.sl_col, vals, b,
+                                                                                   cur, lb.dinv, omega, dst, S);
+                });
+                countLaunch();
                 nxt = cur;
                 cur = dst;
             }
@@ -760,13 +822,20 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
     }
     AmgLevel& N = *A.levels[l + 1];
     Bufs<T> nb = B(N);
-    smooth0_kernel<T><<<grid(L.n), BS, 0, s>>>(L.n, lb.x, b, lb.dinv, omega, S); countLaunch();
-    residual_kernel<T><<<sgrid(L.nslices), BS, 0, s>>>(L.nslices, L.n, L.sl_off, L.sl_col, CycleData<T>::vals(L), b,
-                                                       lb.x, lb.res, S); countLaunch();
+    withLpr(L.lpr, [&](auto c) {
+        constexpr int P = decltype(c)::value;
+        pre_kernel<T, P><<<grid((int64_t)L.n * P), BS, 0, s>>>(L.n, L.sl_off, L.sl_col, vals, b, lb.dinv, omega, lb.x,
+                                                               lb.res, S);
+    });
+    countLaunch();
     restrict_kernel<T><<<grid(N.n), BS, 0, s>>>(N.n, L.m_off.p, L.m_idx.p, lb.res, nb.b, S); countLaunch();
     vcycle<T>(A, l + 1, nb.b, nb.x2, S, s);
-    post_kernel<T><<<sgrid(L.nslices), BS, 0, s>>>(L.nslices, L.n, L.sl_off, L.sl_col, CycleData<T>::vals(L), b, lb.x,
-                                                   nb.x2, L.agg.p, (T)A.scale, lb.dinv, omega, out, S); countLaunch();
+    withLpr(L.lpr, [&](auto c) {
+        constexpr int P = decltype(c)::value;
+        post_kernel<T, P><<<grid((int64_t)L.n * P), BS, 0, s>>>(L.n, L.sl_off, L.sl_col, vals, b, lb.x, nb.x2,
+                                                                L.agg.p, (T)A.scale, lb.dinv, omega, out, S);
+    });
+    countLaunch();
 }
 
 }  // namespace

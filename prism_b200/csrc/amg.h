@@ -14,6 +14,7 @@ namespace pb {
 // kept both as CSR (setup) and SELL-32 (cycle kernels).
 struct AmgLevel {
     int n = 0, nslices = 0;
+    int lpr = 1;  // lanes per row of the cycle kernels
     int64_t nnz = 0, sell_nnz = 0;
     // pattern: CSR view and SELL layout; csr_pos[k] = SELL position of CSR entry k
     const int* rowptr = nullptr;

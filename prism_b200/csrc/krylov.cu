@@ -27,6 +27,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <unordered_map>
 
 #include "krylov.h"
 #include "amg.h"
@@ -100,32 +102,47 @@ inline int vecGrid(int n) { return std::max(1, std::min(ceil_div(n, BS), MAX_GRI
 inline int spmvGrid(int nslices) { return std::max(1, std::min(ceil_div(nslices, WARPS), NUM_SMS * 16)); }
 inline int sliceGrid(int nslices) { return std::max(1, std::min(ceil_div(nslices, WARPS), NUM_SMS * 16)); }
 
+int smCount() {
+    static const int c = [] {
+        int d = 0, v = 0;
+        cudaGetDevice(&d);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d);
+        return v > 0 ? v : NUM_SMS;
+    }();
+    return c;
+}
+
+// Grid of at most one wave of resident blocks: kernels ending in reduceLast()
+// pay the per-block publish (fence + atomic) once per block, so a single wave
+// keeps that tail off the critical path.
+template <typename K>
+int waveGrid(K kernel, int needed) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> occ;
+    int per_sm = 1;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = occ.find(reinterpret_cast<const void*>(kernel));
+        if (it == occ.end()) {
+            int b = 0;
+            PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, BS, 0));
+            it = occ.emplace(reinterpret_cast<const void*>(kernel), std::max(b, 1)).first;
+        }
+        per_sm = it->second;
+    }
+    return std::max(1, std::min(needed, per_sm * smCount()));
+}
+
 // y = A x for a SELL-32 matrix: a warp walks 32-row slices (one row per lane),
-// coalesced loads. For slices up to 8 entries wide every column index and value
-// of the slice is loaded before the x gathers, so a warp keeps 16 independent
-// loads in flight instead of a chain of dependent pairs; the matrix is read with
-// evict-first (streaming) loads so that L2 keeps the gathered x.
+// coalesced loads; the matrix is read with evict-first (streaming) loads so
+// that L2 keeps the gathered x.
 // STAGE 0: plain; 1: alpha = rho / (u.y); 2: w = (u.y)/(y.y)
 template <typename T>
 __device__ __forceinline__ T sliceRow(const int* __restrict__ col, const T* __restrict__ val,
                                       const T* __restrict__ x, int b, int width, int lane) {
     T sum = 0;
-    if (width <= 8) {
-        int c[8];
-        T v[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            if (j < width) {
-                c[j] = __ldcs(col + b + 32 * j + lane);
-                v[j] = __ldcs(val + b + 32 * j + lane);
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-            if (j < width) sum += v[j] * x[c[j]];
-    } else {
-        for (int j = 0; j < width; ++j) sum += __ldcs(val + b + 32 * j + lane) * x[__ldcs(col + b + 32 * j + lane)];
-    }
+#pragma unroll 4
+    for (int j = 0; j < width; ++j) sum += __ldcs(val + b + 32 * j + lane) * x[__ldcs(col + b + 32 * j + lane)];
     return sum;
 }
 
@@ -431,7 +448,7 @@ void KrylovWork::ensure(int n_pad, int64_t nnz_padded, bool mixed) {
         nnz = nnz_padded;
         for (auto* b : {&r, &r0, &p, &v, &s, &t, &xs, &dinv, &tmp}) b->alloc(n_pad);
         As.alloc(nnz_padded);
-        partials.alloc((size_t)std::max(sliceGrid(n_pad / 32), NUM_SMS * 16) * 4);
+        partials.alloc((size_t)std::max(sliceGrid(n_pad / 32), std::max(NUM_SMS, smCount()) * 16) * 4);
         counter.alloc(1);
         PB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned int)));
         scal.alloc(8);
@@ -568,7 +585,9 @@ template <typename T>
 void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, long long count, bool sample,
                   KrylovWork& w, cudaStream_t s) {
     KState* S = w.state.p;
-    const int n = A.n, vg = vecGrid(n), sg = sliceGrid(A.nslices);
+    const int n = A.n, vg = vecGrid(n);
+    const int sg1 = waveGrid(spmv_kernel<T, 1>, ceil_div(A.nslices, WARPS));
+    const int sg2 = waveGrid(spmv_kernel<T, 2>, ceil_div(A.nslices, WARPS));
     for (long long it = 0; it < count; ++it) {
         p_kernel<T><<<vg, BS, 0, s>>>(n, V.p, V.r, V.v, S); countLaunch();
         const T* dp = V.p;
@@ -578,7 +597,7 @@ void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T*
         }
         Sample smp;
         bool sampled = sample && sampleBegin<T>(smp, A, s);
-        spmv_kernel<T, 1><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, dp, V.v, V.r0, w.partials.p,
+        spmv_kernel<T, 1><<<sg1, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, dp, V.v, V.r0, w.partials.p,
                                             w.counter.p, S); countLaunch();
         if (sampled) sampleEnd(smp, s);
         s_kernel<T><<<vg, BS, 0, s>>>(n, V.s, V.r, V.v, S); countLaunch();
@@ -587,7 +606,7 @@ void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T*
             precApply(amg, V.s, z, S, s);
             ds = z;
         }
-        spmv_kernel<T, 2><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, ds, V.t, V.s, w.partials.p,
+        spmv_kernel<T, 2><<<sg2, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, ds, V.t, V.s, w.partials.p,
                                             w.counter.p, S); countLaunch();
         xr_kernel<T><<<vg, BS, 0, s>>>(n, V.x, V.r, dp, ds, V.s, V.t, V.r0, w.partials.p, w.counter.p, S); countLaunch();
     }
@@ -876,7 +895,7 @@ void explicitUpdate(const SellMatrix& A, const double* b, const double* x, doubl
 
 double scaledResidual(const SellMatrix& A, const double* b, const double* x, KrylovWork& w, cudaStream_t s) {
     w.ensure(A.nslices * 32, A.nnz_padded, false);
-    resid_kernel<<<spmvGrid(A.nslices), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x,
+    resid_kernel<<<waveGrid(resid_kernel, ceil_div(A.nslices, WARPS)), BS, 0, s>>>(A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x,
                                                      w.partials.p, w.counter.p, w.scal.p); countLaunch();
     PB_LAUNCH("resid_kernel");
     double h[3];
