@@ -9,10 +9,11 @@ urf 0.7/0.3 (configs[1]'s recipe) on 1448x1448x1 hexes (2,096,704 cells): the
 the working set (~1 GB) is larger than L2, so no flush is needed.
 
 Also reported: time to 1e-8 relative error of the 128^3 jittered-hex transport
-solve (LinearUpwind + Corrected), FP64 vs FP32-inner/FP64-refinement BiCGSTAB
-("s_to_1e8"),
-and the live SpMV bandwidth (CUDA events around the BiCGSTAB SpMV launches in
-the timed region). --impl reference times the CPU restatement of the
+solve (LinearUpwind + Corrected), FP64 vs FP32/FP64-reliable-update BiCGSTAB,
+both AMG-preconditioned, and FP64 with the Jacobi preconditioner ("s_to_1e8"),
+and the live bandwidth of the dominant kernel (the finest-level AMG
+post-smoothing SpMV) and of the BiCGSTAB SpMV (CUDA events around sampled
+launches in the timed region). --impl reference times the CPU restatement of the
 reference (single-threaded, like the reference) on a bounded sample.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
@@ -294,37 +295,59 @@ def run_ours(args, world, rank, local):
     t_e2e = max_over_ranks(world, t0.elapsed_time(t1) / 1000.0)
     e2e = world * args.steps / t_e2e
 
-    # SpMV roofline from the live samples
-    spmv_ms = prof.fp64_ms / max(prof.fp64_launches, 1)
-    spmv_bytes = prof.fp64_bytes / max(prof.fp64_launches, 1)
-    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9 if prof.fp64_launches else None
-    traffic = None
-    prof_file = os.path.join(ROOT, "profiles", "spmv_fp64_traffic.json")
-    if os.path.exists(prof_file):
-        with open(prof_file) as fh:
-            tr = json.load(fh)
-        # DRAM bytes of one launch measured by ncu on the 128^3 matrix, scaled to this launch
-        # by its algorithmic bytes (traffic grows in proportion to them: no re-reads)
-        traffic = tr["traffic_per_algorithmic_byte"] * spmv_bytes
-    roof = {"kernel": "spmv_kernel<double,1> (SELL-32 SpMV + fused dot, BiCGSTAB)", "bound": "hbm",
-            "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-            "frac": achieved / hbm if achieved else None, "traffic": traffic,
+    # live samples: BiCGSTAB SpMV and the finest-level AMG cycle kernels
+    def live(launches, ms, nbytes):
+        if not launches:
+            return None, None, None
+        avg_ms, avg_b = ms / launches, nbytes / launches
+        return avg_b / (avg_ms * 1e-3) / 1e9, avg_ms, avg_b
+
+    spmv_gbs, spmv_ms, spmv_bytes = live(prof.fp64_launches, prof.fp64_ms, prof.fp64_bytes)
+    post_gbs, post_ms, post_bytes = live(prof.amg_post_launches, prof.amg_post_ms, prof.amg_post_bytes)
+    pre_gbs, pre_ms, pre_bytes = live(prof.amg_pre_launches, prof.amg_pre_ms, prof.amg_pre_bytes)
+
+    def traffic_for(name, nbytes):
+        # DRAM bytes of one launch measured by ncu on a case larger than L2, scaled to this
+        # launch by its algorithmic bytes (traffic grows in proportion to them: no re-reads)
+        f = os.path.join(ROOT, "profiles", name)
+        if nbytes is None or not os.path.exists(f):
+            return None
+        with open(f) as fh:
+            return json.load(fh)["traffic_per_algorithmic_byte"] * nbytes
+
+    spmv = {"kernel": "spmv_kernel<double,1> (SELL-32 SpMV + fused dot, BiCGSTAB v = A y)", "bound": "hbm",
+            "achieved": spmv_gbs, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": spmv_gbs / hbm if spmv_gbs else None,
+            "traffic": traffic_for("spmv_fp64_traffic.json", spmv_bytes),
             "algorithmic_bytes_per_launch": spmv_bytes, "avg_launch_ms": spmv_ms,
             "sampled_launches": prof.fp64_launches}
-
+    if post_gbs:
+        roof = {"kernel": "post_kernel<double,1> (AMG finest level: prolongation + post-smoothing SpMV)",
+                "bound": "hbm", "achieved": post_gbs, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": post_gbs / hbm, "traffic": traffic_for("amg_post_fp64_traffic.json", post_bytes),
+                "algorithmic_bytes_per_launch": post_bytes, "avg_launch_ms": post_ms,
+                "sampled_launches": prof.amg_post_launches,
+                "pre_kernel": {"achieved": pre_gbs, "frac": pre_gbs / hbm if pre_gbs else None,
+                               "avg_launch_ms": pre_ms, "algorithmic_bytes_per_launch": pre_bytes,
+                               "sampled_launches": prof.amg_pre_launches}}
+    else:
+        roof = spmv
     extra = {}
     if rank == 0 and not args.skip_transport:
         nt = args.transport_n
         tmesh = transport_mesh(lib, nt)
         ref = transport_exact(tmesh)
-        r64 = transport_time_to_tol(tmesh, A.PREC_FP64, ref)
-        r32 = transport_time_to_tol(tmesh, A.PREC_MIXED, ref)
+        r64 = transport_time_to_tol(tmesh, A.PREC_FP64, ref, preconditioner="amg")
+        r32 = transport_time_to_tol(tmesh, A.PREC_MIXED, ref, preconditioner="amg")
+        rj = transport_time_to_tol(tmesh, A.PREC_FP64, ref, preconditioner="jacobi")
         extra["s_to_1e8"] = {"workload": f"{nt}^3 hexes jittered +-0.2h (seed 3), U = (sin pi x cos pi y, "
                                          f"-cos pi x sin pi y, 0), kappa 1e-3, LinearUpwind + Corrected, "
-                                         f"T fixed 1/0 at x=0/1; one step() of the system assembled at T=0",
-                             "fp64": r64, "mixed": r32,
+                                         f"T fixed 1/0 at x=0/1; one step() of the system assembled at T=0 "
+                                         f"(assembly, AMG setup and iterations timed)",
+                             "fp64": r64, "mixed": r32, "fp64_jacobi": rj,
                              "speedup": r64["seconds"] / r32["seconds"] if r32["seconds"] > 0 else None,
-                             "reference_solution": "FP64 BiCGSTAB to ||b-Ax|| <= 1e-14 ||b||"}
+                             "speedup_vs_fp64_jacobi": rj["seconds"] / r32["seconds"] if r32["seconds"] > 0 else None,
+                             "reference_solution": "FP64 BiCGSTAB(Jacobi) to ||b-Ax|| <= 1e-14 ||b||"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -340,11 +363,11 @@ def run_ours(args, world, rank, local):
                 "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": f"cavity SIMPLE {N_CAVITY}x{N_CAVITY}x1 ({n} cells), Re=100, Upwind + "
-                                       "Corrected, urf 0.7/0.3, BiCGSTAB(Jacobi) to 1e-12",
+                                       "Corrected, urf 0.7/0.3, BiCGSTAB (AMG-preconditioned, PRISM_PC_AUTO) to 1e-12",
                            "cells": n, "l2": "inputs larger than L2 (no flush)",
                            "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                            "mesh_build_s": t_build},
-                "spmv_gbs": achieved, "roofline": roof, "clocks": clk,
+                "spmv_gbs": spmv_gbs, "roofline": roof, "spmv": spmv, "clocks": clk,
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(hU.nbytes + hp.nbytes),
                         "d2h_bytes_per_step": int(hU.nbytes + hp.nbytes)},
                 "gpu_launches": int(prof.kernel_launches), "cpu_baseline": cpu,

@@ -337,7 +337,14 @@ int prism_needs_pressure_reference(PrismScalar* p, int32_t* out);
  * with CUDA events on the launching stream while a profiling window is open.
  * bytes are the algorithmic bytes of the sampled launches:
  * nnz*(value + 4) + 4*(n+1) + 2*n*value (CSR values, columns, row pointers,
- * x read once, y written once). No counterpart in the reference. */
+ * x read once, y written once). The amg_* fields sample the two FP64 kernels
+ * of the AMG V-cycle on the finest level (pre-smoothing + residual, and
+ * prolongation + post-smoothing) with their algorithmic bytes:
+ *   pre:  nnz*12 + 4*(n+1) + 32*n        (matrix; b, D^-1 read; x, r written)
+ *   post: nnz*12 + 4*(n+1) + 36*n + 8*nc (matrix; b, x, D^-1, aggregate map read,
+ *                                          output written; coarse correction read)
+ * Iterations replayed from a CUDA graph are not sampled. No counterpart in the
+ * reference. */
 typedef struct {
     int64_t fp64_launches;
     double fp64_ms;
@@ -346,6 +353,12 @@ typedef struct {
     double fp32_ms;
     double fp32_bytes;
     int64_t kernel_launches; /* every kernel this library launched in the window */
+    int64_t amg_pre_launches;
+    double amg_pre_ms;
+    double amg_pre_bytes;
+    int64_t amg_post_launches;
+    double amg_post_ms;
+    double amg_post_bytes;
 } PrismProfile;
 int prism_profile_start(int32_t max_samples);
 int prism_profile_stop(PrismProfile* out);

@@ -107,7 +107,9 @@ class Report(C.Structure):
 class Profile(C.Structure):
     _fields_ = [("fp64_launches", i64), ("fp64_ms", f64), ("fp64_bytes", f64),
                 ("fp32_launches", i64), ("fp32_ms", f64), ("fp32_bytes", f64),
-                ("kernel_launches", i64)]
+                ("kernel_launches", i64),
+                ("amg_pre_launches", i64), ("amg_pre_ms", f64), ("amg_pre_bytes", f64),
+                ("amg_post_launches", i64), ("amg_post_ms", f64), ("amg_post_bytes", f64)]
 
 
 PP = C.POINTER(P)

@@ -22,6 +22,7 @@
 // solve refreshes the values from the current matrix.
 #include <cub/cub.cuh>
 
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <type_traits>
@@ -648,6 +649,15 @@ bool allocCycle(AmgLevel& L, bool mixed, cudaStream_t s) {
 
 }  // namespace
 
+namespace {
+// process-wide, so a hierarchy's buffers can never match the key of another
+// (destroyed) hierarchy that lived at the same address
+uint64_t nextGeneration() {
+    static std::atomic<uint64_t> g{0};
+    return ++g;
+}
+}  // namespace
+
 void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mixed, cudaStream_t s) {
     if (!built || levels.empty() || levels[0]->n != A.n || levels[0]->sl_off != A.sl_off) {
         levels.clear();
@@ -728,16 +738,16 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
                                          DENSE_MAX * DENSE_MAX * (int)sizeof(double)));
         }
         built = true;
-        ++generation;
+        generation = nextGeneration();
     } else if (levels[0]->vals != A.vals) {
         levels[0]->vals = A.vals;
-        ++generation;
+        generation = nextGeneration();
     }
     for (auto& L : levels)
-        if (allocCycle(*L, mixed, s)) ++generation;
+        if (allocCycle(*L, mixed, s)) generation = nextGeneration();
     if (mixed && coarse_inv.p && !coarse_inv32.p) {
         coarse_inv32.alloc(coarse_inv.n);
-        ++generation;
+        generation = nextGeneration();
     }
     has32 = mixed;
     // values of every level from the current matrix
@@ -786,7 +796,7 @@ Bufs<double> bufs64(AmgLevel& L) { return {L.b.p, L.x.p, L.x2.p, L.res.p, L.dinv
 Bufs<float> bufs32(AmgLevel& L) { return {L.b32.p, L.x32.p, L.x232.p, L.res32.p, L.dinv32.p}; }
 
 template <typename T>
-void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s) {
+void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s, bool sample) {
     AmgLevel& L = *A.levels[l];
     auto B = [&](AmgLevel& X) {
         if constexpr (sizeof(T) == 8) return bufs64(X);
@@ -822,25 +832,37 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
     }
     AmgLevel& N = *A.levels[l + 1];
     Bufs<T> nb = B(N);
+    const bool fine = sample && l == 0;
+    const double mat_bytes = (double)L.nnz * (sizeof(T) + 4) + 4.0 * (L.n + 1);
+    int slot = fine ? profBegin(PROF_AMG_PRE, sizeof(T) == 4, mat_bytes + 4.0 * sizeof(T) * L.n, s) : -1;
     withLpr(L.lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
         pre_kernel<T, P><<<grid((int64_t)L.n * P), BS, 0, s>>>(L.n, L.sl_off, L.sl_col, vals, b, lb.dinv, omega, lb.x,
                                                                lb.res, S);
     });
     countLaunch();
+    profEnd(slot, s);
     restrict_kernel<T><<<grid(N.n), BS, 0, s>>>(N.n, L.m_off.p, L.m_idx.p, lb.res, nb.b, S); countLaunch();
-    vcycle<T>(A, l + 1, nb.b, nb.x2, S, s);
+    vcycle<T>(A, l + 1, nb.b, nb.x2, S, s, false);
+    slot = fine ? profBegin(PROF_AMG_POST, sizeof(T) == 4,
+                            mat_bytes + (4.0 * sizeof(T) + 4.0) * L.n + (double)sizeof(T) * N.n, s)
+                : -1;
     withLpr(L.lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
         post_kernel<T, P><<<grid((int64_t)L.n * P), BS, 0, s>>>(L.n, L.sl_off, L.sl_col, vals, b, lb.x, nb.x2,
                                                                 L.agg.p, (T)A.scale, lb.dinv, omega, out, S);
     });
     countLaunch();
+    profEnd(slot, s);
 }
 
 }  // namespace
 
-void Amg::apply(const double* r, double* z, const KState* S, cudaStream_t s) { vcycle<double>(*this, 0, r, z, S, s); }
-void Amg::apply32(const float* r, float* z, const KState* S, cudaStream_t s) { vcycle<float>(*this, 0, r, z, S, s); }
+void Amg::apply(const double* r, double* z, const KState* S, cudaStream_t s, bool sample) {
+    vcycle<double>(*this, 0, r, z, S, s, sample);
+}
+void Amg::apply32(const float* r, float* z, const KState* S, cudaStream_t s) {
+    vcycle<float>(*this, 0, r, z, S, s, false);
+}
 
 }  // namespace pb

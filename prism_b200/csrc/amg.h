@@ -48,7 +48,7 @@ struct Amg {
     DevBuf<int> coarse_bad;
     bool built = false;
     bool has32 = false;
-    uint64_t generation = 0;  // bumped whenever a buffer of the hierarchy is (re)allocated
+    uint64_t generation = 0;  // new process-wide value whenever a buffer of the hierarchy is (re)allocated
     double omega = 0.67, scale = 1.5;
 
     // Build the hierarchy (first call) or refresh its values (later calls) for
@@ -58,7 +58,8 @@ struct Amg {
     // FP32 values of the finest level (valid after setup with mixed)
     const float* vals32() const { return levels.empty() ? nullptr : levels[0]->vals32.p; }
     // z = M^-1 r (one V(1,1) cycle); S (optional): skip the work once the solve has stopped
-    void apply(const double* r, double* z, const KState* S, cudaStream_t s);
+    // sample: time the finest-level kernels when a profiling window is open
+    void apply(const double* r, double* z, const KState* S, cudaStream_t s, bool sample = false);
     void apply32(const float* r, float* z, const KState* S, cudaStream_t s);
 };
 

@@ -24,6 +24,8 @@
 // delta (default 0.1) since the last flush; the FP64 true residual b - A'x' then
 // replaces the FP32 one and the recurrences continue with the Krylov space kept.
 // Convergence is only declared on an FP64 true residual.
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -491,7 +493,7 @@ void KrylovWork::ensurePrec(bool mixed) {
     if (fresh) PB_CUDA(cudaStreamSynchronize(nullptr));
 }
 KrylovWork::~KrylovWork() {
-    for (auto& g : graph)
+    for (auto& g : graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     if (host_state) cudaFreeHost(host_state);
 }
@@ -504,11 +506,13 @@ void spmv(const SellMatrix& A, const double* x, double* y, cudaStream_t s) {
 
 namespace {
 
-// ---- sampled SpMV timing (prism_profile_start / prism_profile_stop)
+// ---- sampled kernel timing (prism_profile_start / prism_profile_stop)
 struct Sample {
     cudaEvent_t a, b;
+    int kind;
     bool fp32;
     double bytes;
+    bool closed;
 };
 struct Profiler {
     bool on = false;
@@ -531,20 +535,6 @@ struct Profiler {
 template <typename T>
 double spmvBytes(const SellMatrix& A) {
     return (double)A.nnz_csr * (sizeof(T) + 4) + 4.0 * (A.n + 1) + 2.0 * A.n * sizeof(T);
-}
-template <typename T>
-bool sampleBegin(Sample& smp, const SellMatrix& A, cudaStream_t s) {
-    if (!g_prof.on || (int)g_prof.samples.size() >= g_prof.max_samples) return false;
-    smp.a = g_prof.get();
-    smp.b = g_prof.get();
-    smp.fp32 = sizeof(T) == 4;
-    smp.bytes = spmvBytes<T>(A);
-    PB_CUDA(cudaEventRecord(smp.a, s));
-    return true;
-}
-void sampleEnd(Sample& smp, cudaStream_t s) {
-    PB_CUDA(cudaEventRecord(smp.b, s));
-    g_prof.samples.push_back(smp);
 }
 
 template <typename T>
@@ -576,8 +566,12 @@ struct VerboseTimer {
 };
 
 // z = M^-1 r by one AMG V-cycle (FP64 or FP32 hierarchy)
-inline void precApply(Amg* amg, const double* r, double* z, const KState* S, cudaStream_t s) { amg->apply(r, z, S, s); }
-inline void precApply(Amg* amg, const float* r, float* z, const KState* S, cudaStream_t s) { amg->apply32(r, z, S, s); }
+inline void precApply(Amg* amg, const double* r, double* z, const KState* S, cudaStream_t s, bool sample) {
+    amg->apply(r, z, S, s, sample);
+}
+inline void precApply(Amg* amg, const float* r, float* z, const KState* S, cudaStream_t s, bool) {
+    amg->apply32(r, z, S, s);
+}
 
 // `count` BiCGSTAB iterations on the operator M (SELL values), launched one
 // kernel at a time. With amg: right-preconditioned, y = M^-1 p and z = M^-1 s.
@@ -592,18 +586,17 @@ void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T*
         p_kernel<T><<<vg, BS, 0, s>>>(n, V.p, V.r, V.v, S); countLaunch();
         const T* dp = V.p;
         if (amg) {
-            precApply(amg, V.p, y, S, s);
+            precApply(amg, V.p, y, S, s, sample);
             dp = y;
         }
-        Sample smp;
-        bool sampled = sample && sampleBegin<T>(smp, A, s);
+        const int slot = sample ? profBegin(PROF_SPMV, sizeof(T) == 4, spmvBytes<T>(A), s) : -1;
         spmv_kernel<T, 1><<<sg1, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, dp, V.v, V.r0, w.partials.p,
                                             w.counter.p, S); countLaunch();
-        if (sampled) sampleEnd(smp, s);
+        profEnd(slot, s);
         s_kernel<T><<<vg, BS, 0, s>>>(n, V.s, V.r, V.v, S); countLaunch();
         const T* ds = V.s;
         if (amg) {
-            precApply(amg, V.s, z, S, s);
+            precApply(amg, V.s, z, S, s, sample);
             ds = z;
         }
         spmv_kernel<T, 2><<<sg2, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, ds, V.t, V.s, w.partials.p,
@@ -633,18 +626,23 @@ void iterate(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, l
         iterateEager<T>(A, M, V, amg, y, z, batch, true, w, s);
         return;
     }
-    auto& g = w.graph[sizeof(T) == 4 ? 1 : 0];
-    std::vector<uintptr_t> key = {(uintptr_t)A.sl_off, (uintptr_t)A.col, (uintptr_t)A.nslices, (uintptr_t)A.n,
-                                  (uintptr_t)M, (uintptr_t)V.x, (uintptr_t)V.r, (uintptr_t)V.r0, (uintptr_t)V.p,
-                                  (uintptr_t)V.v, (uintptr_t)V.s, (uintptr_t)V.t, (uintptr_t)amg,
+    std::vector<uintptr_t> key = {(uintptr_t)sizeof(T), (uintptr_t)A.sl_off, (uintptr_t)A.col, (uintptr_t)A.nslices,
+                                  (uintptr_t)A.n, (uintptr_t)M, (uintptr_t)V.x, (uintptr_t)V.r, (uintptr_t)V.r0,
+                                  (uintptr_t)V.p, (uintptr_t)V.v, (uintptr_t)V.s, (uintptr_t)V.t, (uintptr_t)amg,
                                   (uintptr_t)(amg ? amg->generation : 0), (uintptr_t)y, (uintptr_t)z,
                                   (uintptr_t)w.state.p, (uintptr_t)w.partials.p, (uintptr_t)w.counter.p};
-    if (!g.exec || g.key != key) {
-        if (g.exec) {
-            cudaGraphExecDestroy(g.exec);
-            g.exec = nullptr;
+    constexpr size_t MAX_GRAPHS = 8;
+    auto hit = std::find_if(w.graphs.begin(), w.graphs.end(), [&](const KrylovWork::IterGraph& g) { return g.key == key; });
+    if (hit != w.graphs.end()) {
+        std::rotate(hit, hit + 1, w.graphs.end());  // most recently used last
+    } else {
+        if (w.graphs.size() >= MAX_GRAPHS) {
+            cudaGraphExecDestroy(w.graphs.front().exec);
+            w.graphs.erase(w.graphs.begin());
         }
+        KrylovWork::IterGraph ng;
         const long long c0 = launchCounter().load();
+        const auto t_cap = std::chrono::steady_clock::now();
         PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         cudaGraph_t graph = nullptr;
         try {
@@ -659,12 +657,17 @@ void iterate(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, l
         const long long k = launchCounter().load() - c0;
         launchCounter().fetch_sub(k);
         PB_CUDA(e);
-        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        e = cudaGraphInstantiate(&ng.exec, graph, 0);
         cudaGraphDestroy(graph);
         PB_CUDA(e);
-        g.key = key;
-        g.kernels = k;
+        ng.key = std::move(key);
+        ng.kernels = k;
+        w.graphs.push_back(std::move(ng));
+        if (verbose())
+            std::fprintf(stderr, "[prism] iteration graph captured: %lld kernels, %.3f ms\n", k,
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_cap).count());
     }
+    const KrylovWork::IterGraph& g = w.graphs.back();
     for (long long it = 0; it < batch; ++it) PB_CUDA(cudaGraphLaunch(g.exec, s));
     launchCounter().fetch_add(g.kernels * batch);
 }
@@ -848,6 +851,19 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
     return out;
 }
 
+int profBegin(int kind, bool fp32, double bytes, cudaStream_t s) {
+    if (!g_prof.on || (int)g_prof.samples.size() >= g_prof.max_samples) return -1;
+    Sample smp{g_prof.get(), g_prof.get(), kind, fp32, bytes, false};
+    PB_CUDA(cudaEventRecord(smp.a, s));
+    g_prof.samples.push_back(smp);
+    return (int)g_prof.samples.size() - 1;
+}
+void profEnd(int slot, cudaStream_t s) {
+    if (slot < 0 || slot >= (int)g_prof.samples.size()) return;
+    PB_CUDA(cudaEventRecord(g_prof.samples[slot].b, s));
+    g_prof.samples[slot].closed = true;
+}
+
 void profileStart(int max_samples) {
     for (auto& smp : g_prof.samples) {
         g_prof.pool.push_back(smp.a);
@@ -864,10 +880,21 @@ void profileStop(PrismProfile* out) {
     g_prof.on = false;
     out->kernel_launches = launchCounter().load() - g_prof.launches0;
     for (auto& smp : g_prof.samples) {
+        if (!smp.closed) continue;
         PB_CUDA(cudaEventSynchronize(smp.b));
         float ms = 0.f;
         PB_CUDA(cudaEventElapsedTime(&ms, smp.a, smp.b));
-        if (smp.fp32) {
+        if (smp.kind == PROF_AMG_PRE) {
+            if (smp.fp32) continue;
+            out->amg_pre_launches++;
+            out->amg_pre_ms += ms;
+            out->amg_pre_bytes += smp.bytes;
+        } else if (smp.kind == PROF_AMG_POST) {
+            if (smp.fp32) continue;
+            out->amg_post_launches++;
+            out->amg_post_ms += ms;
+            out->amg_post_bytes += smp.bytes;
+        } else if (smp.fp32) {
             out->fp32_launches++;
             out->fp32_ms += ms;
             out->fp32_bytes += smp.bytes;

@@ -20,9 +20,15 @@ struct SellMatrix {
 void jacobiStepNoAlloc(int64_t n, const int32_t* rowptr, const int32_t* col, const double* values, const double* b,
                        double* x, cudaStream_t stream);
 
-// Sampled CUDA-event timing of the BiCGSTAB SpMV launches (v = A p).
+// Sampled CUDA-event timing of the BiCGSTAB SpMV launches (v = A p) and of
+// the finest-level AMG cycle kernels.
 void profileStart(int max_samples);
 void profileStop(PrismProfile* out);
+enum ProfKind { PROF_SPMV = 0, PROF_AMG_PRE = 1, PROF_AMG_POST = 2 };
+// Opens a sample (records the start event on s) when a window is open and has
+// room: returns its slot, else -1. profEnd(slot) records the end event.
+int profBegin(int kind, bool fp32, double bytes, cudaStream_t s);
+void profEnd(int slot, cudaStream_t s);
 
 struct Amg;
 
@@ -53,13 +59,14 @@ struct KrylovWork {
     DevBuf<unsigned int> counter;
     DevBuf<KState> state;
     KState* host_state = nullptr;  // pinned
-    // one BiCGSTAB iteration captured as a CUDA graph, per precision ([0] FP64, [1] FP32),
-    // reused while the operands (key) stay the same
+    // one BiCGSTAB iteration captured as a CUDA graph, kept per operand set (key:
+    // precision, matrix, vectors, preconditioner), least recently used last out
     struct IterGraph {
         cudaGraphExec_t exec = nullptr;
         std::vector<uintptr_t> key;
         long long kernels = 0;  // kernel nodes per launch
-    } graph[2];
+    };
+    std::vector<IterGraph> graphs;
     void ensure(int n_pad, int64_t nnz_padded, bool mixed);
     ~KrylovWork();
 };

@@ -558,20 +558,27 @@ void solveImplicitMomentum(const PrismSIMPLEControls& c, std::vector<Transport*>
 }
 
 struct PressureResult {
-    std::unique_ptr<Scalar> pp;
-    std::unique_ptr<Tensor> D;
+    Scalar* pp;
+    Tensor* D;
 };
 
-// solvePressureEquation, SIMPLE.cpp:124-196
+// solvePressureEquation, SIMPLE.cpp:124-196. The reference builds p', the D
+// tensor and the pressure equation afresh on every call; here they live in the
+// mesh and are reset to exactly that fresh state (zero values, p's boundary
+// conditions, a new gradient cache, cleared coefficients), which keeps their
+// device buffers -- and the solver's captured iteration graphs -- across steps.
 PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transport*>& mom, Vector& U, Vector& mdot,
                                      Scalar& p, const PrismSolveOpts& so, std::vector<Report>& rep) {
     Mesh& m = *p.m;
     for (auto* eq : mom) eq->ensure();
     // pressureEquationCoeffsTensor, SIMPLE.cpp:77-108
-    auto D = std::make_unique<Tensor>();
-    D->m = &m;
-    D->diag = 1;
-    D->d.alloc(3 * (size_t)m.n_pad);
+    if (!m.p_D) {
+        m.p_D = std::make_unique<Tensor>();
+        m.p_D->m = &m;
+        m.p_D->diag = 1;
+        m.p_D->d.alloc(3 * (size_t)m.n_pad);
+    }
+    Tensor* D = m.p_D.get();
     D->d.zero(m.stream);
     launchDTensor(m.nc, m.pat.diag_pos.p, m.vol.p, mom[0]->A.p, mom[1]->A.p, mom.size() == 3 ? mom[2]->A.p : nullptr,
                   D->d.p, m.n_pad, m.stream);
@@ -585,38 +592,55 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
     launchRhieChow(m.view(), U.view(), D->view(), p.view(), mdot.fd.p, mdot.ff.p, m.stream);
     mdot.has_fd = mdot.has_ff = true;
     // p' named like p, zero valued, with a fresh gradient scheme (scalar.cpp:260-304)
-    auto pp = std::make_unique<Scalar>();
-    pp->m = &m;
+    if (!m.p_corr) {
+        m.p_corr = std::make_unique<Scalar>();
+        Scalar& q = *m.p_corr;
+        q.m = &m;
+        q.coord = -1;
+        q.v.alloc(m.n_pad);
+        q.bc_kind.alloc(std::max(m.npatch, 1));
+        q.bc_val.alloc(std::max(m.npatch, 1));
+        q.bc_vec.alloc(3 * std::max(m.npatch, 1));
+        q.grad = std::make_shared<GradState>();
+        q.grad->g.alloc(3 * (size_t)m.n_pad);
+        q.fv.alloc(std::max(m.nf, 1));
+    }
+    Scalar* pp = m.p_corr.get();
     pp->name = p.name;
-    pp->coord = -1;
     pp->bc = p.bc;
-    pp->v.alloc(m.n_pad);
+    pp->event = 0;
     pp->v.zero(m.stream);
-    pp->bc_kind.alloc(std::max(m.npatch, 1));
-    pp->bc_val.alloc(std::max(m.npatch, 1));
-    pp->bc_vec.alloc(3 * std::max(m.npatch, 1));
     PB_CUDA(cudaMemcpyAsync(pp->bc_kind.p, p.bc_kind.p, pp->bc_kind.n * sizeof(int), cudaMemcpyDeviceToDevice, m.stream));
     PB_CUDA(cudaMemcpyAsync(pp->bc_val.p, p.bc_val.p, pp->bc_val.n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
     PB_CUDA(cudaMemcpyAsync(pp->bc_vec.p, p.bc_vec.p, pp->bc_vec.n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
-    pp->grad = std::make_shared<GradState>();
     pp->grad->type = p.grad->type;
-    pp->grad->g.alloc(3 * (size_t)m.n_pad);
+    pp->grad->computed = std::numeric_limits<uint64_t>::max();
     pp->grad->g.zero(m.stream);
     // constrainPPrime, SIMPLE.cpp:43-75: every face value is 0 (Dirichlet/symmetry patches
     // are zeroed, the others take the owner value of the zero field)
     for (int q = 0; q < m.npatch; ++q)
         if (!m.h->patches[q].empty && !scalarHasHandler(pp->bc[q].kind)) noHandler(m, q, "prism::algo::constrainPPrime()");
-    pp->fv.alloc(std::max(m.nf, 1));
     pp->fv.zero(m.stream);
     pp->has_fv = true;
     if (c.p_ref_cell < 0 && needsPressureReference(*pp)) c.p_ref_cell = 0;
-    Transport pEqn;
-    pEqn.phi = pp.get();
+    if (!m.p_eq) m.p_eq = std::make_unique<Transport>();
+    Transport& pEqn = *m.p_eq;
+    pEqn.phi = pp;
+    pEqn.has_conv = 0;
+    pEqn.conv_scheme = 0;
+    pEqn.conv_first = 1;
     pEqn.has_diff = 1;
     pEqn.corrected = 1;
     pEqn.corrector = PRISM_CORR_OVER_RELAXED;
-    pEqn.kt = D.get();
+    pEqn.U = nullptr;
+    pEqn.ks = nullptr;
+    pEqn.kt = D;
+    pEqn.sources.clear();
     pEqn.sources.push_back({PRISM_SRC_DIVERGENCE, PRISM_SIGN_NEGATIVE, 0, nullptr, &mdot});
+    pEqn.symmetry = false;
+    pEqn.urf = 1.0;
+    pEqn.ensure();
+    zeroOutCoeffs(pEqn);
     if (!m.p_amg) m.p_amg = std::make_shared<Amg>();
     pEqn.amg = m.p_amg;
     for (int64_t i = 0; i <= c.non_ortho_correctors; ++i) {
@@ -625,7 +649,7 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
                        r.converged != 0});
     }
     pp->has_fv = false;  // clearFaceValues
-    return {std::move(pp), std::move(D)};
+    return {pp, D};
 }
 
 // correctFields, SIMPLE.cpp:218-241

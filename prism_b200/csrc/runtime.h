@@ -17,6 +17,10 @@
 
 namespace pb {
 
+struct Scalar;
+struct Tensor;
+struct Transport;
+
 struct Mesh {
     std::unique_ptr<HostMesh> h;
     cudaStream_t stream = nullptr;
@@ -33,6 +37,11 @@ struct Mesh {
     bool ls_ready = false;
     KrylovWork kw;
     std::shared_ptr<Amg> p_amg;  // AMG hierarchy of the pressure-correction equation (SIMPLE/PRIME/PISO)
+    // pressure-correction objects of SIMPLE/PRIME/PISO, reset on every step instead of
+    // re-created (their device buffers stay allocated between steps)
+    std::unique_ptr<Scalar> p_corr;
+    std::unique_ptr<Tensor> p_D;
+    std::unique_ptr<Transport> p_eq;
     DevBuf<double> scratch;  // n_faces doubles for face exports
 
     ~Mesh();
