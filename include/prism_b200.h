@@ -390,6 +390,45 @@ int prism_profile_stop(PrismProfile* out);
 int prism_jacobi_step_noalloc(int64_t n, const int32_t* rowptr, const int32_t* col, const double* values,
                               const double* b, double* x, void* stream);
 
+/* ---- steady fixed point and discrete adjoint ----------------------------- */
+/* A forward/backward pair shaped like a torch.autograd.Function for steady
+ * diffusion, -div(kappa grad phi) = f with a scalar kappa field, NonCorrected or
+ * Corrected diffusion (least-squares gradient), ConstantScalar sources and
+ * Fixed / ZeroGradient / FixedGradient / Symmetry / empty patches. No
+ * counterpart in the reference, whose users repeat ISolver::solve
+ * (numerics/solver.cpp:27-82) until the non-orthogonal correction settles.
+ *
+ * prism_adjoint_forward repeats prism_solve(eq, opts) -- assembly, relaxation,
+ * Krylov solve -- until the relative change ||phi_k - phi_{k-1}|| / ||phi_k||
+ * is <= outer_tol (at most max_outer times). At that fixed point
+ * R(phi, kappa, v) = A phi - b = 0, v being the Dirichlet face values.
+ *
+ * prism_adjoint_backward takes dJ/dphi (host, n_cells) for an objective J(phi)
+ * and solves the adjoint (dR/dphi)^T lambda = dJ/dphi at the current phi by
+ * the transposed deferred correction A^T lambda_{k+1} = dJ/dphi + C^T lambda_k
+ * (C: the correction terms' dependence on phi; one transposed BiCGSTAB solve
+ * per step, opts select precision-independent FP64 Krylov settings and the
+ * preconditioner), stopping like the forward. It writes
+ *   dJ_dkappa[c] = dJ/dkappa_c (host, n_cells), and, when dJ_dface != NULL,
+ *   dJ_dface[f]  = dJ/dv_f for every boundary face f < n_boundary_faces (the
+ *                  value seen by the diffusion Fixed handler and the gradient:
+ *                  the face value of prism_scalar_set_face_values, else the
+ *                  patch value; 0 on empty patches and faces without a value).
+ * The equation's coefficients are cleared on return. PRISM_BAD_ARG for other
+ * equations (convection, tensor kappa, Green-Gauss with Corrected, ...). */
+typedef struct {
+    int64_t outer_iterations;
+    int64_t krylov_iterations;
+    double final_change;  /* relative change of the last outer step */
+    int32_t converged;
+    int32_t status;       /* first non-OK Krylov status, else PRISM_OK */
+} PrismFixedPointResult;
+int prism_adjoint_forward(PrismTransport* eq, const PrismSolveOpts* opts, int32_t max_outer, double outer_tol,
+                          PrismFixedPointResult* result);
+int prism_adjoint_backward(PrismTransport* eq, const double* dJ_dphi, double* dJ_dkappa, double* dJ_dface,
+                           const PrismSolveOpts* opts, int32_t max_outer, double outer_tol,
+                           PrismFixedPointResult* result);
+
 #ifdef __cplusplus
 }
 #endif

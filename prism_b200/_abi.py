@@ -104,6 +104,11 @@ class Report(C.Structure):
                 ("final_residual", f64), ("converged", i32)]
 
 
+class FixedPointResult(C.Structure):
+    _fields_ = [("outer_iterations", i64), ("krylov_iterations", i64), ("final_change", f64),
+                ("converged", i32), ("status", i32)]
+
+
 class Profile(C.Structure):
     _fields_ = [("fp64_launches", i64), ("fp64_ms", f64), ("fp64_bytes", f64),
                 ("fp32_launches", i64), ("fp32_ms", f64), ("fp32_bytes", f64),
@@ -164,6 +169,9 @@ SIGNATURES = {
     "profile_start": (C.c_int, [i32]),
     "profile_stop": (C.c_int, [C.POINTER(Profile)]),
     "jacobi_step_noalloc": (C.c_int, [i64, P, P, P, P, P, P]),
+    "adjoint_forward": (C.c_int, [P, C.POINTER(SolveOpts), i32, f64, C.POINTER(FixedPointResult)]),
+    "adjoint_backward": (C.c_int, [P, pf64, pf64, pf64, C.POINTER(SolveOpts), i32, f64,
+                                   C.POINTER(FixedPointResult)]),
 }
 
 
@@ -176,7 +184,7 @@ class PrismError(RuntimeError):
         self.status = status
 
 
-GPU_ONLY = {"profile_start", "profile_stop", "jacobi_step_noalloc"}
+GPU_ONLY = {"profile_start", "profile_stop", "jacobi_step_noalloc", "adjoint_forward", "adjoint_backward"}
 
 
 class Bound:

@@ -536,3 +536,46 @@ def needs_pressure_reference(p: Scalar) -> bool:
     out = C.c_int32()
     p.lib.check(p.lib.needs_pressure_reference(p.h, C.byref(out)))
     return bool(out.value)
+
+
+# ---- steady fixed point and discrete adjoint ------------------------------------------
+@dataclass
+class FixedPointResult:
+    outer_iterations: int
+    krylov_iterations: int
+    final_change: float
+    converged: bool
+    status: int
+
+
+def _fixed_point(r):
+    return FixedPointResult(r.outer_iterations, r.krylov_iterations, r.final_change, bool(r.converged), r.status)
+
+
+def adjoint_forward(eqn: Transport, solver: Optional[_Solver] = None, max_outer=100,
+                    outer_tol=1e-13) -> FixedPointResult:
+    """Repeat solver.solve(eqn, n_iter=1) until ||phi_k - phi_{k-1}|| <= outer_tol ||phi_k||: the
+    steady state R(phi, kappa, v) = 0 whose adjoint adjoint_backward computes."""
+    solver = solver or BiCGSTAB()
+    o = solver.opts(eqn.lib, n_iter=1, eps=0.0)
+    r = A.FixedPointResult()
+    eqn.lib.check(eqn.lib.adjoint_forward(eqn.h, C.byref(o), int(max_outer), float(outer_tol), C.byref(r)))
+    return _fixed_point(r)
+
+
+def adjoint_backward(eqn: Transport, dJ_dphi, solver: Optional[_Solver] = None, max_outer=100,
+                     outer_tol=1e-13):
+    """Discrete adjoint of the steady diffusion eqn at its current field: returns
+    (dJ/dkappa per cell, dJ/dv per boundary face, FixedPointResult) for dJ/dphi."""
+    solver = solver or BiCGSTAB()
+    mesh = eqn.phi.mesh
+    dJ = np.ascontiguousarray(dJ_dphi, dtype=np.float64)
+    if dJ.shape != (mesh.n_cells,):
+        raise ValueError("dJ_dphi must have one value per cell")
+    gk = np.zeros(mesh.n_cells)
+    gv = np.zeros(max(1, mesh.info.n_boundary_faces))
+    o = solver.opts(eqn.lib, n_iter=1, eps=0.0)
+    r = A.FixedPointResult()
+    eqn.lib.check(eqn.lib.adjoint_backward(eqn.h, _f64p(dJ), _f64p(gk), _f64p(gv), C.byref(o), int(max_outer),
+                                           float(outer_tol), C.byref(r)))
+    return gk, gv[: mesh.info.n_boundary_faces], _fixed_point(r)

@@ -733,3 +733,33 @@ API int prism_jacobi_step_noalloc(int64_t n, const int32_t* rowptr, const int32_
                                   const double* b, double* x, void* stream) {
     return guard([&] { jacobiStepNoAlloc(n, rowptr, col, values, b, x, static_cast<cudaStream_t>(stream)); });
 }
+
+// ---- steady fixed point and discrete adjoint (see include/prism_b200.h)
+namespace {
+void writeFixedPoint(const FixedPointOut& f, PrismFixedPointResult* r) {
+    if (!r) return;
+    r->outer_iterations = f.outer;
+    r->krylov_iterations = f.krylov;
+    r->final_change = f.change;
+    r->converged = f.converged ? 1 : 0;
+    r->status = f.status;
+}
+}  // namespace
+API int prism_adjoint_forward(PrismTransport* pt, const PrismSolveOpts* o, int32_t max_outer, double outer_tol,
+                              PrismFixedPointResult* r) {
+    return guard([&] {
+        ARG(pt && max_outer > 0 && outer_tol >= 0.0, "bad argument");
+        FixedPointOut f = steadySolve(pt->eq, optsOrDefault(o), max_outer, outer_tol);
+        sync(*pt->eq.phi->m);
+        writeFixedPoint(f, r);
+    });
+}
+API int prism_adjoint_backward(PrismTransport* pt, const double* dJ, double* gk, double* gv, const PrismSolveOpts* o,
+                               int32_t max_outer, double outer_tol, PrismFixedPointResult* r) {
+    return guard([&] {
+        ARG(pt && dJ && gk && max_outer > 0 && outer_tol >= 0.0, "bad argument");
+        FixedPointOut f = adjointBackward(pt->eq, dJ, gk, gv, optsOrDefault(o), max_outer, outer_tol);
+        sync(*pt->eq.phi->m);
+        writeFixedPoint(f, r);
+    });
+}

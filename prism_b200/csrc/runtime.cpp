@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "adjoint.h"
 #include "coupling.h"
 #include "gradient.h"
 
@@ -727,6 +728,128 @@ void pisoStep(const PrismPISOControls& pc, std::vector<Transport*>& mom, Vector&
         for (int64_t j = 0; j < pc.momentum_implicit_steps; ++j) simpleStep(sc, mom, U, mdot, p, so, rep);
         for (int64_t j = 1; j < pc.pressure_correction_steps; ++j) primeStep(sc, mom, U, mdot, p, so, rep);
     }
+}
+
+}  // namespace pb
+
+namespace pb {
+
+// ------------------------------------------------------------------ steady fixed point + adjoint
+FixedPointOut steadySolve(Transport& eq, const PrismSolveOpts& o, int max_outer, double outer_tol) {
+    Scalar& phi = *eq.phi;
+    Mesh& m = *phi.m;
+    FixedPointOut out;
+    DevBuf<double> prev(m.n_pad), scratch(2 * NUM_SMS * 8 + 2);
+    double h[2];
+    for (int it = 0; it < max_outer; ++it) {
+        PB_CUDA(cudaMemcpyAsync(prev.p, phi.v.p, m.nc * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+        PrismSolveResult r = solve(eq, o);
+        out.krylov += r.krylov_iterations;
+        ++out.outer;
+        if (r.status != PRISM_OK && out.status == PRISM_OK) out.status = r.status;
+        diffNorms(m.nc, phi.v.p, prev.p, scratch.p, nullptr, scratch.p + 2 * NUM_SMS * 8, h, m.stream);
+        out.change = h[1] > 0 ? std::sqrt(h[0] / h[1]) : std::sqrt(h[0]);
+        if (!std::isfinite(out.change)) {
+            out.status = PRISM_NONFINITE;
+            break;
+        }
+        if (out.change <= outer_tol) {
+            out.converged = true;
+            break;
+        }
+    }
+    return out;
+}
+
+namespace {
+void checkAdjointSupported(const Transport& eq) {
+    const Scalar& phi = *eq.phi;
+    if (!eq.has_diff || eq.has_conv || !eq.ks || eq.kt || eq.symmetry)
+        fail(PRISM_BAD_ARG, "adjoint: only a diffusion equation with a scalar kappa field is supported");
+    if (phi.coord >= 0) fail(PRISM_BAD_ARG, "adjoint: the field must be a scalar field");
+    if (eq.corrected && phi.grad->type != PRISM_GRAD_LEAST_SQUARES)
+        fail(PRISM_BAD_ARG, "adjoint: Corrected diffusion needs the least-squares gradient");
+    for (const auto& src : eq.sources)
+        if (src.kind != PRISM_SRC_CONSTANT) fail(PRISM_BAD_ARG, "adjoint: only ConstantScalar sources are supported");
+}
+}  // namespace
+
+FixedPointOut adjointBackward(Transport& eq, const double* dJ, double* gk, double* gv, const PrismSolveOpts& o,
+                              int max_outer, double outer_tol) {
+    checkAdjointSupported(eq);
+    Scalar& phi = *eq.phi;
+    Mesh& m = *phi.m;
+    cudaStream_t s = m.stream;
+    FixedPointOut out;
+    m.ensureLeastSquares();
+    if (!m.cf_twin) {
+        m.cf_twin.alloc(std::max<size_t>(m.h->cf_face.size(), 1));
+        buildTwin(m.view(), m.cf_twin.p, s);
+    }
+    if (!m.tpos) {
+        m.tpos.alloc(std::max<int64_t>(m.pat.sell_nnz, 1));
+        buildTransposePositions(m.nc, m.pat.nslices, m.pat.rowptr.p, m.pat.sl_off.p, m.pat.sl_col.p, m.tpos.p, s);
+    }
+    // A at the current phi (a clean assembly), then A^T in the same pattern
+    zeroOutCoeffs(eq);
+    updateCoeffs(eq);
+    if (eq.corrected) ensureGradient(phi);
+    if (!eq.AT) eq.AT.alloc(std::max<int64_t>(m.pat.sell_nnz, 1));
+    transposeValues(m.pat.sell_nnz, m.tpos.p, eq.A.p, eq.AT.p, s);
+    SellMatrix AT = m.matrix(eq.AT.p);
+
+    AdjointParams P{};
+    P.m = m.view();
+    P.phi = phi.view();
+    P.ks = eq.ks->view();
+    P.pinv = m.ls_pinv.p;
+    P.w = m.ls_w.p;
+    P.nk = (int64_t)m.h->cf_face.size();
+    P.twin = m.cf_twin.p;
+    P.corrected = eq.corrected;
+    P.corrector = eq.corrector;
+
+    const int64_t np = m.n_pad;
+    DevBuf<double> d_dJ(np), lam(np), lam_prev(np), rhs(np), u(3 * np), d(np), d_gk(np), d_gv(std::max(m.nb, 1)),
+        scratch(2 * NUM_SMS * 8 + 2);
+    for (auto* b : {&d_dJ, &lam, &lam_prev, &rhs, &u, &d, &d_gk}) b->zero(s);
+    d_dJ.upload(dJ, m.nc, s);
+
+    Amg* amg = nullptr;
+    if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
+        if (!eq.amg_adj) eq.amg_adj = std::make_shared<Amg>();
+        amg = eq.amg_adj.get();
+    }
+    const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
+    const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
+    double h[2];
+    for (int it = 0; it < max_outer; ++it) {
+        adjointCorrection(P, lam.p, u.p, d.p, np, s);
+        adjointRhs(P, d_dJ.p, lam.p, u.p, d.p, np, rhs.p, s);
+        PB_CUDA(cudaMemcpyAsync(lam_prev.p, lam.p, m.nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        KrylovOut k = bicgstab(AT, rhs.p, lam.p, ktol, kmax, PRISM_PREC_FP64, 0.1, m.kw, s, amg, m.pat.rowptr.p,
+                               m.pat.col.p);
+        out.krylov += k.iterations;
+        ++out.outer;
+        if (k.status != PRISM_OK && out.status == PRISM_OK) out.status = k.status;
+        diffNorms(m.nc, lam.p, lam_prev.p, scratch.p, nullptr, scratch.p + 2 * NUM_SMS * 8, h, s);
+        out.change = h[1] > 0 ? std::sqrt(h[0] / h[1]) : std::sqrt(h[0]);
+        if (!std::isfinite(out.change)) {
+            out.status = PRISM_NONFINITE;
+            break;
+        }
+        if (out.change <= outer_tol || !eq.corrected) {
+            out.converged = true;
+            break;
+        }
+    }
+    adjointCorrection(P, lam.p, u.p, d.p, np, s);
+    adjointGradients(P, lam.p, u.p, np, d_gk.p, d_gv.p, s);
+    d_gk.download(gk, m.nc, s);
+    if (gv) d_gv.download(gv, m.nb, s);
+    PB_CUDA(cudaStreamSynchronize(s));
+    zeroOutCoeffs(eq);
+    return out;
 }
 
 }  // namespace pb

@@ -36,6 +36,7 @@ struct Mesh {
     DevBuf<double> ls_pinv, ls_w;
     bool ls_ready = false;
     KrylovWork kw;
+    DevBuf<int> cf_twin, tpos;  // adjoint: twin cell-face entries, transpose positions (built on first use)
     std::shared_ptr<Amg> p_amg;  // AMG hierarchy of the pressure-correction equation (SIMPLE/PRIME/PISO)
     // pressure-correction objects of SIMPLE/PRIME/PISO, reset on every step instead of
     // re-created (their device buffers stay allocated between steps)
@@ -110,6 +111,9 @@ struct Transport {
     bool clean = true;
     DevBuf<double> A, b, bconv, bdiff;
     std::shared_ptr<Amg> amg;  // AMG hierarchy (PRISM_PC_AMG), built on the first solve
+    // adjoint: A^T values and the AMG hierarchy of A^T
+    DevBuf<double> AT;
+    std::shared_ptr<Amg> amg_adj;
     void ensure();
 };
 
@@ -134,6 +138,21 @@ void primeStep(const PrismSIMPLEControls& c, std::vector<Transport*>& mom, Vecto
 void pisoStep(const PrismPISOControls& c, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
               const PrismSolveOpts& so, std::vector<Report>& rep);
 bool needsPressureReference(const Scalar& p);
+
+// Steady fixed point of repeated solve() calls and its discrete adjoint (pure
+// diffusion with a scalar kappa). steadySolve repeats solve(eq, o) until the
+// relative change of phi is <= outer_tol; adjointBackward solves the transposed
+// problem at the current phi for dJ/dphi (host, n cells) and writes dJ/dkappa
+// (host, n cells) and dJ/d(boundary face value) (host, n boundary faces, or null).
+struct FixedPointOut {
+    int64_t outer = 0, krylov = 0;
+    double change = 0.0;
+    bool converged = false;
+    int status = PRISM_OK;
+};
+FixedPointOut steadySolve(Transport& eq, const PrismSolveOpts& o, int max_outer, double outer_tol);
+FixedPointOut adjointBackward(Transport& eq, const double* dJ, double* gk, double* gv, const PrismSolveOpts& o,
+                              int max_outer, double outer_tol);
 void simpleDefaults(PrismSIMPLEControls* c);
 void pisoDefaults(PrismPISOControls* c);
 void solveDefaults(PrismSolveOpts* o);

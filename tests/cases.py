@@ -186,3 +186,34 @@ def transport_c3(n, lib, conv="MUSCL", jitter=0.2, seed=3, kappa=1e-3):
     k = api.Scalar("kappa", mesh, kappa)
     eqn = api.Transport(getattr(api.convection, conv)(U, T), api.diffusion.Corrected(k, T))
     return mesh, T, U, eqn
+
+
+def adjoint_c5(n, lib, seed=5, corrected=True):
+    """Steady diffusion for the adjoint: n^3 unit cubes x 6 tets (Kuhn split) on the unit cube,
+    kappa ~ lognormal(0, 0.5) per cell, T Fixed on all six walls with face values ~ U(0, 1) per
+    boundary face, target T* ~ N(0, 1) per cell; Corrected (or NonCorrected) diffusion with the
+    least-squares gradient. J = sum_c V_c (T_c - T*_c)^2.
+    Returns dict(mesh, T, kappa, eqn, kappa0, v0, T_star, vol)."""
+    unv = meshgen.box_tet(n, n, n)
+    case = box_case({"T": {p: ("fixed", 0.0) for p in meshgen.PATCHES}})
+    mesh = api.Mesh(unv, case, lib=lib)
+    rng = np.random.default_rng(seed)
+    nc, nb = mesh.n_cells, mesh.info.n_boundary_faces
+    kappa0 = rng.lognormal(0.0, 0.5, nc)
+    v0 = rng.uniform(0.0, 1.0, nb)
+    T_star = rng.normal(0.0, 1.0, nc)
+    T = api.Scalar("T", mesh, 0.0)
+    fv = np.zeros(mesh.n_faces)
+    fv[:nb] = v0
+    T.set_face_values(fv)
+    kappa = api.Scalar("kappa", mesh, kappa0)
+    scheme = api.diffusion.Corrected if corrected else api.diffusion.NonCorrected
+    eqn = api.Transport(scheme(kappa, T))
+    vol = mesh.export()["cell_volume"]
+    return dict(mesh=mesh, T=T, kappa=kappa, eqn=eqn, kappa0=kappa0, v0=v0, T_star=T_star, vol=vol)
+
+
+def objective(T, T_star, vol):
+    """J = sum_c V_c (T_c - T*_c)^2 and dJ/dT."""
+    r = T - T_star
+    return float(np.sum(vol * r * r)), 2.0 * vol * r
