@@ -390,6 +390,25 @@ int prism_profile_stop(PrismProfile* out);
 int prism_jacobi_step_noalloc(int64_t n, const int32_t* rowptr, const int32_t* col, const double* values,
                               const double* b, double* x, void* stream);
 
+/* ---- batched solves --------------------------------------------------------- */
+/* Many independent equations (any meshes on this GPU) solved together: each is
+ * assembled and relaxed as in prism_solve, then every system is solved in one
+ * persistent launch -- BiCGSTAB with Jacobi preconditioning per system, FP32
+ * inner iterations with FP64 dot products (precision PRISM_PREC_MIXED) or FP64
+ * ones, each inner solve reducing its residual by inner_tol (default 1e-4 mixed)
+ * between FP64 refinement steps, until ||b - Ax|| <= krylov_tol ||b|| (default
+ * 1e-12). The launch shape is autotuned on the first call for a set of
+ * patterns and kept in the handle with the concatenated pattern, so repeated
+ * calls on the same meshes reuse both. results[i] follows prism_solve with
+ * n_iter = 1 (iterations = 1, scaled residuals before and after). The method
+ * must be PRISM_SOLVER_BICGSTAB and ref_cell -1. No counterpart in the
+ * reference. */
+typedef struct PrismBatch PrismBatch;
+int prism_batch_create(PrismBatch** out);
+void prism_batch_destroy(PrismBatch* batch);
+int prism_batch_solve(PrismBatch* batch, PrismTransport* const* eqs, int32_t n, const PrismSolveOpts* opts,
+                      PrismSolveResult* results);
+
 /* ---- steady fixed point and discrete adjoint ----------------------------- */
 /* A forward/backward pair shaped like a torch.autograd.Function for steady
  * diffusion, -div(kappa grad phi) = f with a scalar kappa field, NonCorrected or

@@ -170,6 +170,9 @@ SIGNATURES = {
     "profile_stop": (C.c_int, [C.POINTER(Profile)]),
     "jacobi_step_noalloc": (C.c_int, [i64, P, P, P, P, P, P]),
     "adjoint_forward": (C.c_int, [P, C.POINTER(SolveOpts), i32, f64, C.POINTER(FixedPointResult)]),
+    "batch_create": (C.c_int, [C.POINTER(P)]),
+    "batch_destroy": (None, [P]),
+    "batch_solve": (C.c_int, [P, PP, i32, C.POINTER(SolveOpts), C.POINTER(SolveResult)]),
     "adjoint_backward": (C.c_int, [P, pf64, pf64, pf64, C.POINTER(SolveOpts), i32, f64,
                                    C.POINTER(FixedPointResult)]),
 }
@@ -184,7 +187,8 @@ class PrismError(RuntimeError):
         self.status = status
 
 
-GPU_ONLY = {"profile_start", "profile_stop", "jacobi_step_noalloc", "adjoint_forward", "adjoint_backward"}
+GPU_ONLY = {"profile_start", "profile_stop", "jacobi_step_noalloc", "adjoint_forward", "adjoint_backward",
+            "batch_create", "batch_destroy", "batch_solve"}
 
 
 class Bound:

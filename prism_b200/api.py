@@ -579,3 +579,30 @@ def adjoint_backward(eqn: Transport, dJ_dphi, solver: Optional[_Solver] = None, 
     eqn.lib.check(eqn.lib.adjoint_backward(eqn.h, _f64p(dJ), _f64p(gk), _f64p(gv), C.byref(o), int(max_outer),
                                            float(outer_tol), C.byref(r)))
     return gk, gv[: mesh.info.n_boundary_faces], _fixed_point(r)
+
+
+# ---- batched solves ------------------------------------------------------------------
+class BatchSolver:
+    """Independent equations solved together in one persistent launch
+    (prism_batch_solve): solve(eqns) ~ [solver.solve(e, n_iter=1) for e in eqns]."""
+
+    def __init__(self, solver: Optional[_Solver] = None, lib=None):
+        self.solver = solver or BiCGSTAB(precision=A.PREC_MIXED)
+        self.lib = lib or _default_lib()
+        h = C.c_void_p()
+        self.lib.check(self.lib.batch_create(C.byref(h)))
+        self.h = h
+
+    def solve(self, eqns, eps=1e-7, clear_coeffs=True):
+        n = len(eqns)
+        arr = (C.c_void_p * n)(*[e.h.value if isinstance(e.h, C.c_void_p) else e.h for e in eqns])
+        res = (A.SolveResult * n)()
+        o = self.solver.opts(self.lib, n_iter=1, eps=eps, clear_coeffs=clear_coeffs)
+        self.lib.check(self.lib.batch_solve(self.h, C.cast(arr, A.PP), n, C.byref(o), res))
+        return [SolverResult(r.iterations, r.initial_residual, r.final_residual, bool(r.converged), r.status,
+                             r.krylov_iterations, r.krylov_rel_residual) for r in res]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.batch_destroy(self.h)
+            self.h = None

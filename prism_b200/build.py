@@ -25,7 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-O2"]
 NO_FMA = {"assemble.cu", "gradient.cu", "coupling.cu", "pattern.cu", "adjoint.cu"}
 SOURCES = ["mesh_build.cpp", "runtime.cpp", "capi.cpp", "pattern.cu", "assemble.cu", "gradient.cu",
-           "coupling.cu", "krylov.cu", "amg.cu", "adjoint.cu", "noalloc.cu"]
+           "coupling.cu", "krylov.cu", "amg.cu", "adjoint.cu", "batched.cu", "noalloc.cu"]
 
 
 def nvcc():

@@ -25,6 +25,9 @@ struct PrismTensor {
 struct PrismTransport {
     Transport eq;
 };
+struct PrismBatch {
+    BatchHandle h;
+};
 
 namespace {
 thread_local std::string g_last_error;
@@ -761,5 +764,28 @@ API int prism_adjoint_backward(PrismTransport* pt, const double* dJ, double* gk,
         FixedPointOut f = adjointBackward(pt->eq, dJ, gk, gv, optsOrDefault(o), max_outer, outer_tol);
         sync(*pt->eq.phi->m);
         writeFixedPoint(f, r);
+    });
+}
+
+// ---- batched solves (see include/prism_b200.h)
+API int prism_batch_create(PrismBatch** out) {
+    return guard([&] {
+        ARG(out, "null argument");
+        *out = new PrismBatch();
+    });
+}
+API void prism_batch_destroy(PrismBatch* b) { delete b; }
+API int prism_batch_solve(PrismBatch* b, PrismTransport* const* eqs, int32_t n, const PrismSolveOpts* o,
+                          PrismSolveResult* results) {
+    return guard([&] {
+        ARG(b && eqs && n > 0 && results, "bad argument");
+        std::vector<Transport*> v;
+        for (int32_t i = 0; i < n; ++i) {
+            ARG(eqs[i], "null equation");
+            v.push_back(&eqs[i]->eq);
+        }
+        auto r = solveBatch(b->h, v, optsOrDefault(o));
+        for (int32_t i = 0; i < n; ++i) results[i] = r[i];
+        for (auto* e : v) sync(*e->phi->m);
     });
 }

@@ -9,6 +9,7 @@
 
 #include "amg.h"
 #include "assemble.h"
+#include "batched.h"
 #include "common.h"
 #include "krylov.h"
 #include "mesh_build.h"
@@ -151,6 +152,16 @@ struct FixedPointOut {
     int status = PRISM_OK;
 };
 FixedPointOut steadySolve(Transport& eq, const PrismSolveOpts& o, int max_outer, double outer_tol);
+
+// Batched ISolver::solve(eq, n_iter = 1): every equation is assembled and
+// relaxed on its mesh, then all systems are solved together in one persistent
+// launch (batched.h) and each field receives its solution.
+struct BatchHandle {
+    BatchPlan plan;
+    cudaStream_t stream = nullptr;
+    ~BatchHandle();
+};
+std::vector<PrismSolveResult> solveBatch(BatchHandle& h, std::vector<Transport*>& eqs, const PrismSolveOpts& o);
 FixedPointOut adjointBackward(Transport& eq, const double* dJ, double* gk, double* gv, const PrismSolveOpts& o,
                               int max_outer, double outer_tol);
 void simpleDefaults(PrismSIMPLEControls* c);

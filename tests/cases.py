@@ -217,3 +217,23 @@ def objective(T, T_star, vol):
     """J = sum_c V_c (T_c - T*_c)^2 and dJ/dT."""
     r = T - T_star
     return float(np.sum(vol * r * r)), 2.0 * vol * r
+
+
+def batch_sizes(count, seed=4, nmin=16, nmax=96):
+    """Per-problem cube edge counts N = round(exp(U(ln nmin, ln nmax))) (seeded)."""
+    rng = np.random.default_rng(seed)
+    return [int(round(float(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))) for _ in range(count)]
+
+
+def diffusion_box(N, lib, seed):
+    """One batched problem: N^3 unit-cube hexes, kappa ~ lognormal(0, 1) per cell, f ~ N(0, 1) per
+    cell as ConstantScalar, T Fixed 0 on all walls, Corrected diffusion."""
+    unv = meshgen.box_hex(N, N, N)
+    case = box_case({"T": {p: ("fixed", 0.0) for p in meshgen.PATCHES}})
+    mesh = api.Mesh(unv, case, lib=lib)
+    rng = np.random.default_rng(seed)
+    kappa = api.Scalar("kappa", mesh, rng.lognormal(0.0, 1.0, mesh.n_cells))
+    f = api.Scalar("f", mesh, rng.normal(0.0, 1.0, mesh.n_cells))
+    T = api.Scalar("T", mesh, 0.0)
+    eqn = api.Transport(api.diffusion.Corrected(kappa, T), api.source.ConstantScalar(f))
+    return dict(mesh=mesh, T=T, kappa=kappa, f=f, eqn=eqn)
