@@ -207,8 +207,48 @@ __device__ __forceinline__ bool runSeek(const BP<T>& P, const int* pre, const in
     return true;
 }
 
+// Row sums of US consecutive units (chunks of one system) starting at R.v:
+// the slots of all units are walked together so that their loads overlap.
+template <typename T, int LPR, int US, typename V, typename F>
+__device__ __forceinline__ void spmvUnits(const BP<T>& P, const V* val, const Run& R, int nh, int lane, int* row,
+                                          int* chunk, double* sum, F xf) {
+    constexpr int RPC = 32 / LPR;
+    const int sub = lane % LPR;
+    int bo[US], w[US];
+    int wmax = 0;
+#pragma unroll
+    for (int u = 0; u < US; ++u) {
+        const int vu = R.v + (u < nh ? u : 0);
+        const int slice = R.slice0 + vu / LPR;
+        chunk[u] = slice * LPR + vu % LPR;
+        row[u] = 32 * slice + (vu % LPR) * RPC + lane / LPR;
+        const int s0 = P.sl_off[slice];
+        w[u] = u < nh ? (P.sl_off[slice + 1] - s0) >> 5 : 0;
+        bo[u] = s0 + (row[u] & 31);
+        sum[u] = 0.0;
+        wmax = max(wmax, w[u]);
+    }
+    for (int j = sub; j < wmax; j += LPR) {
+#pragma unroll
+        for (int u = 0; u < US; ++u)
+            if (j < w[u]) {
+                const int q = bo[u] + 32 * j;
+                sum[u] += (double)val[q] * xf(P.col[q]);
+            }
+    }
+    if constexpr (LPR > 1) {
+#pragma unroll
+        for (int u = 0; u < US; ++u)
+#pragma unroll
+            for (int o = LPR / 2; o > 0; o >>= 1) sum[u] += __shfl_xor_sync(0xffffffffu, sum[u], o);
+    }
+}
+
+// At most 64 registers per thread (2 blocks of 512 per SM): the sweeps are
+// latency-bound, so loads in flight (UR / US units per warp step) and
+// occupancy matter more than registers.
 template <typename T, int LPR>
-__global__ void batch_kernel(const BP<T> P) {
+__global__ void __launch_bounds__(MAX_BLOCK, 2) batch_kernel(const BP<T> P) {
     __shared__ double sh[2 * MAX_BLOCK / 32];
     extern __shared__ int lists[];  // pre (nprob + 1) | ids (nprob) | scan scratch (2 * blockDim + 2)
     int* pre = lists;
@@ -219,6 +259,8 @@ __global__ void batch_kernel(const BP<T> P) {
     const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     constexpr int RPC = 32 / LPR;  // rows per chunk (one warp)
+    constexpr int UR = 2;          // slices per warp step in the row sweeps
+    constexpr int US = LPR == 1 ? 2 : 1;  // units per warp step in the SpMV sweeps
     Run R;
 
     for (int step = 0; step < P.max_steps; ++step) {
@@ -328,37 +370,55 @@ __global__ void batch_kernel(const BP<T> P) {
         }
 
         // ---- one BiCGSTAB iteration of every system in an inner solve
-        // A: p = r + beta (p - omega v)
+        // A: p = r + beta (p - omega v)          (UR slices per warp step: loads first, then stores)
         if (runStart(P, pre, ids, m, total, 1, gwarp, nwarps, R)) {
             double beta = __ldcg(&P.st[R.pr].beta), omega = __ldcg(&P.st[R.pr].omega);
-            for (; R.v < R.vend; ++R.v) {
+            while (R.v < R.vend) {
                 if (runSeek(P, pre, ids, 1, R)) {
                     beta = __ldcg(&P.st[R.pr].beta);
                     omega = __ldcg(&P.st[R.pr].omega);
                 }
-                const int r = 32 * (R.slice0 + R.v) + lane;
-                if (r >= R.rows_end) continue;
-                P.p[r] = (T)((double)ld(P.r, r) + beta * ((double)ld(P.p, r) - omega * (double)ld(P.v, r)));
+                const int nh = min(UR, min(R.kend, R.vend) - R.v);
+                int rr[UR];
+                T a0[UR], a1[UR], a2[UR];
+#pragma unroll
+                for (int u = 0; u < UR; ++u) {
+                    rr[u] = 32 * (R.slice0 + R.v + u) + lane;
+                    if (u < nh && rr[u] < R.rows_end) {
+                        a0[u] = ld(P.r, rr[u]);
+                        a1[u] = ld(P.p, rr[u]);
+                        a2[u] = ld(P.v, rr[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < UR; ++u)
+                    if (u < nh && rr[u] < R.rows_end)
+                        P.p[rr[u]] = (T)((double)a0[u] + beta * ((double)a1[u] - omega * (double)a2[u]));
+                R.v += nh;
             }
         }
         grid.sync();
         // B: v = A' p ; r0.v
         if (runStart(P, pre, ids, m, total * LPR, LPR, gwarp, nwarps, R)) {
-            for (; R.v < R.vend; ++R.v) {
+            while (R.v < R.vend) {
                 runSeek(P, pre, ids, LPR, R);
-                const int slice = R.slice0 + R.v / LPR;
-                const int chunk = slice * LPR + R.v % LPR;
-                const int row = 32 * slice + (R.v % LPR) * RPC + lane / LPR, sub = lane % LPR;
-                const double av = rowDot<LPR>(P.sl_off, P.col, P.A, row, sub,
-                                              [&](int c) { return (double)ld(P.p, c); });
-                double t0 = 0.0;
-                if (row < R.rows_end && sub == 0) {
-                    const T vt = (T)av;
-                    P.v[row] = vt;
-                    t0 = (double)ld(P.r0, row) * (double)vt;
+                const int nh = min(US, min(R.kend, R.vend) - R.v);
+                int row[US], chunk[US];
+                double sum[US];
+                const int sub = lane % LPR;
+                spmvUnits<T, LPR, US>(P, P.A, R, nh, lane, row, chunk, sum, [&](int c) { return (double)ld(P.p, c); });
+#pragma unroll
+                for (int u = 0; u < US; ++u) {
+                    double t0 = 0.0;
+                    if (u < nh && row[u] < R.rows_end && sub == 0) {
+                        const T vt = (T)sum[u];
+                        P.v[row[u]] = vt;
+                        t0 = (double)ld(P.r0, row[u]) * (double)vt;
+                    }
+                    t0 = warpSum(t0);
+                    if (lane == 0 && u < nh) P.cdot[3 * chunk[u]] = t0;
                 }
-                t0 = warpSum(t0);
-                if (lane == 0) P.cdot[3 * chunk] = t0;
+                R.v += nh;
             }
         }
         grid.sync();
@@ -385,41 +445,61 @@ __global__ void batch_kernel(const BP<T> P) {
         if (runStart(P, pre, ids, m, total, 1, gwarp, nwarps, R)) {
             bool on = stateOf(P.st, R.pr) == S_INNER;
             double alpha = __ldcg(&P.st[R.pr].alpha);
-            for (; R.v < R.vend; ++R.v) {
+            while (R.v < R.vend) {
                 if (runSeek(P, pre, ids, 1, R)) {
                     on = stateOf(P.st, R.pr) == S_INNER;
                     alpha = __ldcg(&P.st[R.pr].alpha);
                 }
-                const int r = 32 * (R.slice0 + R.v) + lane;
-                if (!on || r >= R.rows_end) continue;
-                P.s[r] = (T)((double)ld(P.r, r) - alpha * (double)ld(P.v, r));
+                const int nh = min(UR, min(R.kend, R.vend) - R.v);
+                if (on) {
+                    int rr[UR];
+                    T a0[UR], a1[UR];
+#pragma unroll
+                    for (int u = 0; u < UR; ++u) {
+                        rr[u] = 32 * (R.slice0 + R.v + u) + lane;
+                        if (u < nh && rr[u] < R.rows_end) {
+                            a0[u] = ld(P.r, rr[u]);
+                            a1[u] = ld(P.v, rr[u]);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < UR; ++u)
+                        if (u < nh && rr[u] < R.rows_end) P.s[rr[u]] = (T)((double)a0[u] - alpha * (double)a1[u]);
+                }
+                R.v += nh;
             }
         }
         grid.sync();
         // E: t = A' s ; t.s, t.t
         if (runStart(P, pre, ids, m, total * LPR, LPR, gwarp, nwarps, R)) {
             bool on = stateOf(P.st, R.pr) == S_INNER;
-            for (; R.v < R.vend; ++R.v) {
+            while (R.v < R.vend) {
                 if (runSeek(P, pre, ids, LPR, R)) on = stateOf(P.st, R.pr) == S_INNER;
-                if (!on) continue;  // the same system in the whole warp
-                const int slice = R.slice0 + R.v / LPR;
-                const int chunk = slice * LPR + R.v % LPR;
-                const int row = 32 * slice + (R.v % LPR) * RPC + lane / LPR, sub = lane % LPR;
-                const double at = rowDot<LPR>(P.sl_off, P.col, P.A, row, sub,
-                                              [&](int c) { return (double)ld(P.s, c); });
-                double t0 = 0.0, t1 = 0.0;
-                if (row < R.rows_end && sub == 0) {
-                    const T tt = (T)at;
-                    P.t[row] = tt;
-                    t0 = (double)tt * (double)ld(P.s, row);
-                    t1 = (double)tt * (double)tt;
+                const int nh = min(US, min(R.kend, R.vend) - R.v);
+                if (on) {  // the same system in the whole warp
+                    int row[US], chunk[US];
+                    double sum[US];
+                    const int sub = lane % LPR;
+                    spmvUnits<T, LPR, US>(P, P.A, R, nh, lane, row, chunk, sum,
+                                          [&](int c) { return (double)ld(P.s, c); });
+#pragma unroll
+                    for (int u = 0; u < US; ++u) {
+                        double t0 = 0.0, t1 = 0.0;
+                        if (u < nh && row[u] < R.rows_end && sub == 0) {
+                            const T tt = (T)sum[u];
+                            P.t[row[u]] = tt;
+                            t0 = (double)tt * (double)ld(P.s, row[u]);
+                            t1 = (double)tt * (double)tt;
+                        }
+                        t0 = warpSum(t0);
+                        t1 = warpSum(t1);
+                        if (lane == 0 && u < nh) {
+                            P.cdot[3 * chunk[u]] = t0;
+                            P.cdot[3 * chunk[u] + 1] = t1;
+                        }
+                    }
                 }
-                t0 = warpSum(t0);
-                t1 = warpSum(t1);
-                if (lane == 0) {
-                    P.cdot[3 * chunk] = t0;
-                    P.cdot[3 * chunk + 1] = t1;
-                }
+                R.v += nh;
             }
         }
         grid.sync();
@@ -441,29 +521,49 @@ __global__ void batch_kernel(const BP<T> P) {
         if (runStart(P, pre, ids, m, total, 1, gwarp, nwarps, R)) {
             bool on = stateOf(P.st, R.pr) == S_INNER;
             double alpha = __ldcg(&P.st[R.pr].alpha), omega = __ldcg(&P.st[R.pr].omega);
-            for (; R.v < R.vend; ++R.v) {
+            while (R.v < R.vend) {
                 if (runSeek(P, pre, ids, 1, R)) {
                     on = stateOf(P.st, R.pr) == S_INNER;
                     alpha = __ldcg(&P.st[R.pr].alpha);
                     omega = __ldcg(&P.st[R.pr].omega);
                 }
-                if (!on) continue;  // the same system in the whole warp
-                const int row = 32 * (R.slice0 + R.v) + lane;
-                double t0 = 0.0, t1 = 0.0;
-                if (row < R.rows_end) {
-                    const double si = (double)ld(P.s, row);
-                    P.d[row] = (T)((double)ld(P.d, row) + alpha * (double)ld(P.p, row) + omega * si);
-                    const T rt = (T)(si - omega * (double)ld(P.t, row));
-                    P.r[row] = rt;
-                    t0 = (double)ld(P.r0, row) * (double)rt;
-                    t1 = (double)rt * (double)rt;
+                const int nh = min(UR, min(R.kend, R.vend) - R.v);
+                if (on) {  // the same system in the whole warp
+                    int rr[UR];
+                    T a0[UR], a1[UR], a2[UR], a3[UR], a4[UR];
+                    bool ok[UR];
+#pragma unroll
+                    for (int u = 0; u < UR; ++u) {
+                        rr[u] = 32 * (R.slice0 + R.v + u) + lane;
+                        ok[u] = u < nh && rr[u] < R.rows_end;
+                        if (ok[u]) {
+                            a0[u] = ld(P.s, rr[u]);
+                            a1[u] = ld(P.d, rr[u]);
+                            a2[u] = ld(P.p, rr[u]);
+                            a3[u] = ld(P.t, rr[u]);
+                            a4[u] = ld(P.r0, rr[u]);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < UR; ++u) {
+                        double t0 = 0.0, t1 = 0.0;
+                        if (ok[u]) {
+                            const double si = (double)a0[u];
+                            P.d[rr[u]] = (T)((double)a1[u] + alpha * (double)a2[u] + omega * si);
+                            const T rt = (T)(si - omega * (double)a3[u]);
+                            P.r[rr[u]] = rt;
+                            t0 = (double)a4[u] * (double)rt;
+                            t1 = (double)rt * (double)rt;
+                        }
+                        t0 = warpSum(t0);
+                        t1 = warpSum(t1);
+                        if (lane == 0 && u < nh) {
+                            P.sdot[2 * (R.slice0 + R.v + u)] = t0;
+                            P.sdot[2 * (R.slice0 + R.v + u) + 1] = t1;
+                        }
+                    }
                 }
-                t0 = warpSum(t0);
-                t1 = warpSum(t1);
-                if (lane == 0) {
-                    P.sdot[2 * (row >> 5)] = t0;
-                    P.sdot[2 * (row >> 5) + 1] = t1;
-                }
+                R.v += nh;
             }
         }
         grid.sync();
