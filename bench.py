@@ -2,7 +2,7 @@
 
 Headline workload (N=1): steady lid-driven cavity, Re=100 (nu=0.01, lid u=1),
 Upwind convection + Corrected diffusion + pressure-gradient source, SIMPLE with
-urf 0.7/0.3 (configs[1]'s recipe) on 1448x1448x1 hexes (2,096,704 cells): the
+urf 0.7/0.3 (the 512x512 cavity recipe) on 1448x1448x1 hexes (2,096,704 cells): the
 "2M-cell SIMPLE it/s" of the metric. One step = one SIMPLE outer iteration
 (2 momentum solves + 3 pressure solves, each step() solved to ||b-Ax|| <=
 1e-12 ||b|| like the reference's machine-precision step). Inputs live in HBM;
@@ -11,10 +11,13 @@ the working set (~1 GB) is larger than L2, so no flush is needed.
 Also reported: time to 1e-8 relative error of the 128^3 jittered-hex transport
 solve (LinearUpwind + Corrected), FP64 vs FP32/FP64-reliable-update BiCGSTAB,
 both AMG-preconditioned, and FP64 with the Jacobi preconditioner ("s_to_1e8"),
-and the live bandwidth of the dominant kernel (the finest-level AMG
+the live bandwidth of the dominant kernel (the finest-level AMG
 post-smoothing SpMV) and of the BiCGSTAB SpMV (CUDA events around sampled
-launches in the timed region). --impl reference times the CPU restatement of the
-reference (single-threaded, like the reference) on a bounded sample.
+launches in the timed region), the discrete adjoint of steady diffusion on
+64^3 x 6 tets ("adjoint": times and finite-difference agreement) and 256
+independent diffusion solves in one persistent launch ("batched").
+--impl reference times the CPU restatement of the reference
+(single-threaded, like the reference) on a bounded sample.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -225,6 +228,94 @@ def transport_time_to_tol(mesh, precision, ref, tol=1e-8, preconditioner="auto")
     return last
 
 
+def adjoint_measure(lib, n=64, directions=2):
+    """Discrete adjoint of steady diffusion on n^3 x 6 tets (kappa ~ lognormal(0, 0.5), Fixed face values
+    ~ U(0, 1), J = sum V (T - T*)^2): forward and backward times, and fourth-order central differences
+    of J along random directions against the adjoint gradient."""
+    import numpy as np
+    import torch
+    from prism_b200 import api
+    from tests import cases
+    t = time.perf_counter()
+    c = cases.adjoint_c5(n, lib)
+    t_build = time.perf_counter() - t
+    S = api.BiCGSTAB(krylov_tol=1e-13, krylov_max_iter=100000)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    fw = api.adjoint_forward(c["eqn"], S, max_outer=500, outer_tol=1e-13)
+    t_fw = time.perf_counter() - t
+    phi0 = c["T"].values()
+    _, dJ = cases.objective(phi0, c["T_star"], c["vol"])
+    t = time.perf_counter()
+    gk, gv, bw = api.adjoint_backward(c["eqn"], dJ, S, max_outer=500, outer_tol=1e-13)
+    t_bw = time.perf_counter() - t
+    rng = np.random.default_rng(32)
+    eps, errs = 1e-3, []
+    for _ in range(directions):
+        dk = rng.normal(size=c["mesh"].n_cells)
+        dv = rng.normal(size=len(c["v0"]))
+
+        def J_at(sgn):
+            c["kappa"].set_values(c["kappa0"] * (1 + sgn * eps * dk))
+            fv = np.zeros(c["mesh"].n_faces)
+            fv[: len(dv)] = c["v0"] + sgn * eps * dv
+            c["T"].set_face_values(fv)
+            c["T"].set_values(phi0)
+            api.adjoint_forward(c["eqn"], S, max_outer=500, outer_tol=1e-13)
+            return cases.objective(c["T"].values(), c["T_star"], c["vol"])[0]
+
+        fd = (8 * (J_at(1) - J_at(-1)) - (J_at(2) - J_at(-2))) / (12 * eps)
+        an = float(np.sum(gk * c["kappa0"] * dk) + np.sum(gv * dv))
+        errs.append(abs(fd - an) / abs(an))
+    return {"workload": f"{n}^3 cubes x 6 tets ({c['mesh'].n_cells} cells), kappa ~ lognormal(0,0.5), Fixed face "
+                        f"values ~ U(0,1), Corrected diffusion, least-squares gradient, J = sum V (T - T*)^2",
+            "mesh_build_s": t_build, "forward_s": t_fw, "forward_outer": fw.outer_iterations,
+            "forward_krylov": fw.krylov_iterations, "backward_s": t_bw, "backward_outer": bw.outer_iterations,
+            "backward_krylov": bw.krylov_iterations, "fd_rel_errors": errs,
+            "fd": f"fourth-order central differences, eps = {eps} (relative in kappa)"}
+
+
+def batched_measure(lib, count=256, nmin=16, nmax=96):
+    """count independent diffusion problems (N^3 hexes, N log-uniform in [nmin, nmax], seed 4) solved in one
+    persistent launch (mixed precision), against the same systems solved one by one (FP64, Jacobi)."""
+    import numpy as np
+    import torch
+    from prism_b200 import _abi as A
+    from prism_b200 import api
+    from prism_b200.batch_case import build
+    t = time.perf_counter()
+    sizes, probs = build(count, nmin, nmax, lib)
+    t_build = time.perf_counter() - t
+    cells = sum(p["mesh"].n_cells for p in probs)
+    bs = api.BatchSolver(api.BiCGSTAB(precision=A.PREC_MIXED, krylov_tol=1e-10), lib=lib)
+    times = []
+    for rep in range(2):  # the first call builds the plan and tunes the launch shape
+        for p in probs:
+            p["T"].set_values(np.zeros(p["mesh"].n_cells))
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        res = bs.solve([p["eqn"] for p in probs])
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+    for p in probs:
+        p["T"].set_values(np.zeros(p["mesh"].n_cells))
+    s = api.BiCGSTAB(krylov_tol=1e-10, preconditioner="jacobi")
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    seq_its = [s.solve(p["eqn"], 1, 0.0).krylov_iterations for p in probs]
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t
+    return {"workload": f"{count} problems, N^3 hexes with N = round(exp(U(ln {nmin}, ln {nmax}))) (seed 4), "
+                        f"{cells} cells; kappa ~ lognormal(0,1), f ~ N(0,1), Fixed 0 walls, Corrected diffusion; "
+                        f"||b - Ax|| <= 1e-10 ||b||",
+            "mesh_build_s": t_build, "first_call_s": times[0], "batched_s": times[1],
+            "solves_per_s": count / times[1], "max_iterations": max(r.krylov_iterations for r in res),
+            "worst_rel_residual": max(r.krylov_rel_residual for r in res),
+            "failed": sum(r.status != 0 for r in res),
+            "sequential_fp64_jacobi_s": t_seq, "sequential_max_iterations": max(seq_its),
+            "speedup_vs_sequential": t_seq / times[1]}
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -349,6 +440,11 @@ def run_ours(args, world, rank, local):
                              "speedup_vs_fp64_jacobi": rj["seconds"] / r32["seconds"] if r32["seconds"] > 0 else None,
                              "reference_solution": "FP64 BiCGSTAB(Jacobi) to ||b-Ax|| <= 1e-14 ||b||"}
 
+    if rank == 0 and not args.skip_adjoint:
+        extra["adjoint"] = adjoint_measure(lib)
+    if rank == 0 and not args.skip_batch:
+        extra["batched"] = batched_measure(lib)
+
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         it_s, dt = cpu_simple_sample(1)
@@ -385,6 +481,8 @@ def main():
     ap.add_argument("--skip-transport", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--transport-n", type=int, default=128)
+    ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--skip-batch", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_init(args)
     try:
