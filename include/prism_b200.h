@@ -105,6 +105,9 @@ extern "C" {
 #define PRISM_SIGN_POSITIVE 0
 #define PRISM_SIGN_NEGATIVE 1
 
+#define PRISM_TEMPORAL_BACKWARD_EULER 0 /* scheme::temporal::BackwardEuler */
+#define PRISM_TEMPORAL_ADAM_MOULTON 1   /* scheme::temporal::AdamMoulton */
+
 #define PRISM_SOLVER_BICGSTAB 0
 #define PRISM_SOLVER_JACOBI 1
 
@@ -207,6 +210,16 @@ int prism_scalar_face_values(PrismScalar* s, double* out);
 int prism_scalar_grad(PrismScalar* s, double* grad_out);
 /* computeAllCellGradients (forced sweep) */
 int prism_scalar_compute_gradients(PrismScalar* s);
+/* time-step history (field/history.cpp:1-63): setHistorySize (scalar.cpp:306-308;
+ * shrinking drops the oldest steps, 0 clears), updatePrevTimeSteps
+ * (scalar.cpp:322-324: the current values become step 0), update (scalar.cpp:
+ * 311-320: updatePrevTimeSteps, then values = values, then clearFaceValues) and
+ * getHistory (scalar.cpp:336-338: step `index`, 0 = previous time step;
+ * *available = 0 and out untouched when there is no such step). */
+int prism_scalar_set_history_size(PrismScalar* s, int32_t n_steps);
+int prism_scalar_update_prev_time_steps(PrismScalar* s);
+int prism_scalar_update(PrismScalar* s, const double* values);
+int prism_scalar_history(const PrismScalar* s, int32_t index, double* out, int32_t* available);
 
 /* values: SoA 3*n_cells (NULL = zeros) */
 int prism_vector_create(PrismMesh* mesh, const char* name, const double* values,
@@ -236,6 +249,13 @@ int prism_transport_add_diffusion(PrismTransport* eq, int32_t corrected, int32_t
 /* CONSTANT: src_scalar; DIVERGENCE: src_vector; GRADIENT: src_scalar + coord */
 int prism_transport_add_source(PrismTransport* eq, int32_t kind, int32_t sign,
                                PrismScalar* src_scalar, PrismVector* src_vector, int32_t coord);
+/* scheme::temporal::BackwardEuler / AdamMoulton (phi, dt) (backward_euler.cpp:62-86,
+ * adam_moulton.cpp:62-107): at most one per equation, in registration order with
+ * the other schemes; dt > 0. Assembly needs one history step of the field
+ * (two for AdamMoulton's second-order form, one falls back to BackwardEuler). */
+int prism_transport_add_temporal(PrismTransport* eq, int32_t kind, double dt);
+/* ITemporal::setTimeStep (temporal.cpp:24-31) */
+int prism_transport_set_time_step(PrismTransport* eq, double dt);
 /* eqn::boundary::Symmetry<Transport> (needs a convection and a diffusion scheme) */
 int prism_transport_add_symmetry_handler(PrismTransport* eq);
 int prism_transport_set_urf(PrismTransport* eq, double factor);

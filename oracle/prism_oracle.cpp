@@ -426,7 +426,23 @@ struct Scalar {
     std::shared_ptr<Grad> grad;
     uint64_t event = 0;
     double& at(int64_t c) { ++event; return v[c]; } // operator[] non-const, scalar.cpp:355-360
+    // HistoryManager (field/history.cpp:1-63): hist[0] = previous time step
+    size_t hist_max = 0;
+    std::vector<std::vector<double>> hist;
 };
+
+// HistoryManager::update, history.cpp:28-46 (Scalar::updatePrevTimeSteps, scalar.cpp:322-324)
+void updatePrevTimeSteps(Scalar& s) {
+    if (s.hist_max == 0) return;
+    if (s.hist.size() == s.hist_max) s.hist.pop_back();
+    s.hist.insert(s.hist.begin(), s.v);
+}
+// HistoryManager::resize, history.cpp:48-60
+void setHistorySize(Scalar& s, size_t n) {
+    if (n == s.hist_max) return;
+    if (n < s.hist.size()) s.hist.resize(n);
+    s.hist_max = n;
+}
 
 struct Vector {
     Mesh* m = nullptr;
@@ -640,9 +656,11 @@ struct LinSys {
     }
 };
 
-enum SchemeKind { SK_CONV, SK_DIFF };
+enum SchemeKind { SK_CONV, SK_DIFF, SK_TEMPORAL };
 struct Scheme {
     SchemeKind kind;
+    int temporal = 0;  // PRISM_TEMPORAL_*
+    double dt = 1e-5;  // ITemporal default, temporal.h:22
     int conv = 0;
     bool corrected = false;
     int corrector = PRISM_CORR_OVER_RELAXED;
@@ -928,12 +946,40 @@ void applySymmetry(Transport& eq, int32_t p) {
     for (int64_t c = 0; c < m->nc(); ++c) eq.ls.b[c] += sys.b[c];
 }
 
+// BackwardEuler::applyIncompressible (backward_euler.cpp:62-83) and
+// AdamMoulton::applyIncompressible (adam_moulton.cpp:62-99): the scheme's matrix is
+// the diagonal alone and its rhs is assigned (no accumulation across applies).
+void applyTemporal(Scheme& s, Scalar& phi) {
+    Mesh* m = phi.m;
+    const std::string who = s.temporal == PRISM_TEMPORAL_BACKWARD_EULER ? "BackwardEuler" : "AdamMoulton";
+    if (phi.hist.empty())
+        fail(PRISM_BAD_ARG, "prism::scheme::temporal::" + who + "::apply() was called for field `" + phi.name +
+                                "`, but the field does not have any previous time step values stored.");
+    std::fill(s.ls.A.begin(), s.ls.A.end(), 0.0);
+    const std::vector<double>& vol = m->volumes;
+    const std::vector<double>& p1 = phi.hist[0];
+    if (s.temporal == PRISM_TEMPORAL_ADAM_MOULTON && phi.hist.size() >= 2) {
+        const std::vector<double>& p2 = phi.hist[1];
+        for (int64_t c = 0; c < m->nc(); ++c) {
+            s.ls.A[m->slot(c, c)] = ((3.0 / 2.0) * vol[c]) / s.dt;
+            s.ls.b[c] = (2.0 * (vol[c] * p1[c])) / s.dt;
+        }
+        for (int64_t c = 0; c < m->nc(); ++c) s.ls.b[c] += (-0.5 * (vol[c] * p2[c])) / s.dt;
+    } else {  // BackwardEuler, or AdamMoulton's first step
+        for (int64_t c = 0; c < m->nc(); ++c) {
+            s.ls.A[m->slot(c, c)] = vol[c] / s.dt;
+            s.ls.b[c] = (vol[c] * p1[c]) / s.dt;
+        }
+    }
+}
+
 // Transport::updateCoeffs, transport.cpp:4-21
 void updateCoeffs(Transport& eq) {
     Mesh* m = eq.phi->m;
     for (auto& s : eq.schemes) {
         if (s.kind == SK_CONV) applyConvection(s, *eq.phi);
-        else applyDiffusion(s, *eq.phi);
+        else if (s.kind == SK_DIFF) applyDiffusion(s, *eq.phi);
+        else applyTemporal(s, *eq.phi);
         for (size_t k = 0; k < s.ls.A.size(); ++k) eq.ls.A[k] += s.ls.A[k];
         for (int64_t c = 0; c < m->nc(); ++c) eq.ls.b[c] += s.ls.b[c];
     }
@@ -1412,8 +1458,9 @@ void correctFields(Vector& U, Vector& mdot, Scalar& p, const Tensor& D, Scalar& 
         mdot.ff[f] = dot(u, m->faces[f].areaVector());
     }
     ++p.event;
+    updatePrevTimeSteps(p);  // Scalar::update, scalar.cpp:311-320
     for (int64_t c = 0; c < m->nc(); ++c) p.v[c] = p.v[c] + (urf * pp.v[c]);
-    ++p.event; // Scalar::update
+    ++p.event;
     p.fv.clear();
 }
 
@@ -1665,6 +1712,35 @@ ORC_API int orc_scalar_grad(PrismScalar* ps, double* out) {
         }
     })
 }
+ORC_API int orc_scalar_set_history_size(PrismScalar* ps, int32_t n) {
+    GUARD({
+        CHECK_ARG(ps && n >= 0, "bad argument");
+        setHistorySize(*ps->s, (size_t)n);
+    })
+}
+ORC_API int orc_scalar_update_prev_time_steps(PrismScalar* ps) {
+    GUARD({
+        CHECK_ARG(ps, "null argument");
+        updatePrevTimeSteps(*ps->s);
+    })
+}
+ORC_API int orc_scalar_update(PrismScalar* ps, const double* v) {
+    GUARD({
+        CHECK_ARG(ps && v, "null argument");
+        updatePrevTimeSteps(*ps->s);
+        std::copy(v, v + ps->s->m->nc(), ps->s->v.begin());
+        ++ps->s->event;
+        ps->s->fv.clear();
+    })
+}
+ORC_API int orc_scalar_history(const PrismScalar* ps, int32_t index, double* out, int32_t* available) {
+    GUARD({
+        CHECK_ARG(ps && out && available && index >= 0, "bad argument");
+        const Scalar& s = *ps->s;
+        *available = (size_t)index < s.hist.size() ? 1 : 0;
+        if (*available) std::copy(s.hist[index].begin(), s.hist[index].end(), out);
+    })
+}
 ORC_API int orc_scalar_compute_gradients(PrismScalar* ps) {
     GUARD({
         CHECK_ARG(ps, "null argument");
@@ -1802,6 +1878,34 @@ ORC_API int orc_transport_add_diffusion(PrismTransport* pt, int32_t corrected, i
         s.ls.init(pt->eq.phi->m);
         pt->eq.schemes.push_back(std::move(s));
         pt->eq.diff_idx = (int)pt->eq.schemes.size() - 1;
+    })
+}
+ORC_API int orc_transport_add_temporal(PrismTransport* pt, int32_t kind, double dt) {
+    GUARD({
+        CHECK_ARG(pt, "null argument");
+        CHECK_ARG(kind == PRISM_TEMPORAL_BACKWARD_EULER || kind == PRISM_TEMPORAL_ADAM_MOULTON, "bad temporal scheme");
+        CHECK_ARG(dt > 0.0, "prism::scheme::temporal::ITemporal(phi, dt): dt must be positive");
+        for (const auto& q : pt->eq.schemes)
+            CHECK_ARG(q.kind != SK_TEMPORAL, "equation already has a temporal scheme");
+        Scheme s;
+        s.kind = SK_TEMPORAL;
+        s.temporal = kind;
+        s.dt = dt;
+        s.ls.init(pt->eq.phi->m);
+        pt->eq.schemes.push_back(std::move(s));
+    })
+}
+ORC_API int orc_transport_set_time_step(PrismTransport* pt, double dt) {
+    GUARD({
+        CHECK_ARG(pt, "null argument");
+        CHECK_ARG(dt > 0.0, "prism::scheme::temporal::ITemporal::setTimeStep(): dt must be positive");
+        bool found = false;
+        for (auto& q : pt->eq.schemes)
+            if (q.kind == SK_TEMPORAL) {
+                q.dt = dt;
+                found = true;
+            }
+        CHECK_ARG(found, "equation has no temporal scheme");
     })
 }
 ORC_API int orc_transport_add_source(PrismTransport* pt, int32_t kind, int32_t sign, PrismScalar* ss,

@@ -29,6 +29,7 @@ SRC_CONSTANT, SRC_DIVERGENCE, SRC_GRADIENT = 0, 1, 2
 SIGN_POSITIVE, SIGN_NEGATIVE = 0, 1
 SOLVER_BICGSTAB, SOLVER_JACOBI = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
+TEMPORAL_BACKWARD_EULER, TEMPORAL_ADAM_MOULTON = 0, 1
 PC_AUTO, PC_JACOBI, PC_AMG = 0, 1, 2
 PC_AUTO_MIN_ROWS = 32768
 PRECONDITIONERS = {"auto": PC_AUTO, "jacobi": PC_JACOBI, "amg": PC_AMG}
@@ -146,6 +147,12 @@ SIGNATURES = {
     "transport_destroy": (C.c_int, [P]),
     "transport_add_convection": (C.c_int, [P, i32, P]),
     "transport_add_diffusion": (C.c_int, [P, i32, i32, P, P]),
+    "transport_add_temporal": (C.c_int, [P, i32, f64]),
+    "transport_set_time_step": (C.c_int, [P, f64]),
+    "scalar_set_history_size": (C.c_int, [P, i32]),
+    "scalar_update_prev_time_steps": (C.c_int, [P]),
+    "scalar_update": (C.c_int, [P, pf64]),
+    "scalar_history": (C.c_int, [P, i32, pf64, pi32]),
     "transport_add_source": (C.c_int, [P, i32, i32, P, P, i32]),
     "transport_add_symmetry_handler": (C.c_int, [P]),
     "transport_set_urf": (C.c_int, [P, f64]),

@@ -153,6 +153,31 @@ class Scalar:
     def compute_all_cell_gradients(self):
         self.lib.check(self.lib.scalar_compute_gradients(self.h))
 
+    # time-step history (field/history.cpp)
+    def set_history_size(self, n):
+        self.lib.check(self.lib.scalar_set_history_size(self.h, int(n)))
+
+    def update_prev_time_steps(self):
+        self.lib.check(self.lib.scalar_update_prev_time_steps(self.h))
+
+    def update(self, values):
+        """Scalar::update: history push, new values, face values cleared."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self.lib.check(self.lib.scalar_update(self.h, _f64p(v)))
+
+    def history(self, index):
+        """getHistory(index): values of the time step `index` back (0 = previous), or None."""
+        out = np.zeros(self.mesh.n_cells)
+        ok = C.c_int32()
+        self.lib.check(self.lib.scalar_history(self.h, int(index), _f64p(out), C.byref(ok)))
+        return out if ok.value else None
+
+    def prev_values(self):
+        return self.history(0)
+
+    def prev_prev_values(self):
+        return self.history(1)
+
     def __del__(self):
         if not getattr(self, "_borrowed", True) and getattr(self, "h", None):
             self.lib.scalar_destroy(self.h)
@@ -286,6 +311,21 @@ class diffusion:  # noqa: N801  (namespace scheme::diffusion)
         corrected = 1
 
 
+class temporal:  # noqa: N801  (namespace scheme::temporal)
+    class BackwardEuler:
+        """scheme::temporal::BackwardEuler(phi, dt) (backward_euler.cpp:62-83)."""
+        code = A.TEMPORAL_BACKWARD_EULER
+
+        def __init__(self, phi, dt=1e-5):
+            if dt <= 0.0:
+                raise ValueError("dt must be positive")
+            self.phi, self.dt = phi, float(dt)
+
+    class AdamMoulton(BackwardEuler):
+        """scheme::temporal::AdamMoulton(phi, dt) (adam_moulton.cpp:62-107)."""
+        code = A.TEMPORAL_ADAM_MOULTON
+
+
 class source:  # noqa: N801  (namespace scheme::source)
     class ConstantScalar:
         def __init__(self, phi, sign=A.SIGN_POSITIVE):
@@ -312,7 +352,9 @@ class Transport:
         self.lib.check(self.lib.transport_create(phi.h, C.byref(h)))
         self.h = h
         for s in schemes:
-            if isinstance(s, _Convection):
+            if isinstance(s, temporal.BackwardEuler):
+                self.lib.check(self.lib.transport_add_temporal(self.h, s.code, s.dt))
+            elif isinstance(s, _Convection):
                 self.lib.check(self.lib.transport_add_convection(self.h, s.code, s.U.h))
             elif isinstance(s, diffusion.NonCorrected):
                 ks = s.kappa.h if isinstance(s.kappa, Scalar) else None
@@ -333,6 +375,10 @@ class Transport:
 
     def field(self):
         return self.phi
+
+    def set_time_step(self, dt):
+        """ITemporal::setTimeStep on the equation's temporal scheme."""
+        self.lib.check(self.lib.transport_set_time_step(self.h, float(dt)))
 
     def add_symmetry_handler(self):
         self.lib.check(self.lib.transport_add_symmetry_handler(self.h))

@@ -265,12 +265,32 @@ __global__ void __launch_bounds__(256) assemble_kernel(const AssembleParams P) {
         if (P.has_conv) bcv = P.bconv[c] + rcv;
         if (P.has_diff) bdf = P.bdiff[c] + rdf;
     }
-    if (P.conv_first) {
-        if (P.has_conv) { A = A + dcv; b = b + bcv; }
-        if (P.has_diff) { A = A + ddf; b = b + bdf; }
-    } else {
-        if (P.has_diff) { A = A + ddf; b = b + bdf; }
-        if (P.has_conv) { A = A + dcv; b = b + bcv; }
+    // temporal scheme (backward_euler.cpp:80-82, adam_moulton.cpp:94-98): diagonal and a
+    // right-hand side assigned afresh on every apply
+    double dtm = 0.0, btm = 0.0;
+    if (P.has_temporal) {
+        const double vol = m.vol[c];
+        if (P.tm.second_order) {
+            dtm = ((3.0 / 2.0) * vol) / P.tm.dt;
+            btm = (2.0 * (vol * P.tm.prev[c])) / P.tm.dt;
+            btm = btm + ((-0.5 * (vol * P.tm.prev2[c])) / P.tm.dt);
+        } else {
+            dtm = vol / P.tm.dt;
+            btm = (vol * P.tm.prev[c]) / P.tm.dt;
+        }
+    }
+    for (int k = 0; k < P.nsch; ++k) {
+        const int kind = P.order[k];
+        if (kind == SCH_CONV) {
+            A = A + dcv;
+            b = b + bcv;
+        } else if (kind == SCH_DIFF) {
+            A = A + ddf;
+            b = b + bdf;
+        } else {
+            A = A + dtm;
+            b = b + btm;
+        }
     }
     for (int s = 0; s < P.nsrc; ++s) b = b + rsrc[s];
     for (int s = 0; s < nsym; ++s) {

@@ -22,12 +22,23 @@ struct SourceDesc {
     ScalarView s;
     VectorView U;
 };
+// temporal::BackwardEuler / AdamMoulton: previous time steps of the field
+struct TemporalDesc {
+    int second_order;      // AdamMoulton with two history steps
+    double dt;
+    const double* prev;    // step 0 of the history
+    const double* prev2;   // step 1 (second order only)
+};
+enum { SCH_CONV = 0, SCH_DIFF = 1, SCH_TEMPORAL = 2 };
 
 struct AssembleParams {
     MeshView m;
     ScalarView phi;
     int phi_coord;
     int has_conv, has_diff, conv_first, need_grad;
+    int has_temporal;
+    int nsch, order[3];  // schemes in registration order (SCH_*): Transport::updateCoeffs sums in this order
+    TemporalDesc tm;
     int nsrc, symmetry, accumulate;
     ConvDesc conv;
     DiffDesc diff;

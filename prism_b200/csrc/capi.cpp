@@ -290,6 +290,41 @@ API int prism_scalar_compute_gradients(PrismScalar* ps) {
         sync(*ps->s->m);
     });
 }
+API int prism_scalar_set_history_size(PrismScalar* ps, int32_t n) {
+    return guard([&] {
+        ARG(ps && n >= 0, "bad argument");
+        setHistorySize(*ps->s, (size_t)n);
+    });
+}
+API int prism_scalar_update_prev_time_steps(PrismScalar* ps) {
+    return guard([&] {
+        ARG(ps, "null argument");
+        updatePrevTimeSteps(*ps->s);
+        sync(*ps->s->m);
+    });
+}
+API int prism_scalar_update(PrismScalar* ps, const double* values) {
+    return guard([&] {
+        ARG(ps && values, "null argument");
+        Scalar& s = *ps->s;
+        updatePrevTimeSteps(s);
+        s.v.upload(values, s.m->nc, s.m->stream);
+        ++s.event;
+        s.has_fv = false;
+        sync(*s.m);
+    });
+}
+API int prism_scalar_history(const PrismScalar* ps, int32_t index, double* out, int32_t* available) {
+    return guard([&] {
+        ARG(ps && out && available && index >= 0, "bad argument");
+        const Scalar& s = *ps->s;
+        *available = (size_t)index < s.hist.size() ? 1 : 0;
+        if (*available) {
+            s.hist[index].download(out, s.m->nc, s.m->stream);
+            sync(*s.m);
+        }
+    });
+}
 
 // ---- vector
 API int prism_vector_create(PrismMesh* pm, const char* name, const double* values, int32_t grad, const PrismBC* bcs,
@@ -474,6 +509,7 @@ API int prism_transport_add_convection(PrismTransport* pt, int32_t scheme, Prism
         pt->eq.conv_scheme = scheme;
         pt->eq.U = U->v.get();
         if (!pt->eq.has_diff) pt->eq.conv_first = 1;
+        pt->eq.order[pt->eq.nsch++] = SCH_CONV;
     });
 }
 API int prism_transport_add_diffusion(PrismTransport* pt, int32_t corrected, int32_t corrector, PrismScalar* ks,
@@ -488,6 +524,27 @@ API int prism_transport_add_diffusion(PrismTransport* pt, int32_t corrected, int
         pt->eq.ks = ks ? ks->s.get() : nullptr;
         pt->eq.kt = kt ? kt->t.get() : nullptr;
         if (!pt->eq.has_conv) pt->eq.conv_first = 0;
+        pt->eq.order[pt->eq.nsch++] = SCH_DIFF;
+    });
+}
+API int prism_transport_add_temporal(PrismTransport* pt, int32_t kind, double dt) {
+    return guard([&] {
+        ARG(pt, "null argument");
+        ARG(kind == PRISM_TEMPORAL_BACKWARD_EULER || kind == PRISM_TEMPORAL_ADAM_MOULTON, "bad temporal scheme");
+        ARG(dt > 0.0, "prism::scheme::temporal::ITemporal(phi, dt): dt must be positive");
+        ARG(!pt->eq.has_temporal, "equation already has a temporal scheme");
+        pt->eq.has_temporal = 1;
+        pt->eq.temporal_kind = kind;
+        pt->eq.dt = dt;
+        pt->eq.order[pt->eq.nsch++] = SCH_TEMPORAL;
+    });
+}
+API int prism_transport_set_time_step(PrismTransport* pt, double dt) {
+    return guard([&] {
+        ARG(pt, "null argument");
+        ARG(dt > 0.0, "prism::scheme::temporal::ITemporal::setTimeStep(): dt must be positive");
+        ARG(pt->eq.has_temporal, "equation has no temporal scheme");
+        pt->eq.dt = dt;
     });
 }
 API int prism_transport_add_source(PrismTransport* pt, int32_t kind, int32_t sign, PrismScalar* ss, PrismVector* sv,

@@ -302,6 +302,30 @@ void ensureGradient(Scalar& s) {
     if (s.event != s.grad->computed) computeGradient(s);
 }
 
+// ------------------------------------------------------------------ time-step history
+// HistoryManager::resize (history.cpp:48-60)
+void setHistorySize(Scalar& s, size_t n) {
+    if (n == s.hist_max) return;
+    if (n < s.hist.size()) s.hist.resize(n);
+    s.hist_max = n;
+}
+// HistoryManager::update (history.cpp:28-46): the current values become step 0;
+// the oldest buffer is reused once the history is full
+void updatePrevTimeSteps(Scalar& s) {
+    if (s.hist_max == 0) return;
+    Mesh& m = *s.m;
+    DevBuf<double> front;
+    if (s.hist.size() == s.hist_max) {
+        front = std::move(s.hist.back());
+        s.hist.pop_back();
+    } else {
+        front.alloc(m.n_pad);
+        front.zero(m.stream);
+    }
+    PB_CUDA(cudaMemcpyAsync(front.p, s.v.p, m.nc * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    s.hist.insert(s.hist.begin(), std::move(front));
+}
+
 // ------------------------------------------------------------------ transport
 void Transport::ensure() {
     Mesh& m = *phi->m;
@@ -365,6 +389,21 @@ void updateCoeffs(Transport& eq) {
     P.has_conv = eq.has_conv;
     P.has_diff = eq.has_diff;
     P.conv_first = eq.conv_first;
+    P.nsch = eq.nsch;
+    for (int k = 0; k < eq.nsch; ++k) P.order[k] = eq.order[k];
+    if (eq.has_temporal) {
+        // BackwardEuler::applyIncompressible (backward_euler.cpp:62-76), AdamMoulton (adam_moulton.cpp:62-91)
+        if (phi.hist.empty())
+            fail(PRISM_BAD_ARG, std::string("prism::scheme::temporal::") +
+                                    (eq.temporal_kind == PRISM_TEMPORAL_BACKWARD_EULER ? "BackwardEuler" : "AdamMoulton") +
+                                    "::apply() was called for field `" + phi.name +
+                                    "`, but the field does not have any previous time step values stored.");
+        P.has_temporal = 1;
+        P.tm.dt = eq.dt;
+        P.tm.prev = phi.hist[0].p;
+        P.tm.second_order = (eq.temporal_kind == PRISM_TEMPORAL_ADAM_MOULTON && phi.hist.size() >= 2) ? 1 : 0;
+        P.tm.prev2 = P.tm.second_order ? phi.hist[1].p : nullptr;
+    }
     P.need_grad = need_grad ? 1 : 0;
     if (eq.has_conv) {
         P.conv.scheme = eq.conv_scheme;
@@ -631,6 +670,9 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
     pEqn.has_conv = 0;
     pEqn.conv_scheme = 0;
     pEqn.conv_first = 1;
+    pEqn.has_temporal = 0;
+    pEqn.nsch = 1;
+    pEqn.order[0] = SCH_DIFF;
     pEqn.has_diff = 1;
     pEqn.corrected = 1;
     pEqn.corrector = PRISM_CORR_OVER_RELAXED;
@@ -658,6 +700,7 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
 void correctFields(Vector& U, Vector& mdot, Scalar& p, const Tensor& D, Scalar& pp, double urf) {
     Mesh& m = *U.m;
     ensureGradient(pp);
+    updatePrevTimeSteps(p);  // p->update(...) keeps the old values in p's history (scalar.cpp:311-320)
     launchCorrectFields(m.view(), U.c[0]->view(), U.c[1]->view(), U.c[2]->view(), D.view(), pp.view(), mdot.fd.p,
                         mdot.ff.p, p.v.p, urf, m.stream);
     for (auto& c : U.c) ++c->event;
@@ -765,7 +808,7 @@ FixedPointOut steadySolve(Transport& eq, const PrismSolveOpts& o, int max_outer,
 namespace {
 void checkAdjointSupported(const Transport& eq) {
     const Scalar& phi = *eq.phi;
-    if (!eq.has_diff || eq.has_conv || !eq.ks || eq.kt || eq.symmetry)
+    if (!eq.has_diff || eq.has_conv || eq.has_temporal || !eq.ks || eq.kt || eq.symmetry)
         fail(PRISM_BAD_ARG, "adjoint: only a diffusion equation with a scalar kappa field is supported");
     if (phi.coord >= 0) fail(PRISM_BAD_ARG, "adjoint: the field must be a scalar field");
     if (eq.corrected && phi.grad->type != PRISM_GRAD_LEAST_SQUARES)

@@ -72,8 +72,13 @@ struct Scalar {
     DevBuf<double> bc_val, bc_vec;
     std::shared_ptr<GradState> grad;
     uint64_t event = 0;
+    // time-step history (field/history.cpp): hist[0] = previous time step
+    size_t hist_max = 0;
+    std::vector<DevBuf<double>> hist;
     ScalarView view() const;
 };
+void setHistorySize(Scalar& s, size_t n);
+void updatePrevTimeSteps(Scalar& s);
 
 struct Vector {
     Mesh* m = nullptr;
@@ -103,6 +108,9 @@ struct Source {
 struct Transport {
     Scalar* phi = nullptr;
     int has_conv = 0, conv_scheme = 0, has_diff = 0, corrected = 0, corrector = 0, conv_first = 1;
+    int has_temporal = 0, temporal_kind = 0;
+    double dt = 1e-5;           // ITemporal default (temporal.h:22)
+    int nsch = 0, order[3] = {};  // schemes in registration order (SCH_*)
     Vector* U = nullptr;
     Scalar* ks = nullptr;
     Tensor* kt = nullptr;

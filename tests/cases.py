@@ -71,6 +71,42 @@ def advection_reference(unv, case, lib, solver=None):
     return {"T": x, "diff_norm": np.array(np.linalg.norm(x - exact))}
 
 
+def transient_exact(x, t, kappa, modes=100):
+    """The series solution the reference's transient test compares with
+    (tests/test_transient_1d.cpp:14-26)."""
+    s = np.zeros_like(x)
+    for n in range(modes):
+        lam = ((2 * n) - 1) * np.pi / 2
+        v = ((-1.0) ** (n + 1)) * np.exp(-kappa * t * lam ** 2) * np.cos(lam * x) / ((2 * n) - 1)
+        s = s + v
+    return s * (4.0 / np.pi) * 100
+
+
+def transient_reference(unv, case, lib, solver=None, steps=200, dt=2.0):
+    """tests/test_transient_1d.cpp:29-83: T = 200 with a 2-step history, AdamMoulton(T, dt) +
+    Corrected(1e-3, T); per time step solve(10, 1e-20) then updatePrevTimeSteps. Returns the
+    final field and the relative L2 errors against the series at t = 40, 60 and at the end."""
+    mesh = api.Mesh(unv, case, lib=lib)
+    x = mesh.export()["cell_center"][0]
+    T = api.Scalar("T", mesh, 200.0)
+    T.set_history_size(2)
+    T.update_prev_time_steps()
+    kappa = 1e-3
+    k = api.Scalar("kappa", mesh, kappa)
+    eqn = api.Transport(api.temporal.AdamMoulton(T, dt), api.diffusion.Corrected(k, T))
+    solver = solver or api.BiCGSTAB()
+    norms, final = [], None
+    for step in range(steps):
+        solver.solve(eqn, 10, 1e-20)
+        exact = transient_exact(x, dt * step, kappa)
+        err = float(np.linalg.norm(T.values() - exact) / np.linalg.norm(exact))
+        if dt * step in (40, 60):
+            norms.append(err)
+        final = err
+        T.update_prev_time_steps()
+    return {"T": T.values(), "diff_norms": np.array(norms), "final_diff_norm": np.array(final)}
+
+
 def simple_fields(mesh, nu=1e-3):
     """makePressureVelocityFields (tests/test_utils.h:176-195)."""
     U = api.Vector("U", mesh, (0.0, 0.0, 0.0))
@@ -127,6 +163,8 @@ def run_reference_test(name, lib, solver=None):
         return simple_reference(unv, case, lib, 20, nu=0.01, solver=solver)
     if name == "duct_simple":
         return simple_reference(unv, case, lib, 100, symmetry=True, solver=solver)
+    if name == "versteeg_trans_1d":
+        return transient_reference(unv, case, lib, solver=solver)
     raise KeyError(name)
 
 

@@ -2,13 +2,13 @@
 
 Run in a container where the reference checkout is available:
 
-    python tests/golden/make_golden.py /root/reference/tests/cases
+    python tests/golden/make_golden.py /root/reference/tests/cases [case names]
 
 For each case it stores the mesh in converter form (nodes, element list,
 groups; re-encoded from the case's mesh.unv), the parsed fields.json and
 <field>.json documents, and the CPU oracle's results for the reference test
 that uses the case (tests/test_poisson.cpp, test_advection_1d.cpp,
-test_simple_coarse_pipe.cpp, test_needs_pressure_ref.cpp). The GPU tests
+test_simple_coarse_pipe.cpp, test_needs_pressure_ref.cpp, test_transient_1d.cpp). The GPU tests
 compare the sm_100a path with these arrays; the CPU tests re-run the oracle and
 check it against the reference tests' own thresholds.
 """
@@ -32,12 +32,15 @@ CASES = {
     "coarse_pipe": ("coarsePipeHex", "mesh.unv"),
     "cavity_hex": ("cavity_hex", "mesh.unv"),
     "duct_simple": ("ductSIMPLE", "mesh.unv"),
+    "versteeg_trans_1d": ("versteeg_trans_1d", "mesh.unv"),
 }
 
 
-def main(src):
+def main(src, only=None):
     out_dir = os.path.dirname(os.path.abspath(__file__))
     for name, (case_dir, mesh_file) in CASES.items():
+        if only and name not in only:
+            continue
         base = os.path.join(src, case_dir)
         unv = io.read_unv(os.path.join(base, mesh_file))
         with open(os.path.join(base, "fields.json")) as fh:
@@ -74,4 +77,4 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests/cases")
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests/cases", sys.argv[2:])

@@ -88,3 +88,90 @@ def test_solver_tridiagonal_pin(orc, solver):
     for _ in range(20):
         x = s.step(orc, rp, col, val, x, b)
     assert np.linalg.norm(x - x_exact) / np.linalg.norm(x_exact) < 1e-4
+
+
+def test_transient_1d_pin(orc):
+    # tests/test_transient_1d.cpp:70-82: errors at t = 40 and 60 below 0.10 and decreasing,
+    # below 0.02 after 200 steps (AdamMoulton + Corrected, dt = 2)
+    got = cases.run_reference_test("versteeg_trans_1d", orc)
+    n40, n60 = got["diff_norms"]
+    assert n40 < 0.10 and n60 < 0.10 and n60 < n40
+    assert got["final_diff_norm"] < 0.02
+    ref = cases.load_oracle_results("versteeg_trans_1d")
+    np.testing.assert_array_equal(got["T"], ref["T"])
+
+
+def _history_sections(lib):
+    """tests/test_scalar_history.cpp:6-132, section by section, on the advection mesh."""
+    unv, case, _ = cases.load_golden("versteeg_advection_1d")
+    mesh = api.Mesh(unv, case, lib=lib)
+    n = mesh.n_cells
+    t = [np.full(n, float(k + 1)) for k in range(6)]
+
+    def fresh():
+        return api.Scalar("T", mesh, t[0])
+
+    # basic tracking
+    T = fresh()
+    T.set_history_size(3)
+    assert T.prev_values() is None
+    T.update(t[1])
+    np.testing.assert_array_equal(T.values(), t[1])
+    np.testing.assert_array_equal(T.prev_values(), t[0])
+    assert T.prev_prev_values() is None
+    T.update(t[2])
+    np.testing.assert_array_equal(T.prev_values(), t[1])
+    np.testing.assert_array_equal(T.prev_prev_values(), t[0])
+    assert T.history(3) is None
+    T.update(t[3])
+    np.testing.assert_array_equal(T.history(2), t[0])
+    T.update(t[4])
+    np.testing.assert_array_equal(T.values(), t[4])
+    np.testing.assert_array_equal(T.prev_values(), t[3])
+    np.testing.assert_array_equal(T.prev_prev_values(), t[2])
+    np.testing.assert_array_equal(T.history(2), t[1])
+    assert T.history(3) is None
+    # truncation
+    T = fresh()
+    T.set_history_size(4)
+    for k in range(1, 5):
+        T.update(t[k])
+    for i in range(4):
+        np.testing.assert_array_equal(T.history(i), t[3 - i])
+    T.set_history_size(2)
+    np.testing.assert_array_equal(T.history(0), t[3])
+    np.testing.assert_array_equal(T.history(1), t[2])
+    assert T.history(2) is None
+    T.update(t[5])
+    np.testing.assert_array_equal(T.prev_values(), t[4])
+    np.testing.assert_array_equal(T.prev_prev_values(), t[3])
+    assert T.history(2) is None
+    # expansion
+    T = fresh()
+    T.set_history_size(1)
+    T.update(t[1])
+    T.update(t[2])
+    np.testing.assert_array_equal(T.prev_values(), t[1])
+    assert T.prev_prev_values() is None
+    T.set_history_size(3)
+    np.testing.assert_array_equal(T.prev_values(), t[1])
+    assert T.prev_prev_values() is None
+    T.update(t[3])
+    np.testing.assert_array_equal(T.prev_values(), t[2])
+    np.testing.assert_array_equal(T.prev_prev_values(), t[1])
+    T.update(t[4])
+    np.testing.assert_array_equal(T.history(2), t[1])
+    # clearing
+    T = fresh()
+    T.set_history_size(2)
+    T.update(t[1])
+    T.update(t[2])
+    assert T.prev_values() is not None
+    T.set_history_size(0)
+    assert T.prev_values() is None and T.prev_prev_values() is None
+    T.update(t[3])
+    assert T.prev_values() is None
+
+
+def test_scalar_history_pin(orc):
+    _history_sections(orc)
