@@ -127,7 +127,20 @@ class Scalar {
         check(prism_scalar_get_values(_h.get(), v.data()));
         return v;
     }
-    void update(const std::vector<double>& v) { check(prism_scalar_set_values(_h.get(), v.data())); }
+    // Scalar::update (scalar.cpp:311-320): history push, new values, face values cleared
+    void update(const std::vector<double>& v) { check(prism_scalar_update(_h.get(), v.data())); }
+    // time-step history (field/history.cpp)
+    void setHistorySize(size_t n) { check(prism_scalar_set_history_size(_h.get(), (int32_t)n)); }
+    void updatePrevTimeSteps() { check(prism_scalar_update_prev_time_steps(_h.get())); }
+    auto getHistory(size_t index) const -> std::optional<std::vector<double>> {
+        std::vector<double> v(_mesh->cellCount());
+        int32_t ok = 0;
+        check(prism_scalar_history(_h.get(), (int32_t)index, v.data(), &ok));
+        if (!ok) return std::nullopt;
+        return v;
+    }
+    auto prevValues() const { return getHistory(0); }
+    auto prevPrevValues() const { return getHistory(1); }
     void setFaceValues(const std::vector<double>& fv) { check(prism_scalar_set_face_values(_h.get(), fv.data())); }
     void clearFaceValues() { check(prism_scalar_set_face_values(_h.get(), nullptr)); }
     auto handle() const -> PrismScalar* { return _h.get(); }
@@ -252,6 +265,18 @@ struct Gradient {
     int coord;
 };
 }  // namespace source
+namespace temporal {
+template <int Kind>
+struct Scheme {
+    explicit Scheme(std::shared_ptr<field::Scalar> phi, double dt = 1e-5) : phi(std::move(phi)), dt(dt) {
+        if (dt <= 0.0) throw std::invalid_argument("prism::scheme::temporal::ITemporal(phi, dt): dt must be positive");
+    }
+    std::shared_ptr<field::Scalar> phi;
+    double dt;
+};
+using BackwardEuler = Scheme<PRISM_TEMPORAL_BACKWARD_EULER>;
+using AdamMoulton = Scheme<PRISM_TEMPORAL_ADAM_MOULTON>;
+}  // namespace temporal
 }  // namespace scheme
 
 namespace eqn {
@@ -271,6 +296,8 @@ class Transport {
     void relax() { check(prism_transport_relax(_h.get())); }
     void zeroOutCoeffs() { check(prism_transport_zero_coeffs(_h.get())); }
     void addSymmetryHandler() { check(prism_transport_add_symmetry_handler(_h.get())); }
+    // temporalScheme()->setTimeStep(dt) (temporal.cpp:24-31)
+    void setTimeStep(double dt) { check(prism_transport_set_time_step(_h.get(), dt)); }
     auto field() const -> const std::shared_ptr<field::Scalar>& { return _phi; }
     auto handle() const -> PrismTransport* { return _h.get(); }
 
@@ -286,6 +313,10 @@ class Transport {
                                             s.kt ? s.kt->handle() : nullptr));
         _keep.push_back(s.ks);
         _keep.push_back(s.kt);
+    }
+    template <int K>
+    void add(scheme::temporal::Scheme<K> s) {
+        check(prism_transport_add_temporal(_h.get(), K, s.dt));
     }
     template <int S>
     void add(scheme::source::ConstantScalar<S> s) {
