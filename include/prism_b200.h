@@ -35,6 +35,9 @@
  *   prism_prime_step         algorithm/PRIME.cpp:11-37 PRIME::step
  *   prism_piso_step          algorithm/PISO.cpp:10-55 PISO::step
  *   prism_needs_pressure_reference  algorithm/SIMPLE.cpp:110-122
+ *   prism_ops_div            operations/operations.h:84-100 ops::div
+ *   prism_courant_number     monitor/courant.cpp:7-24 monitor::courantNumber
+ *   prism_cell_to_point      export.cpp:73-111 (anonymous) cellToPoint
  */
 #ifndef PRISM_B200_H
 #define PRISM_B200_H
@@ -161,6 +164,8 @@ typedef struct {
     int64_t nnz; /* entries of the CSR pattern (diagonal + face neighbours) */
     int32_t n_patches;
     int32_t n_gs_levels; /* levels of the Green-Gauss in-place sweep schedule */
+    int64_t n_vertices;      /* PMesh::vertices(): every UNV node (pmesh.h:40) */
+    int64_t n_cell_vertices; /* sum over cells of Cell::verticesIds().size() */
 } PrismMeshInfo;
 
 /* Caller-allocated export buffers; any pointer may be NULL. Vectors are SoA. */
@@ -179,6 +184,9 @@ typedef struct {
     int64_t* csr_col;           /* nnz, column-sorted rows */
     int64_t* patch_face_offsets; /* n_patches+1 */
     int64_t* patch_faces;
+    double* vertex_coords;        /* 3*n_vertices */
+    int64_t* cell_vertex_offsets; /* n_cells+1 */
+    int64_t* cell_vertices;       /* n_cell_vertices: UNV element node order (cell.h:25) */
 } PrismMeshExport;
 
 int prism_mesh_from_unv(const PrismUnvMesh* desc, PrismMesh** out);
@@ -233,6 +241,30 @@ int prism_vector_set_values(PrismVector* v, const double* values);
 int prism_vector_get_values(const PrismVector* v, double* values);
 /* fluxAtFace for every face (n_faces); empty-patch faces are written as 0 */
 int prism_vector_face_flux(PrismVector* v, double* out);
+/* GeneralVector::setFaceFluxValues (vector.h:359-377): n_faces fluxes that
+ * fluxAtFace returns from now on */
+int prism_vector_set_face_flux(PrismVector* v, const double* flux);
+
+/* ---- diagnostics and point data for export ------------------------------ */
+/* ops::div (operations/operations.h:84-100,144-169): a new scalar named
+ * "div(<name>)" holding, per cell, the signed sum of fluxAtFace over the
+ * cell's non-empty faces divided by the cell volume. */
+int prism_ops_div(PrismVector* U, PrismScalar** out);
+/* monitor::courantNumber (monitor/courant.cpp:7-24): a new scalar named "Co"
+ * holding 0.5 * dt * sum(|fluxAtFace|) / volume per cell (empty faces skipped). */
+int prism_courant_number(PrismVector* mdot, double dt, PrismScalar** out);
+/* output::cellToPoint (export.cpp:73-111): inverse-distance weighted
+ * interpolation of cell data to every mesh vertex, weights
+ * 1 / max(|x_v - x_c|, DBL_EPSILON) over the cells that use the vertex.
+ * cell_data: n_cells*n_components, point_data: n_vertices*n_components, both
+ * interleaved per cell / vertex (the VTU layout, not SoA). A vertex that no
+ * cell uses fails with PRISM_INVALID_MESH. */
+int prism_cell_to_point(PrismMesh* mesh, const double* cell_data, int32_t n_components,
+                        double* point_data);
+/* cellToPoint of a device-resident field: n_vertices values / 3*n_vertices
+ * interleaved x,y,z per vertex (flattenVector order, export.cpp:139-151) */
+int prism_scalar_to_points(PrismScalar* s, double* point_data);
+int prism_vector_to_points(PrismVector* v, double* point_data);
 
 /* values: 9*n_cells SoA, NULL = identity */
 int prism_tensor_create(PrismMesh* mesh, const char* name, const double* values,

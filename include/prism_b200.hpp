@@ -92,7 +92,14 @@ class PMesh {
     auto faceCount() const -> size_t { return (size_t)_info.n_faces; }
     auto boundaryFaceCount() const -> size_t { return (size_t)_info.n_boundary_faces; }
     auto patchCount() const -> size_t { return (size_t)_info.n_patches; }
+    auto vertexCount() const -> size_t { return (size_t)_info.n_vertices; }
     auto handle() const -> PrismMesh* { return _h.get(); }
+    // output::cellToPoint (export.cpp:73-111): interleaved cell data -> interleaved vertex data
+    auto cellToPoint(const std::vector<double>& cell_data, size_t n_components) const -> std::vector<double> {
+        std::vector<double> out(vertexCount() * n_components);
+        check(prism_cell_to_point(_h.get(), cell_data.data(), (int32_t)n_components, out.data()));
+        return out;
+    }
 
   private:
     std::shared_ptr<PrismMesh> _h;
@@ -120,6 +127,18 @@ class Scalar {
     Scalar(PrismScalar* borrowed, std::shared_ptr<void> owner, std::shared_ptr<mesh::PMesh> mesh, std::string name)
         : _mesh(std::move(mesh)), _name(std::move(name)), _owner(std::move(owner)) {
         _h.reset(borrowed, [](PrismScalar*) {});
+    }
+    // a scalar the library created (ops::div, monitor::courantNumber): owned
+    static auto adopt(PrismScalar* owned, std::shared_ptr<mesh::PMesh> mesh, std::string name) -> Scalar {
+        Scalar s(owned, nullptr, std::move(mesh), std::move(name));
+        s._h.reset(owned, [](PrismScalar* p) { prism_scalar_destroy(p); });
+        return s;
+    }
+    // cellToPoint of the cell values: one value per mesh vertex
+    auto toPoints() const -> std::vector<double> {
+        std::vector<double> v(_mesh->vertexCount());
+        check(prism_scalar_to_points(_h.get(), v.data()));
+        return v;
     }
     auto name() const -> const std::string& { return _name; }
     auto values() const -> std::vector<double> {
@@ -179,7 +198,25 @@ class Vector : public std::enable_shared_from_this<Vector> {
     auto x() { return component(0); }
     auto y() { return component(1); }
     auto z() { return component(2); }
+    auto name() const -> const std::string& { return _name; }
+    auto mesh() const -> const std::shared_ptr<mesh::PMesh>& { return _mesh; }
     auto handle() const -> PrismVector* { return _h.get(); }
+    // setFaceFluxValues (vector.h:359-377)
+    void setFaceFluxValues(const std::vector<double>& flux) {
+        check(prism_vector_set_face_flux(_h.get(), flux.data()));
+    }
+    // fluxAtFace for every face (empty-patch faces 0)
+    auto faceFlux() const -> std::vector<double> {
+        std::vector<double> f(_mesh->faceCount());
+        check(prism_vector_face_flux(_h.get(), f.data()));
+        return f;
+    }
+    // cellToPoint of the cell values, x,y,z interleaved per vertex
+    auto toPoints() const -> std::vector<double> {
+        std::vector<double> v(3 * _mesh->vertexCount());
+        check(prism_vector_to_points(_h.get(), v.data()));
+        return v;
+    }
 
   private:
     Vector(std::shared_ptr<mesh::PMesh> mesh, std::string name, PrismVector* h) : _mesh(std::move(mesh)), _name(std::move(name)) {
@@ -212,6 +249,24 @@ class Tensor {
     std::shared_ptr<PrismTensor> _h;
 };
 }  // namespace field
+
+namespace ops {
+// ops::div (operations/operations.h:84-100): "div(<name>)" = signed flux sum / volume
+inline auto div(const field::Vector& U) -> field::Scalar {
+    PrismScalar* h = nullptr;
+    check(prism_ops_div(U.handle(), &h));
+    return field::Scalar::adopt(h, U.mesh(), "div(" + U.name() + ")");
+}
+}  // namespace ops
+
+namespace monitor {
+// monitor::courantNumber (monitor/courant.cpp:7-24): "Co" = 0.5 dt sum|flux| / volume
+inline auto courantNumber(const field::Vector& mdot, double dt) -> field::Scalar {
+    PrismScalar* h = nullptr;
+    check(prism_courant_number(mdot.handle(), dt, &h));
+    return field::Scalar::adopt(h, mdot.mesh(), "Co");
+}
+}  // namespace monitor
 
 namespace scheme {
 namespace convection {

@@ -126,6 +126,7 @@ struct Face {
 };
 struct Cell {
     std::vector<int64_t> faces;
+    std::vector<int64_t> vids; // UNV element node order (cell.h:13, unv.cpp:206-207)
     double volume = 0.0;
     V3 center;
 };
@@ -310,6 +311,7 @@ std::unique_ptr<Mesh> buildFromUnv(const PrismUnvMesh* d) {
                     for (auto& fl : WEDGE_T) c.faces.push_back(processFace({en[fl[0]], en[fl[1]], en[fl[2]]}));
                     for (auto& fl : WEDGE_Q) c.faces.push_back(processFace({en[fl[0]], en[fl[1]], en[fl[2]], en[fl[3]]}));
                 }
+                c.vids = en;
                 cellGeometry(c, faces);
                 cells.push_back(std::move(c));
                 ++cell_counter;
@@ -1591,6 +1593,10 @@ ORC_API int orc_mesh_info(const PrismMesh* pm, PrismMeshInfo* info) {
         info->n_nonempty_boundary_faces = m.n_nonempty;
         info->nnz = (int64_t)m.col.size();
         info->n_patches = (int32_t)m.patches.size();
+        info->n_vertices = (int64_t)m.verts.size();
+        int64_t ncv = 0;
+        for (auto& c : m.cells) ncv += (int64_t)c.vids.size();
+        info->n_cell_vertices = ncv;
         // levels of the in-place Green-Gauss sweep dependency (lower-id neighbours)
         std::vector<int32_t> lev(m.nc(), 0);
         int32_t nl = 0;
@@ -1648,6 +1654,19 @@ ORC_API int orc_mesh_export(const PrismMesh* pm, PrismMeshExport* o) {
             }
         }
         if (o->patch_face_offsets) o->patch_face_offsets[m.patches.size()] = pos;
+        const int64_t nv = (int64_t)m.verts.size();
+        for (int64_t v = 0; v < nv; ++v)
+            for (int k = 0; k < 3; ++k)
+                if (o->vertex_coords) o->vertex_coords[k * nv + v] = m.verts[v][k];
+        pos = 0;
+        for (int64_t c = 0; c < nc; ++c) {
+            if (o->cell_vertex_offsets) o->cell_vertex_offsets[c] = pos;
+            for (auto v : m.cells[c].vids) {
+                if (o->cell_vertices) o->cell_vertices[pos] = v;
+                ++pos;
+            }
+        }
+        if (o->cell_vertex_offsets) o->cell_vertex_offsets[nc] = pos;
     })
 }
 ORC_API int orc_mesh_destroy(PrismMesh* pm) { GUARD({ delete pm; }) }
@@ -1821,6 +1840,129 @@ ORC_API int orc_vector_face_flux(PrismVector* pv, double* out) {
             const Face& fc = m->faces[f];
             out[f] = (fc.nbr < 0 && m->patches[fc.patch].empty) ? 0.0 : fluxAtFace(*pv->v, f);
         }
+    })
+}
+
+// GeneralVector::setFaceFluxValues, vector.h:359-377
+ORC_API int orc_vector_set_face_flux(PrismVector* pv, const double* flux) {
+    GUARD({
+        CHECK_ARG(pv && flux, "null argument");
+        Vector& U = *pv->v;
+        U.ff.assign(flux, flux + U.m->nf());
+        U.has_ff = true;
+    })
+}
+
+// ---------------------------------------------------------------- diagnostics
+namespace {
+std::shared_ptr<Scalar> resultScalar(Mesh* m, const std::string& name, std::vector<double> v) {
+    // field::Scalar(name, mesh, data): no boundary handlers, least-squares gradient
+    auto s = std::make_shared<Scalar>();
+    s->m = m;
+    s->name = name;
+    s->v = std::move(v);
+    PrismBC none{};
+    none.kind = PRISM_BC_UNKNOWN;
+    s->bc.assign(m->patches.size(), none);
+    s->grad = makeGrad(m, PRISM_GRAD_LEAST_SQUARES);
+    return s;
+}
+
+// ensureCache, export.cpp:44-71: vertex -> adjacent cells in cell order
+std::vector<std::vector<int64_t>> vertexCells(const Mesh& m) {
+    std::vector<std::vector<int64_t>> v2c(m.verts.size());
+    for (int64_t c = 0; c < m.nc(); ++c)
+        for (auto v : m.cells[c].vids) v2c[v].push_back(c);
+    return v2c;
+}
+
+// cellToPoint, export.cpp:73-111
+std::vector<double> cellToPoint(const Mesh& m, const double* cell_data, int64_t ncomp) {
+    auto v2c = vertexCells(m);
+    const int64_t nv = (int64_t)m.verts.size();
+    std::vector<double> out(nv * ncomp, 0.0);
+    for (int64_t v = 0; v < nv; ++v) {
+        const auto& adj = v2c[v];
+        if (adj.empty())
+            fail(PRISM_INVALID_MESH,
+                 "Vertex " + std::to_string(v) + " has no adjacent cells; point data cannot be computed.");
+        std::vector<double> w(adj.size());
+        double sw = 0.0;
+        for (size_t i = 0; i < adj.size(); ++i) {
+            double d = norm(m.verts[v] - m.cells[adj[i]].center);
+            w[i] = 1.0 / std::max(d, EPSILON);
+            sw += w[i];
+        }
+        for (size_t i = 0; i < adj.size(); ++i) {
+            double wi = w[i] / sw;
+            for (int64_t k = 0; k < ncomp; ++k) out[v * ncomp + k] += wi * cell_data[adj[i] * ncomp + k];
+        }
+    }
+    return out;
+}
+}  // namespace
+
+// ops::div, operations.h:84-100 (fluxSumAtCell, :144-169)
+ORC_API int orc_ops_div(PrismVector* pv, PrismScalar** out) {
+    GUARD({
+        CHECK_ARG(pv && out, "null argument");
+        const Vector& U = *pv->v;
+        Mesh* m = U.m;
+        std::vector<double> d(m->nc());
+        for (int64_t c = 0; c < m->nc(); ++c) d[c] = fluxSumAtCell(U, c) / m->cells[c].volume;
+        auto* ps = new PrismScalar();
+        ps->s = resultScalar(m, "div(" + U.name + ")", std::move(d));
+        *out = ps;
+    })
+}
+
+// monitor::courantNumber, courant.cpp:7-24
+ORC_API int orc_courant_number(PrismVector* pv, double dt, PrismScalar** out) {
+    GUARD({
+        CHECK_ARG(pv && out, "null argument");
+        const Vector& U = *pv->v;
+        Mesh* m = U.m;
+        std::vector<double> co(m->nc(), 0.0);
+        for (int64_t c = 0; c < m->nc(); ++c) {
+            double flux_sum = 0.0;
+            for (auto f : m->cells[c].faces) {
+                const Face& fc = m->faces[f];
+                if (fc.nbr < 0 && m->patches[fc.patch].empty) continue;
+                flux_sum += std::abs(fluxAtFace(U, f));
+            }
+            co[c] = 0.5 * dt * flux_sum / m->cells[c].volume;
+        }
+        auto* ps = new PrismScalar();
+        ps->s = resultScalar(m, "Co", std::move(co));
+        *out = ps;
+    })
+}
+
+ORC_API int orc_cell_to_point(PrismMesh* pm, const double* cell_data, int32_t ncomp, double* point_data) {
+    GUARD({
+        CHECK_ARG(pm && cell_data && point_data, "null argument");
+        CHECK_ARG(ncomp >= 1 && ncomp <= 9, "n_components must be 1..9");
+        auto r = cellToPoint(*pm->m, cell_data, ncomp);
+        std::copy(r.begin(), r.end(), point_data);
+    })
+}
+ORC_API int orc_scalar_to_points(PrismScalar* ps, double* point_data) {
+    GUARD({
+        CHECK_ARG(ps && point_data, "null argument");
+        auto r = cellToPoint(*ps->s->m, ps->s->v.data(), 1);
+        std::copy(r.begin(), r.end(), point_data);
+    })
+}
+ORC_API int orc_vector_to_points(PrismVector* pv, double* point_data) {
+    GUARD({
+        CHECK_ARG(pv && point_data, "null argument");
+        const Vector& U = *pv->v;
+        const int64_t n = U.m->nc();
+        std::vector<double> flat(3 * n);  // flattenVector, export.cpp:139-151
+        for (int64_t c = 0; c < n; ++c)
+            for (int k = 0; k < 3; ++k) flat[3 * c + k] = U.c[k]->v[c];
+        auto r = cellToPoint(*U.m, flat.data(), 3);
+        std::copy(r.begin(), r.end(), point_data);
     })
 }
 

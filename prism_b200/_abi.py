@@ -56,7 +56,7 @@ class UnvMesh(C.Structure):
 class MeshInfo(C.Structure):
     _fields_ = [("n_cells", i64), ("n_faces", i64), ("n_boundary_faces", i64),
                 ("n_nonempty_boundary_faces", i64), ("nnz", i64), ("n_patches", i32),
-                ("n_gs_levels", i32)]
+                ("n_gs_levels", i32), ("n_vertices", i64), ("n_cell_vertices", i64)]
 
 
 class MeshExport(C.Structure):
@@ -64,7 +64,8 @@ class MeshExport(C.Structure):
                 ("face_normal", pf64), ("face_center", pf64), ("cell_volume", pf64),
                 ("cell_center", pf64), ("cell_face_offsets", pi64), ("cell_faces", pi64),
                 ("csr_rowptr", pi64), ("csr_col", pi64), ("patch_face_offsets", pi64),
-                ("patch_faces", pi64)]
+                ("patch_faces", pi64), ("vertex_coords", pf64), ("cell_vertex_offsets", pi64),
+                ("cell_vertices", pi64)]
 
 
 class BC(C.Structure):
@@ -141,6 +142,12 @@ SIGNATURES = {
     "vector_set_values": (C.c_int, [P, pf64]),
     "vector_get_values": (C.c_int, [P, pf64]),
     "vector_face_flux": (C.c_int, [P, pf64]),
+    "vector_set_face_flux": (C.c_int, [P, pf64]),
+    "ops_div": (C.c_int, [P, PP]),
+    "courant_number": (C.c_int, [P, f64, PP]),
+    "cell_to_point": (C.c_int, [P, pf64, i32, pf64]),
+    "scalar_to_points": (C.c_int, [P, pf64]),
+    "vector_to_points": (C.c_int, [P, pf64]),
     "tensor_create": (C.c_int, [P, C.c_char_p, pf64, PP]),
     "tensor_destroy": (C.c_int, [P]),
     "transport_create": (C.c_int, [P, PP]),

@@ -66,6 +66,7 @@ class Mesh:
         self.info = info
         self.n_cells = info.n_cells
         self.n_faces = info.n_faces
+        self.n_vertices = info.n_vertices
 
     def export(self):
         """Flattened PMesh + CSR pattern as numpy arrays (SoA vectors)."""
@@ -84,7 +85,9 @@ class Mesh:
             face_center=np.zeros(3 * nf), cell_volume=np.zeros(nc), cell_center=np.zeros(3 * nc),
             cell_face_offsets=cfo, cell_faces=np.zeros(max(1, cfo[-1]), np.int64),
             csr_rowptr=np.zeros(nc + 1, np.int64), csr_col=np.zeros(max(1, i.nnz), np.int64),
-            patch_face_offsets=pfo, patch_faces=np.zeros(max(1, pfo[-1]), np.int64))
+            patch_face_offsets=pfo, patch_faces=np.zeros(max(1, pfo[-1]), np.int64),
+            vertex_coords=np.zeros(3 * i.n_vertices), cell_vertex_offsets=np.zeros(nc + 1, np.int64),
+            cell_vertices=np.zeros(max(1, i.n_cell_vertices), np.int64))
         e = A.MeshExport()
         for k, v in out.items():
             ptype = dict(e._fields_)[k]
@@ -93,6 +96,33 @@ class Mesh:
         for k in ("face_normal", "face_center"):
             out[k] = out[k].reshape(3, nf)
         out["cell_center"] = out["cell_center"].reshape(3, nc)
+        out["vertex_coords"] = out["vertex_coords"].reshape(3, i.n_vertices)
+        return out
+
+    def topology(self):
+        """Vertices (n_vertices, 3) and the cells' vertex lists (offsets n_cells+1,
+        vertex ids in UNV element node order)."""
+        if getattr(self, "_topology", None) is None:
+            i = self.info
+            xyz = np.zeros(3 * i.n_vertices)
+            off = np.zeros(i.n_cells + 1, np.int64)
+            ids = np.zeros(max(1, i.n_cell_vertices), np.int64)
+            e = A.MeshExport()
+            e.vertex_coords = xyz.ctypes.data_as(A.pf64)
+            e.cell_vertex_offsets = off.ctypes.data_as(A.pi64)
+            e.cell_vertices = ids.ctypes.data_as(A.pi64)
+            self.lib.check(self.lib.mesh_export(self.h, C.byref(e)))
+            self._topology = (xyz.reshape(3, -1).T.copy(), off, ids[:i.n_cell_vertices])
+        return self._topology
+
+    def cell_to_point(self, cell_data, n_components=1):
+        """cellToPoint (export.cpp:73-111): inverse-distance weighted vertex values
+        of interleaved cell data (n_cells * n_components), interleaved per vertex."""
+        d = np.ascontiguousarray(cell_data, dtype=np.float64).reshape(-1)
+        if d.size != self.n_cells * n_components:
+            raise ValueError("cell_data must hold n_cells * n_components values")
+        out = np.zeros(self.n_vertices * n_components)
+        self.lib.check(self.lib.cell_to_point(self.h, _f64p(d), int(n_components), _f64p(out)))
         return out
 
     def __del__(self):
@@ -171,6 +201,12 @@ class Scalar:
         ok = C.c_int32()
         self.lib.check(self.lib.scalar_history(self.h, int(index), _f64p(out), C.byref(ok)))
         return out if ok.value else None
+
+    def to_points(self):
+        """cellToPoint of the cell values: one value per mesh vertex."""
+        out = np.zeros(self.mesh.n_vertices)
+        self.lib.check(self.lib.scalar_to_points(self.h, _f64p(out)))
+        return out
 
     def prev_values(self):
         return self.history(0)
@@ -252,6 +288,19 @@ class Vector:
         self.lib.check(self.lib.vector_face_flux(self.h, _f64p(out)))
         return out
 
+    def set_face_flux(self, flux):
+        """setFaceFluxValues: the n_faces fluxes fluxAtFace returns from now on."""
+        f = np.ascontiguousarray(flux, dtype=np.float64)
+        if f.size != self.mesh.n_faces:
+            raise ValueError("need one flux per face")
+        self.lib.check(self.lib.vector_set_face_flux(self.h, _f64p(f)))
+
+    def to_points(self):
+        """cellToPoint of the cell values, shape (n_vertices, 3)."""
+        out = np.zeros(3 * self.mesh.n_vertices)
+        self.lib.check(self.lib.vector_to_points(self.h, _f64p(out)))
+        return out.reshape(-1, 3)
+
     def __del__(self):
         if getattr(self, "h", None):
             self.lib.vector_destroy(self.h)
@@ -265,7 +314,7 @@ class Tensor:
     """field::Tensor; values (9, n_cells) SoA or None for the identity."""
 
     def __init__(self, name, mesh: Mesh, value=None):
-        self.mesh, self.lib = mesh, mesh.lib
+        self.mesh, self.lib, self.name = mesh, mesh.lib, name
         vals = None
         if value is not None:
             value = np.asarray(value, dtype=np.float64)
@@ -273,14 +322,93 @@ class Tensor:
                 vals = np.repeat(value.reshape(9, 1), mesh.n_cells, axis=1).reshape(-1).copy()
             else:
                 vals = np.ascontiguousarray(value, dtype=np.float64).reshape(-1)
+        # tensors are immutable through this API: the cell values are kept for export
+        self._values = (np.repeat(np.eye(3).reshape(9, 1), mesh.n_cells, axis=1) if vals is None
+                        else vals.reshape(9, -1).copy())
         h = C.c_void_p()
         self.lib.check(self.lib.tensor_create(mesh.h, name.encode(), _f64p(vals), C.byref(h)))
         self.h = h
+
+    def values(self):
+        """Cell values, shape (9, n_cells); row 3*i+j holds T(i, j)."""
+        return self._values.copy()
 
     def __del__(self):
         if getattr(self, "h", None):
             self.lib.tensor_destroy(self.h)
             self.h = None
+
+
+# ---- operations and monitors (operations/operations.h, monitor/courant.h) -----
+def _adopt_scalar(name, mesh, handle):
+    """Wrap a scalar handle created by the library (owned: destroyed with the wrapper)."""
+    s = Scalar.__new__(Scalar)
+    s.mesh, s.lib, s.name, s._owner, s._borrowed, s.h = mesh, mesh.lib, name, None, False, handle
+    return s
+
+
+class ops:  # noqa: N801  (namespace prism::ops)
+    @staticmethod
+    def div(U):
+        """ops::div (operations.h:84-100): Scalar "div(<name>)" = (sum of signed face
+        fluxes) / volume, computed on the device."""
+        h = C.c_void_p()
+        U.lib.check(U.lib.ops_div(U.h, C.byref(h)))
+        return _adopt_scalar(f"div({U.name})", U.mesh, h)
+
+    @staticmethod
+    def grad(field, coord=None):
+        """ops::grad (operations.h:102-141): of a Scalar, a Vector "grad(<name>)"
+        (or, with coord 0/1/2, the Scalar "grad(<name>)_<x|y|z>"); of a Vector, the
+        Tensor "grad(<name>)" with column j the gradient of component j."""
+        mesh = field.mesh
+        if isinstance(field, Scalar):
+            g = field.grad()
+            if coord is not None:
+                name = f"grad({field.name})_{'xyz'[coord]}"
+                return Scalar(name, mesh, g[coord], grad_scheme=A.GRAD_LEAST_SQUARES, bcs=_default_bcs(mesh))
+            return Vector(f"grad({field.name})", mesh, value=g, grad_scheme=A.GRAD_LEAST_SQUARES,
+                          bcs=_default_bcs(mesh))
+        if isinstance(field, Vector):
+            g = [field._component(k).grad() for k in range(3)]  # g[j][i] = d U_j / d x_i
+            t = np.empty((9, mesh.n_cells))
+            for i in range(3):
+                for j in range(3):
+                    t[3 * i + j] = g[j][i]
+            return Tensor(f"grad({field.name})", mesh, t)
+        raise TypeError("ops.grad needs a Scalar or a Vector")
+
+    @staticmethod
+    def symm(a):
+        """0.5 (A + A^T) (operations.h:185-187)."""
+        a = np.asarray(a, dtype=np.float64)
+        return 0.5 * (a + a.T)
+
+    @staticmethod
+    def two_symm(a):
+        """A + A^T (operations.h:189-191)."""
+        a = np.asarray(a, dtype=np.float64)
+        return a + a.T
+
+    @staticmethod
+    def dev(a):
+        """A - tr(A)/3 I (operations.h:193-195)."""
+        a = np.asarray(a, dtype=np.float64)
+        return a - np.eye(3) * (np.trace(a) / 3.0)
+
+    @staticmethod
+    def double_contraction(a, b):
+        """sum_ij A_ij B_ij (operations.h:197-199)."""
+        return float((np.asarray(a, dtype=np.float64) * np.asarray(b, dtype=np.float64)).sum())
+
+
+class monitor:  # noqa: N801  (namespace prism::monitor)
+    @staticmethod
+    def courant_number(mdot, dt):
+        """monitor::courantNumber (courant.cpp:7-24): Scalar "Co" = 0.5 dt sum|flux| / V."""
+        h = C.c_void_p()
+        mdot.lib.check(mdot.lib.courant_number(mdot.h, float(dt), C.byref(h)))
+        return _adopt_scalar("Co", mdot.mesh, h)
 
 
 # ---- schemes (descriptors consumed by Transport) ------------------------------

@@ -23,9 +23,9 @@ OBJ = os.path.join(HERE, "..", "_build", "obj")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
           "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-O2"]
-NO_FMA = {"assemble.cu", "gradient.cu", "coupling.cu", "pattern.cu", "adjoint.cu"}
+NO_FMA = {"assemble.cu", "gradient.cu", "coupling.cu", "pattern.cu", "adjoint.cu", "diag.cu"}
 SOURCES = ["mesh_build.cpp", "runtime.cpp", "capi.cpp", "pattern.cu", "assemble.cu", "gradient.cu",
-           "coupling.cu", "krylov.cu", "amg.cu", "adjoint.cu", "batched.cu", "noalloc.cu"]
+           "coupling.cu", "krylov.cu", "amg.cu", "adjoint.cu", "batched.cu", "noalloc.cu", "diag.cu"]
 
 
 def nvcc():

@@ -85,19 +85,6 @@ __device__ __forceinline__ void decompose(int corr, D3 S, D3 e, D3& E, D3& T) {
     T = S - E;
 }
 
-// ops::div flux sum (operations.h:144-169)
-__device__ __forceinline__ double fluxSum(const MeshView& m, const VectorView& U, int c) {
-    double sum = 0.0;
-    for (int q = m.cf_off[c]; q < m.cf_off[c + 1]; ++q) {
-        int f = m.cf_face[q];
-        if (f < m.nb && m.patch_empty[m.bpatch[f]]) continue;
-        double flux = vectorFlux(m, U, f);
-        if (m.owner[f] != c) flux = -flux;
-        sum += flux;
-    }
-    return sum;
-}
-
 __global__ void __launch_bounds__(256) assemble_kernel(const AssembleParams P) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const MeshView& m = P.m;

@@ -152,6 +152,8 @@ API int prism_mesh_info(const PrismMesh* pm, PrismMeshInfo* info) {
         info->nnz = m.pat.nnz;
         info->n_patches = m.npatch;
         info->n_gs_levels = (int32_t)m.level_off.size() - 1;
+        info->n_vertices = m.h->nv;
+        info->n_cell_vertices = m.h->cv_off[m.h->nc];
     });
 }
 API int prism_mesh_export(const PrismMesh* pm, PrismMeshExport* o) {
@@ -199,6 +201,10 @@ API int prism_mesh_export(const PrismMesh* pm, PrismMeshExport* o) {
             }
         }
         if (o->patch_face_offsets) o->patch_face_offsets[h.patches.size()] = pos;
+        for (int k = 0; k < 3; ++k)
+            if (o->vertex_coords) std::copy(h.vx[k].begin(), h.vx[k].end(), o->vertex_coords + k * h.nv);
+        if (o->cell_vertex_offsets) std::copy(h.cv_off.begin(), h.cv_off.end(), o->cell_vertex_offsets);
+        if (o->cell_vertices) std::copy(h.cv_node.begin(), h.cv_node.end(), o->cell_vertices);
     });
 }
 API int prism_mesh_destroy(PrismMesh* pm) {
@@ -455,6 +461,87 @@ API int prism_vector_face_flux(PrismVector* pv, double* out) {
                 }
         launchVectorFlux(m.view(), U.view(), m.scratch.p, m.stream);
         m.scratch.download(out, m.nf, m.stream);
+        sync(m);
+    });
+}
+
+// ---- diagnostics and point data
+namespace {
+PrismScalar* diagnosticScalar(Mesh& m, const std::string& name) {
+    // field::Scalar(name, mesh, data): no boundary handlers, least-squares gradient
+    std::vector<PrismBC> none(std::max(m.npatch, 1));
+    for (auto& b : none) {
+        std::memset(&b, 0, sizeof(PrismBC));
+        b.kind = PRISM_BC_UNKNOWN;
+    }
+    auto ps = std::make_unique<PrismScalar>();
+    ps->s = newScalar(m, name, nullptr, PRISM_GRAD_LEAST_SQUARES, none.data(), -1);
+    return ps.release();
+}
+void downloadPoints(Mesh& m, int ncomp, const double* const* comp, int64_t stride, double* out) {
+    DevBuf<double> pts((size_t)m.h->nv * ncomp);
+    cellToPoint(m, comp, ncomp, stride, pts.p);
+    pts.download(out, pts.n, m.stream);
+    sync(m);
+}
+}  // namespace
+
+API int prism_ops_div(PrismVector* pv, PrismScalar** out) {
+    return guard([&] {
+        ARG(pv && out, "null argument");
+        Vector& U = *pv->v;
+        std::unique_ptr<PrismScalar> ps(diagnosticScalar(*U.m, "div(" + U.name + ")"));
+        opsDiv(U, ps->s->v.p);
+        sync(*U.m);
+        *out = ps.release();
+    });
+}
+API int prism_courant_number(PrismVector* pv, double dt, PrismScalar** out) {
+    return guard([&] {
+        ARG(pv && out, "null argument");
+        Vector& U = *pv->v;
+        std::unique_ptr<PrismScalar> ps(diagnosticScalar(*U.m, "Co"));
+        courantNumber(U, dt, ps->s->v.p);
+        sync(*U.m);
+        *out = ps.release();
+    });
+}
+API int prism_cell_to_point(PrismMesh* pm, const double* cell_data, int32_t ncomp, double* point_data) {
+    return guard([&] {
+        ARG(pm && cell_data && point_data, "null argument");
+        ARG(ncomp >= 1 && ncomp <= 9, "n_components must be 1..9");
+        Mesh& m = *pm->m;
+        DevBuf<double> cells((size_t)m.nc * ncomp);
+        cells.upload(cell_data, cells.n, m.stream);
+        const double* comp[9];
+        for (int k = 0; k < ncomp; ++k) comp[k] = cells.p + k;
+        downloadPoints(m, ncomp, comp, ncomp, point_data);
+    });
+}
+API int prism_scalar_to_points(PrismScalar* ps, double* point_data) {
+    return guard([&] {
+        ARG(ps && point_data, "null argument");
+        const double* comp[1] = {ps->s->v.p};
+        downloadPoints(*ps->s->m, 1, comp, 1, point_data);
+    });
+}
+API int prism_vector_to_points(PrismVector* pv, double* point_data) {
+    return guard([&] {
+        ARG(pv && point_data, "null argument");
+        Vector& U = *pv->v;
+        const double* comp[3] = {U.c[0]->v.p, U.c[1]->v.p, U.c[2]->v.p};
+        downloadPoints(*U.m, 3, comp, 1, point_data);
+    });
+}
+
+API int prism_vector_set_face_flux(PrismVector* pv, const double* flux) {
+    return guard([&] {
+        ARG(pv && flux, "null argument");
+        Vector& U = *pv->v;
+        Mesh& m = *U.m;
+        if (U.ff.n < (size_t)m.nf) U.ff.alloc(std::max(m.nf, 1));
+        U.ff.upload(flux, m.nf, m.stream);
+        U.has_ff = true;
         sync(m);
     });
 }

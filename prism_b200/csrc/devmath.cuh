@@ -78,6 +78,20 @@ __device__ __forceinline__ double vectorFlux(const MeshView& m, const VectorView
     return dot(vectorFace(m, U, f), areaVector(m, f));
 }
 
+// ops::div flux sum (operations.h:144-169): signed fluxAtFace over the cell's
+// non-empty faces, in the cell's face order
+__device__ __forceinline__ double fluxSum(const MeshView& m, const VectorView& U, int c) {
+    double sum = 0.0;
+    for (int q = m.cf_off[c]; q < m.cf_off[c + 1]; ++q) {
+        int f = m.cf_face[q];
+        if (f < m.nb && m.patch_empty[m.bpatch[f]]) continue;
+        double flux = vectorFlux(m, U, f);
+        if (m.owner[f] != c) flux = -flux;
+        sum += flux;
+    }
+    return sum;
+}
+
 // T^T v with a cell or an interpolated face tensor (diffusion_coeff.cpp:21-30).
 __device__ __forceinline__ double tget(const TensorView& T, int i, int j, int c) {
     if (T.diag) return i == j ? T.d[i * T.stride + c] : 0.0;

@@ -101,7 +101,7 @@ void faceGeometry(const V3* fv, int n, double& area, V3& normal, V3& center) {
 std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
     if (!d) fail(PRISM_BAD_ARG, "null mesh description");
     if (d->n_nodes <= 0) fail(PRISM_INVALID_MESH, "UnvToPMeshConverter(): mesh has zero vertices");
-    if (d->n_nodes >= (int64_t(1) << 32)) fail(PRISM_INVALID_MESH, "too many nodes");
+    if (d->n_nodes >= (int64_t(1) << 31)) fail(PRISM_INVALID_MESH, "too many nodes");
     const int64_t ne = d->n_elements;
     std::vector<V3> X(d->n_nodes);
     for (int64_t i = 0; i < d->n_nodes; ++i) X[i] = {d->xyz[3 * i], d->xyz[3 * i + 1], d->xyz[3 * i + 2]};
@@ -327,6 +327,23 @@ std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
         V3 ef = divs(Sf, std::sqrt(dot(Sf, Sf)));
         V3 dCf = sub(fcv, co), dfN = sub(cn, fcv);
         hm->gc[f - nb] = dot(dCf, ef) / (dot(dCf, ef) + dot(dfN, ef));
+    }
+    // vertices and cell vertex lists (kept for point data and export)
+    hm->nv = d->n_nodes;
+    for (int k = 0; k < 3; ++k) {
+        hm->vx[k].resize(d->n_nodes);
+        for (int64_t i = 0; i < d->n_nodes; ++i) hm->vx[k][i] = d->xyz[3 * i + k];
+    }
+    hm->cv_off.assign(nc + 1, 0);
+    for (int64_t c = 0; c < nc; ++c) {
+        int64_t e = cell_elem[c];
+        hm->cv_off[c + 1] = hm->cv_off[c] + (d->elem_offsets[e + 1] - d->elem_offsets[e]);
+    }
+    hm->cv_node.resize(hm->cv_off[nc]);
+    for (int64_t c = 0; c < nc; ++c) {
+        int64_t e = cell_elem[c];
+        const int64_t* en = d->elem_nodes + d->elem_offsets[e];
+        for (int64_t q = hm->cv_off[c]; q < hm->cv_off[c + 1]; ++q) hm->cv_node[q] = (int32_t)en[q - hm->cv_off[c]];
     }
     return hm;
 }

@@ -17,6 +17,11 @@ struct HostMesh {
     std::vector<double> gc;                  // per interior face (index f - nb)
     std::vector<int64_t> cf_off;             // cell -> faces (reference local order)
     std::vector<int32_t> cf_face;
+    // PMesh::vertices() (every UNV node) and Cell::verticesIds() (element node order)
+    int64_t nv = 0;
+    std::vector<double> vx[3];
+    std::vector<int64_t> cv_off;
+    std::vector<int32_t> cv_node;
     struct Patch {
         std::string name;
         bool empty = false;

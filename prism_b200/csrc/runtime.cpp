@@ -11,6 +11,7 @@
 
 #include "adjoint.h"
 #include "coupling.h"
+#include "diag.h"
 #include "gradient.h"
 
 namespace pb {
@@ -968,6 +969,65 @@ std::vector<PrismSolveResult> solveBatch(BatchHandle& h, std::vector<Transport*>
                      ms(t1, t2), ms(t2, std::chrono::steady_clock::now()));
     }
     return res;
+}
+
+// ------------------------------------------------------------------ diagnostics
+// ops::div (operations.h:84-100)
+void opsDiv(Vector& U, double* out) {
+    checkVectorFlux(U, "ops::div()");
+    Mesh& m = *U.m;
+    launchDiv(m.view(), U.view(), out, m.stream);
+}
+
+// monitor::courantNumber (courant.cpp:7-24)
+void courantNumber(Vector& mdot, double dt, double* out) {
+    checkVectorFlux(mdot, "monitor::courantNumber()");
+    Mesh& m = *mdot.m;
+    launchCourant(m.view(), mdot.view(), dt, out, m.stream);
+}
+
+// ensureCache (export.cpp:44-71): vertex -> cells in cell order, built once per mesh
+void ensurePointMap(Mesh& m) {
+    if (m.points_ready) return;
+    const HostMesh& h = *m.h;
+    const int64_t nv = h.nv, nc = h.nc;
+    std::vector<int64_t> off(nv + 1, 0);
+    for (int64_t q = 0; q < h.cv_off[nc]; ++q) off[h.cv_node[q] + 1]++;
+    for (int64_t v = 0; v < nv; ++v) {
+        if (off[v + 1] == 0)
+            fail(PRISM_INVALID_MESH,
+                 "Vertex " + std::to_string(v) + " has no adjacent cells; point data cannot be computed.");
+        off[v + 1] += off[v];
+    }
+    std::vector<int> cell(off[nv]);
+    std::vector<int64_t> fill(off.begin(), off.end() - 1);
+    for (int64_t c = 0; c < nc; ++c)
+        for (int64_t q = h.cv_off[c]; q < h.cv_off[c + 1]; ++q) cell[fill[h.cv_node[q]]++] = (int)c;
+    std::vector<double> xyz(3 * nv);
+    for (int k = 0; k < 3; ++k) std::copy(h.vx[k].begin(), h.vx[k].end(), xyz.begin() + k * nv);
+    m.vtx.upload(xyz, m.stream);
+    m.v2c_off.upload(off, m.stream);
+    m.v2c_cell.upload(cell, m.stream);
+    PB_CUDA(cudaStreamSynchronize(m.stream));
+    m.points_ready = true;
+}
+
+// cellToPoint (export.cpp:73-111)
+void cellToPoint(Mesh& m, const double* const* comp, int ncomp, int64_t stride, double* out) {
+    if (ncomp < 1 || ncomp > MAX_POINT_COMPONENTS) fail(PRISM_BAD_ARG, "n_components must be 1..9");
+    ensurePointMap(m);
+    PointMapView pm;
+    pm.nv = m.h->nv;
+    pm.vx = m.vtx.p;
+    pm.vy = m.vtx.p + pm.nv;
+    pm.vz = m.vtx.p + 2 * pm.nv;
+    pm.off = m.v2c_off.p;
+    pm.cell = m.v2c_cell.p;
+    PointComponents pc;
+    for (int k = 0; k < ncomp; ++k) pc.p[k] = comp[k];
+    pc.stride = stride;
+    pc.ncomp = ncomp;
+    launchCellToPoint(m.view(), pm, pc, out, m.stream);
 }
 
 }  // namespace pb

@@ -45,6 +45,11 @@ struct Mesh {
     std::unique_ptr<Tensor> p_D;
     std::unique_ptr<Transport> p_eq;
     DevBuf<double> scratch;  // n_faces doubles for face exports
+    // vertex -> cells map and vertex coordinates for point data (built on first use)
+    DevBuf<double> vtx;
+    DevBuf<int64_t> v2c_off;
+    DevBuf<int> v2c_cell;
+    bool points_ready = false;
 
     ~Mesh();
     MeshView view() const;
@@ -133,6 +138,13 @@ void updateCoeffs(Transport& eq);
 void relax(Transport& eq);
 void zeroOutCoeffs(Transport& eq);
 PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o);
+
+// diagnostics into device buffers of n_cells values; cellToPoint writes
+// n_vertices * ncomp interleaved values, component k of cell c read from
+// comp[k][c * stride]
+void opsDiv(Vector& U, double* out);
+void courantNumber(Vector& mdot, double dt, double* out);
+void cellToPoint(Mesh& m, const double* const* comp, int ncomp, int64_t stride, double* out);
 
 struct Report {
     std::string name;

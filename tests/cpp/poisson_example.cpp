@@ -71,5 +71,18 @@ int main(int argc, char** argv) {
     solver::BiCGSTAB solver;
     for (int i = 0; i < 5; ++i) solver.solve(eq, 15, 1e-20);
     for (double v : P->values()) std::printf("%.17g\n", v);
+    // diagnostics of a uniform flow (1, 0, 0) through the same mesh, on stderr:
+    // Courant number 0.5 * dt * 2u/h = u dt n everywhere, zero divergence, and the
+    // solution interpolated to the vertices
+    std::vector<field::BC> ubc(patches.size());
+    for (size_t p = 0; p < patches.size(); ++p)
+        ubc[p] = patches[p].empty ? field::BC{PRISM_BC_EMPTY, PRISM_BCV_NIL, 0.0, {0, 0, 0}}
+                                  : field::BC{PRISM_BC_FIXED, PRISM_BCV_VECTOR, 0.0, {1, 0, 0}};
+    const double u0[3] = {1.0, 0.0, 0.0};
+    field::Vector U("U", pm, u0, ubc);
+    auto co = monitor::courantNumber(U, 0.01).values();
+    auto dv = ops::div(U).values();
+    auto pts = P->toPoints();
+    std::fprintf(stderr, "Co[0] %.6g div[0] %.3g points %zu\n", co[0], dv[0], pts.size());
     return 0;
 }
