@@ -35,6 +35,7 @@
  *   prism_prime_step         algorithm/PRIME.cpp:11-37 PRIME::step
  *   prism_piso_step          algorithm/PISO.cpp:10-55 PISO::step
  *   prism_needs_pressure_reference  algorithm/SIMPLE.cpp:110-122
+ *   prism_mesh_reorder       mesh/reorder.h:9-13 CuthillMckee::reorder
  *   prism_ops_div            operations/operations.h:84-100 ops::div
  *   prism_courant_number     monitor/courant.cpp:7-24 monitor::courantNumber
  *   prism_cell_to_point      export.cpp:73-111 (anonymous) cellToPoint
@@ -187,12 +188,21 @@ typedef struct {
     double* vertex_coords;        /* 3*n_vertices */
     int64_t* cell_vertex_offsets; /* n_cells+1 */
     int64_t* cell_vertices;       /* n_cell_vertices: UNV element node order (cell.h:25) */
+    int64_t* cell_original;       /* n_cells: each cell's id before prism_mesh_reorder */
 } PrismMeshExport;
 
 int prism_mesh_from_unv(const PrismUnvMesh* desc, PrismMesh** out);
 int prism_mesh_info(const PrismMesh* mesh, PrismMeshInfo* info);
 int prism_mesh_export(const PrismMesh* mesh, PrismMeshExport* out);
 int prism_mesh_destroy(PrismMesh* mesh);
+/* mesh::CuthillMckee(mesh).reorder(reverse) (mesh/reorder.cpp:8-130): renumbers
+ * the cells in (reverse) Cuthill-McKee order -- breadth first from the
+ * lowest-degree unvisited cell, neighbours appended by ascending degree, ties
+ * as the reference's std::sort leaves them; faces keep their ids and order.
+ * Opt-in; call before any field is created on the mesh (PRISM_BAD_ARG after),
+ * since field values are indexed by cell id. Volumes follow their cells (the
+ * reference's cached volume vector is left in the old order). */
+int prism_mesh_reorder(PrismMesh* mesh, int32_t reverse);
 
 /* ---- fields -------------------------------------------------------------- */
 /* Boundary condition of one patch for one field (mesh/boundary.h:86-111). */

@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <limits>
 #include <map>
 #include <memory>
@@ -185,6 +186,8 @@ struct Mesh {
     int64_t n_boundary = 0, n_nonempty = 0;
     std::vector<int64_t> rowptr, col; // CSR pattern (setFromTriplets of all inserts)
     std::vector<double> volumes;
+    std::vector<int64_t> cell_orig;   // cell id before any reordering
+    bool frozen = false;              // fields exist: the cells can no longer be renumbered
 
     int64_t nc() const { return (int64_t)cells.size(); }
     int64_t nf() const { return (int64_t)faces.size(); }
@@ -230,6 +233,34 @@ struct VecHash {
         return h;
     }
 };
+
+// cached volumes (pmesh.cpp:45-47) and the pattern produced by setFromTriplets of
+// the assembly inserts (linear.cpp:21-28): each row holds its diagonal and its
+// face neighbours, sorted by column.
+void finishMesh(Mesh& m) {
+    m.volumes.resize(m.cells.size());
+    for (size_t c = 0; c < m.cells.size(); ++c) m.volumes[c] = m.cells[c].volume;
+    if (m.cell_orig.size() != m.cells.size()) {
+        m.cell_orig.resize(m.cells.size());
+        for (size_t c = 0; c < m.cells.size(); ++c) m.cell_orig[c] = (int64_t)c;
+    }
+    int64_t nc = m.nc();
+    std::vector<std::vector<int64_t>> rows(nc);
+    for (int64_t c = 0; c < nc; ++c) rows[c].push_back(c);
+    for (int64_t f = m.n_boundary; f < m.nf(); ++f) {
+        rows[m.faces[f].owner].push_back(m.faces[f].nbr);
+        rows[m.faces[f].nbr].push_back(m.faces[f].owner);
+    }
+    m.rowptr.assign(nc + 1, 0);
+    for (int64_t c = 0; c < nc; ++c) {
+        std::sort(rows[c].begin(), rows[c].end());
+        rows[c].erase(std::unique(rows[c].begin(), rows[c].end()), rows[c].end());
+        m.rowptr[c + 1] = m.rowptr[c] + (int64_t)rows[c].size();
+    }
+    m.col.clear();
+    m.col.reserve(m.rowptr[nc]);
+    for (auto& r : rows) m.col.insert(m.col.end(), r.begin(), r.end());
+}
 
 std::unique_ptr<Mesh> buildFromUnv(const PrismUnvMesh* d) {
     auto m = std::make_unique<Mesh>();
@@ -380,27 +411,80 @@ std::unique_ptr<Mesh> buildFromUnv(const PrismUnvMesh* d) {
     m->n_nonempty = n_nonempty;
     for (int64_t f = 0; f < n_boundary; ++f)
         if (faces[f].nbr >= 0) fail(PRISM_INVALID_MESH, "boundary face with two cells");
-    m->volumes.resize(cells.size());
-    for (size_t c = 0; c < cells.size(); ++c) m->volumes[c] = cells[c].volume;
-
-    // Pattern produced by setFromTriplets of the assembly inserts (linear.cpp:21-28):
-    // each row holds its diagonal and its face neighbours, sorted by column.
-    int64_t nc = (int64_t)cells.size();
-    std::vector<std::vector<int64_t>> rows(nc);
-    for (int64_t c = 0; c < nc; ++c) rows[c].push_back(c);
-    for (int64_t f = n_boundary; f < n_faces; ++f) {
-        rows[faces[f].owner].push_back(faces[f].nbr);
-        rows[faces[f].nbr].push_back(faces[f].owner);
-    }
-    m->rowptr.assign(nc + 1, 0);
-    for (int64_t c = 0; c < nc; ++c) {
-        std::sort(rows[c].begin(), rows[c].end());
-        rows[c].erase(std::unique(rows[c].begin(), rows[c].end()), rows[c].end());
-        m->rowptr[c + 1] = m->rowptr[c] + (int64_t)rows[c].size();
-    }
-    m->col.reserve(m->rowptr[nc]);
-    for (auto& r : rows) m->col.insert(m->col.end(), r.begin(), r.end());
+    finishMesh(*m);
     return m;
+}
+
+// CuthillMckee (mesh/reorder.cpp:8-130), restated with the reference's own data
+// structures: nodes sorted by degree (std::sort), a deque of not-visited nodes
+// searched linearly, the not-visited neighbours of the queue front sorted by
+// degree (std::sort) and appended. O(n^2): small meshes only.
+struct RcmNode {
+    size_t id = 0, degree = 0;
+    std::vector<size_t> nbrs;
+};
+std::vector<size_t> cuthillMckeePermute(const Mesh& m) {
+    std::vector<RcmNode> nodes;
+    nodes.reserve(m.cells.size());
+    for (size_t c = 0; c < m.cells.size(); ++c) {
+        RcmNode node{c, 0, {}};
+        for (auto f : m.cells[c].faces) {
+            const Face& fc = m.faces[f];
+            if (fc.nbr < 0) continue;
+            node.nbrs.push_back((size_t)(fc.owner == (int64_t)c ? fc.nbr : fc.owner));
+            node.degree++;
+        }
+        nodes.push_back(std::move(node));
+    }
+    auto byDegree = [](const RcmNode& a, const RcmNode& b) { return a.degree < b.degree; };
+    std::sort(nodes.begin(), nodes.end(), byDegree);
+    std::vector<size_t> perm;
+    std::deque<RcmNode> queue;
+    std::deque<RcmNode> not_visited(nodes.begin(), nodes.end());
+    while (!not_visited.empty()) {
+        queue.push_back(not_visited.front());
+        not_visited.pop_front();
+        while (!queue.empty()) {
+            std::vector<RcmNode> nv;
+            for (auto nid : queue.front().nbrs) {
+                auto it = std::find_if(not_visited.begin(), not_visited.end(),
+                                       [nid](const RcmNode& n) { return n.id == nid; });
+                if (it != not_visited.end()) {
+                    nv.push_back(*it);
+                    not_visited.erase(it);
+                }
+            }
+            std::sort(nv.begin(), nv.end(), byDegree);
+            queue.insert(queue.end(), nv.begin(), nv.end());
+            perm.push_back(queue.front().id);
+            queue.pop_front();
+        }
+    }
+    return perm;
+}
+
+// CuthillMckee::reorder, reorder.cpp:89-129: cells move to their new ids, faces keep
+// theirs with owner/neighbour renamed. The reference leaves PMesh's cached volume
+// vector (pmesh.cpp:45-47) in the old order; here it follows the cells, and the
+// matrix pattern is rebuilt for the new numbering.
+void reorderCells(Mesh& m, bool reverse) {
+    auto perm = cuthillMckeePermute(m);
+    if (reverse) std::reverse(perm.begin(), perm.end());
+    std::vector<int64_t> old_to_new(perm.size());
+    for (size_t i = 0; i < perm.size(); ++i) old_to_new[perm[i]] = (int64_t)i;
+    std::vector<Cell> nc(m.cells.size());
+    std::vector<int64_t> orig(m.cells.size());
+    for (size_t i = 0; i < perm.size(); ++i) {
+        nc[i] = m.cells[perm[i]];
+        orig[i] = m.cell_orig[perm[i]];
+    }
+    m.cells.swap(nc);
+    m.cell_orig.swap(orig);
+    for (auto& f : m.faces) {
+        f.owner = old_to_new[f.owner];
+        if (f.nbr >= 0) f.nbr = old_to_new[f.nbr];
+    }
+    finishMesh(m);
 }
 
 // ---------------------------------------------------------------- fields
@@ -1667,14 +1751,23 @@ ORC_API int orc_mesh_export(const PrismMesh* pm, PrismMeshExport* o) {
             }
         }
         if (o->cell_vertex_offsets) o->cell_vertex_offsets[nc] = pos;
+        if (o->cell_original) std::copy(m.cell_orig.begin(), m.cell_orig.end(), o->cell_original);
     })
 }
 ORC_API int orc_mesh_destroy(PrismMesh* pm) { GUARD({ delete pm; }) }
+ORC_API int orc_mesh_reorder(PrismMesh* pm, int32_t reverse) {
+    GUARD({
+        CHECK_ARG(pm, "null argument");
+        CHECK_ARG(!pm->m->frozen, "reorder the mesh before creating fields on it");
+        reorderCells(*pm->m, reverse != 0);
+    })
+}
 
 ORC_API int orc_scalar_create(PrismMesh* pm, const char* name, const double* values, int32_t grad_scheme,
                               const PrismBC* bcs, PrismScalar** out) {
     GUARD({
         CHECK_ARG(pm && name && bcs && out, "null argument");
+        pm->m->frozen = true;
         CHECK_ARG(grad_scheme == PRISM_GRAD_LEAST_SQUARES || grad_scheme == PRISM_GRAD_GREEN_GAUSS, "bad gradient scheme");
         auto s = std::make_shared<Scalar>();
         s->m = pm->m.get();
@@ -1771,6 +1864,7 @@ ORC_API int orc_vector_create(PrismMesh* pm, const char* name, const double* val
                               const PrismBC* bcs, PrismVector** out) {
     GUARD({
         CHECK_ARG(pm && name && bcs && out, "null argument");
+        pm->m->frozen = true;
         CHECK_ARG(grad_scheme == PRISM_GRAD_LEAST_SQUARES || grad_scheme == PRISM_GRAD_GREEN_GAUSS, "bad gradient scheme");
         auto* pv = new PrismVector();
         pv->v = std::make_unique<Vector>();
@@ -1969,6 +2063,7 @@ ORC_API int orc_vector_to_points(PrismVector* pv, double* point_data) {
 ORC_API int orc_tensor_create(PrismMesh* pm, const char* name, const double* values, PrismTensor** out) {
     GUARD({
         CHECK_ARG(pm && out, "null argument");
+        pm->m->frozen = true;
         (void)name;
         auto* pt = new PrismTensor();
         pt->t = std::make_unique<Tensor>();

@@ -65,7 +65,7 @@ class MeshExport(C.Structure):
                 ("cell_center", pf64), ("cell_face_offsets", pi64), ("cell_faces", pi64),
                 ("csr_rowptr", pi64), ("csr_col", pi64), ("patch_face_offsets", pi64),
                 ("patch_faces", pi64), ("vertex_coords", pf64), ("cell_vertex_offsets", pi64),
-                ("cell_vertices", pi64)]
+                ("cell_vertices", pi64), ("cell_original", pi64)]
 
 
 class BC(C.Structure):
@@ -127,6 +127,7 @@ SIGNATURES = {
     "mesh_info": (C.c_int, [P, C.POINTER(MeshInfo)]),
     "mesh_export": (C.c_int, [P, C.POINTER(MeshExport)]),
     "mesh_destroy": (C.c_int, [P]),
+    "mesh_reorder": (C.c_int, [P, i32]),
     "scalar_create": (C.c_int, [P, C.c_char_p, pf64, i32, C.POINTER(BC), PP]),
     "scalar_destroy": (C.c_int, [P]),
     "scalar_set_values": (C.c_int, [P, pf64]),

@@ -87,7 +87,8 @@ class Mesh:
             csr_rowptr=np.zeros(nc + 1, np.int64), csr_col=np.zeros(max(1, i.nnz), np.int64),
             patch_face_offsets=pfo, patch_faces=np.zeros(max(1, pfo[-1]), np.int64),
             vertex_coords=np.zeros(3 * i.n_vertices), cell_vertex_offsets=np.zeros(nc + 1, np.int64),
-            cell_vertices=np.zeros(max(1, i.n_cell_vertices), np.int64))
+            cell_vertices=np.zeros(max(1, i.n_cell_vertices), np.int64),
+            cell_original=np.zeros(nc, np.int64))
         e = A.MeshExport()
         for k, v in out.items():
             ptype = dict(e._fields_)[k]
@@ -98,6 +99,13 @@ class Mesh:
         out["cell_center"] = out["cell_center"].reshape(3, nc)
         out["vertex_coords"] = out["vertex_coords"].reshape(3, i.n_vertices)
         return out
+
+    def reorder(self, reverse=False):
+        """CuthillMckee(mesh).reorder(reverse) (mesh/reorder.cpp): renumbers the cells in
+        (reverse) Cuthill-McKee order. Call before creating fields on the mesh;
+        export()["cell_original"] maps each new cell id to its id before reordering."""
+        self.lib.check(self.lib.mesh_reorder(self.h, 1 if reverse else 0))
+        self._topology = None
 
     def topology(self):
         """Vertices (n_vertices, 3) and the cells' vertex lists (offsets n_cells+1,

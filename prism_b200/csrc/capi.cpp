@@ -205,10 +205,17 @@ API int prism_mesh_export(const PrismMesh* pm, PrismMeshExport* o) {
             if (o->vertex_coords) std::copy(h.vx[k].begin(), h.vx[k].end(), o->vertex_coords + k * h.nv);
         if (o->cell_vertex_offsets) std::copy(h.cv_off.begin(), h.cv_off.end(), o->cell_vertex_offsets);
         if (o->cell_vertices) std::copy(h.cv_node.begin(), h.cv_node.end(), o->cell_vertices);
+        if (o->cell_original) std::copy(h.cell_orig.begin(), h.cell_orig.end(), o->cell_original);
     });
 }
 API int prism_mesh_destroy(PrismMesh* pm) {
     return guard([&] { delete pm; });
+}
+API int prism_mesh_reorder(PrismMesh* pm, int32_t reverse) {
+    return guard([&] {
+        ARG(pm, "null argument");
+        reorderMesh(*pm->m, reverse != 0);
+    });
 }
 
 // ---- scalar
@@ -216,6 +223,7 @@ API int prism_scalar_create(PrismMesh* pm, const char* name, const double* value
                             PrismScalar** out) {
     return guard([&] {
         ARG(pm && name && bcs && out, "null argument");
+        pm->m->frozen = true;
         ARG(grad == PRISM_GRAD_LEAST_SQUARES || grad == PRISM_GRAD_GREEN_GAUSS, "bad gradient scheme");
         auto ps = std::make_unique<PrismScalar>();
         ps->s = newScalar(*pm->m, name, values, grad, bcs, -1);
@@ -337,6 +345,7 @@ API int prism_vector_create(PrismMesh* pm, const char* name, const double* value
                             PrismVector** out) {
     return guard([&] {
         ARG(pm && name && bcs && out, "null argument");
+        pm->m->frozen = true;
         ARG(grad == PRISM_GRAD_LEAST_SQUARES || grad == PRISM_GRAD_GREEN_GAUSS, "bad gradient scheme");
         Mesh& m = *pm->m;
         auto pv = std::make_unique<PrismVector>();
@@ -550,6 +559,7 @@ API int prism_vector_set_face_flux(PrismVector* pv, const double* flux) {
 API int prism_tensor_create(PrismMesh* pm, const char* name, const double* values, PrismTensor** out) {
     return guard([&] {
         ARG(pm && out, "null argument");
+        pm->m->frozen = true;
         (void)name;
         Mesh& m = *pm->m;
         auto pt = std::make_unique<PrismTensor>();

@@ -345,7 +345,90 @@ std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
         const int64_t* en = d->elem_nodes + d->elem_offsets[e];
         for (int64_t q = hm->cv_off[c]; q < hm->cv_off[c + 1]; ++q) hm->cv_node[q] = (int32_t)en[q - hm->cv_off[c]];
     }
+    hm->cell_orig.resize(nc);
+    std::iota(hm->cell_orig.begin(), hm->cell_orig.end(), 0);
     return hm;
+}
+
+// The reference keeps a deque of not-visited nodes and searches it linearly
+// (O(n^2)); a node leaves that deque exactly when it is enqueued, so an
+// "enqueued" flag per cell and a cursor over the degree-sorted list give the
+// same sequence in O(n log n). Both std::sort calls see the same sequences
+// with the same comparator as the reference's, so ties resolve alike.
+std::vector<int64_t> cuthillMckee(const HostMesh& h) {
+    struct Node {
+        int64_t id, degree;
+    };
+    const int64_t nc = h.nc;
+    std::vector<Node> nodes(nc);
+    for (int64_t c = 0; c < nc; ++c) {
+        int64_t d = 0;
+        for (int64_t q = h.cf_off[c]; q < h.cf_off[c + 1]; ++q)
+            if (h.nbr[h.cf_face[q]] >= 0) ++d;
+        nodes[c] = {c, d};
+    }
+    auto byDegree = [](const Node& a, const Node& b) { return a.degree < b.degree; };
+    std::vector<Node> sorted = nodes;
+    std::sort(sorted.begin(), sorted.end(), byDegree);
+    std::vector<char> enqueued(nc, 0);
+    std::vector<Node> queue(nc), nv;
+    std::vector<int64_t> perm;
+    perm.reserve(nc);
+    int64_t head = 0, tail = 0;
+    size_t cursor = 0;
+    while ((int64_t)perm.size() < nc) {
+        while (enqueued[sorted[cursor].id]) ++cursor;
+        enqueued[sorted[cursor].id] = 1;
+        queue[tail++] = sorted[cursor];
+        while (head < tail) {
+            const int64_t c = queue[head].id;
+            nv.clear();
+            for (int64_t q = h.cf_off[c]; q < h.cf_off[c + 1]; ++q) {
+                const int32_t f = h.cf_face[q];
+                if (h.nbr[f] < 0) continue;
+                const int64_t n = h.owner[f] == c ? h.nbr[f] : h.owner[f];
+                if (enqueued[n]) continue;
+                enqueued[n] = 1;
+                nv.push_back(nodes[n]);
+            }
+            std::sort(nv.begin(), nv.end(), byDegree);
+            for (const Node& x : nv) queue[tail++] = x;
+            perm.push_back(c);
+            ++head;
+        }
+    }
+    return perm;
+}
+
+void permuteCells(HostMesh& h, const std::vector<int64_t>& perm) {
+    const int64_t nc = h.nc;
+    if ((int64_t)perm.size() != nc) fail(PRISM_INTERNAL, "permutation size");
+    std::vector<int32_t> o2n(nc);
+    for (int64_t i = 0; i < nc; ++i) o2n[perm[i]] = (int32_t)i;
+    auto gather = [&](auto& v) {
+        auto old = v;
+        for (int64_t i = 0; i < nc; ++i) v[i] = old[perm[i]];
+    };
+    for (int k = 0; k < 3; ++k) gather(h.cc[k]);
+    gather(h.vol);
+    gather(h.cell_orig);
+    auto lists = [&](std::vector<int64_t>& off, auto& items) {
+        std::vector<int64_t> noff(nc + 1, 0);
+        auto nitems = items;
+        for (int64_t i = 0; i < nc; ++i) {
+            const int64_t b = off[perm[i]], e = off[perm[i] + 1];
+            noff[i + 1] = noff[i] + (e - b);
+            std::copy(items.begin() + b, items.begin() + e, nitems.begin() + noff[i]);
+        }
+        off.swap(noff);
+        items.swap(nitems);
+    };
+    lists(h.cf_off, h.cf_face);
+    lists(h.cv_off, h.cv_node);
+    for (int64_t f = 0; f < h.nf; ++f) {
+        h.owner[f] = o2n[h.owner[f]];
+        if (h.nbr[f] >= 0) h.nbr[f] = o2n[h.nbr[f]];
+    }
 }
 
 }  // namespace pb

@@ -22,6 +22,7 @@ struct HostMesh {
     std::vector<double> vx[3];
     std::vector<int64_t> cv_off;
     std::vector<int32_t> cv_node;
+    std::vector<int64_t> cell_orig;  // id of each cell before any reordering
     struct Patch {
         std::string name;
         bool empty = false;
@@ -31,5 +32,12 @@ struct HostMesh {
 };
 
 std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d);
+
+// CuthillMckee::permute (mesh/reorder.cpp:40-87): new -> old cell ids
+std::vector<int64_t> cuthillMckee(const HostMesh& h);
+// CuthillMckee::reorder (reorder.cpp:89-129) on the host arrays: cells (centres,
+// volumes, face and vertex lists) move to their new ids, faces keep theirs with
+// owner and neighbour renamed
+void permuteCells(HostMesh& h, const std::vector<int64_t>& new_to_old);
 
 }  // namespace pb

@@ -139,14 +139,10 @@ SellMatrix Mesh::matrix(const double* vals) const {
     return A;
 }
 
-std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d) {
-    auto mesh = std::make_unique<Mesh>();
-    mesh->h = buildHostMesh(d);
-    HostMesh& h = *mesh->h;
-    if (h.nc >= (int64_t(1) << 31) || h.nf >= (int64_t(1) << 31) || (int64_t)h.cf_face.size() >= (int64_t(1) << 31))
-        fail(PRISM_INVALID_MESH, "mesh too large for 32-bit indices");
-    Mesh& m = *mesh;
-    PB_CUDA(cudaStreamCreateWithFlags(&m.stream, cudaStreamNonBlocking));
+namespace {
+// device copy of the host mesh, the matrix pattern and the Green-Gauss schedule
+void setupDevice(Mesh& m) {
+    HostMesh& h = *m.h;
     cudaStream_t s = m.stream;
     m.nc = (int)h.nc;
     m.nf = (int)h.nf;
@@ -206,8 +202,32 @@ std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d) {
     for (int c = 0; c < m.nc; ++c) lc[fill[level[c]]++] = c;
     upload(m.level_cells, lc, s);
     m.scratch.alloc(std::max(3 * m.nf, 1));
+    m.ls_ready = false;
+    m.points_ready = false;
     PB_CUDA(cudaStreamSynchronize(s));
+}
+}  // namespace
+
+std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d) {
+    auto mesh = std::make_unique<Mesh>();
+    mesh->h = buildHostMesh(d);
+    const HostMesh& h = *mesh->h;
+    if (h.nc >= (int64_t(1) << 31) || h.nf >= (int64_t(1) << 31) || (int64_t)h.cf_face.size() >= (int64_t(1) << 31))
+        fail(PRISM_INVALID_MESH, "mesh too large for 32-bit indices");
+    PB_CUDA(cudaStreamCreateWithFlags(&mesh->stream, cudaStreamNonBlocking));
+    setupDevice(*mesh);
     return mesh;
+}
+
+// CuthillMckee(mesh).reorder(reverse) (reorder.cpp:89-129); nothing on the
+// device refers to the old numbering yet (no fields exist), so the device copy
+// is rebuilt from the permuted host mesh
+void reorderMesh(Mesh& m, bool reverse) {
+    if (m.frozen) fail(PRISM_BAD_ARG, "reorder the mesh before creating fields on it");
+    std::vector<int64_t> perm = cuthillMckee(*m.h);
+    if (reverse) std::reverse(perm.begin(), perm.end());
+    permuteCells(*m.h, perm);
+    setupDevice(m);
 }
 
 // LeastSquares::setPseudoInvMatrices (least_squares.cpp:12-61): pinv = (D^T D)^-1 D^T

@@ -50,6 +50,7 @@ struct Mesh {
     DevBuf<int64_t> v2c_off;
     DevBuf<int> v2c_cell;
     bool points_ready = false;
+    bool frozen = false;  // fields exist: the cells can no longer be renumbered
 
     ~Mesh();
     MeshView view() const;
@@ -58,6 +59,7 @@ struct Mesh {
 };
 
 std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d);
+void reorderMesh(Mesh& m, bool reverse);
 
 struct GradState {
     int type = PRISM_GRAD_LEAST_SQUARES;

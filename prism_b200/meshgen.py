@@ -128,3 +128,20 @@ def box_tet(nx, ny, nz, lengths=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0), jitter=
         t2 = np.where(first[:, None], np.stack([a, cc, d], 1), np.stack([b, cc, d], 1))
         faces[name] = np.stack([t1, t2], axis=1).reshape(-1, 3).astype(np.int64)
     return _assemble(xyz, faces, tets, A.ELEM_TETRA)
+
+
+def shuffle_cells(unv, seed=0):
+    """The same mesh with its volume cells listed in a random order (as an
+    unstructured mesher may write them): cell ids lose their locality, the
+    boundary-face elements and groups are unchanged."""
+    kinds = unv.elem_kind
+    is_cell = (kinds == A.ELEM_HEX) | (kinds == A.ELEM_TETRA) | (kinds == A.ELEM_WEDGE)
+    first = int(np.argmax(is_cell))
+    if not np.all(is_cell[first:]):
+        raise ValueError("cells must follow the boundary elements")
+    order = np.concatenate([np.arange(first), first + np.random.default_rng(seed).permutation(len(kinds) - first)])
+    counts = np.diff(unv.elem_offsets)[order]
+    offs = np.zeros(len(order) + 1, dtype=np.int64)
+    np.cumsum(counts, out=offs[1:])
+    src = np.repeat(unv.elem_offsets[order] - offs[:-1], counts) + np.arange(offs[-1])
+    return UnvData(unv.xyz, kinds[order], offs, unv.elem_nodes[src], unv.groups)
