@@ -20,6 +20,7 @@
 //     (single-block Gauss-Jordan with partial pivoting) on the coarsest level.
 // The hierarchy's structure is built once per matrix pattern and reused; every
 // solve refreshes the values from the current matrix.
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 #include <atomic>
@@ -389,6 +390,7 @@ __global__ void __launch_bounds__(BS) pre_kernel(int n, const int* __restrict__ 
                                                  const T* __restrict__ val, const T* __restrict__ b,
                                                  const T* __restrict__ dinv, T omega, T* __restrict__ x,
                                                  T* __restrict__ res, const KState* S) {
+    pdlEnter();
     if (S && S->done) return;
     const int gt = blockIdx.x * BS + threadIdx.x;
     const int row = gt / LPR, sub = gt % LPR;
@@ -402,6 +404,7 @@ __global__ void __launch_bounds__(BS) pre_kernel(int n, const int* __restrict__ 
 
 template <typename T>
 __global__ void restrict_kernel(int nc, const int* m_off, const int* m_idx, const T* res, T* bc, const KState* S) {
+    pdlEnter();
     if (S && S->done) return;
     int c = blockIdx.x * BS + threadIdx.x;
     if (c >= nc) return;
@@ -417,6 +420,7 @@ __global__ void __launch_bounds__(BS) post_kernel(int n, const int* __restrict__
                                                   const T* __restrict__ x, const T* __restrict__ xc,
                                                   const int* __restrict__ agg, T scale, const T* __restrict__ dinv,
                                                   T omega, T* __restrict__ out, const KState* S) {
+    pdlEnter();
     if (S && S->done) return;
     const int gt = blockIdx.x * BS + threadIdx.x;
     const int row = gt / LPR, sub = gt % LPR;
@@ -432,6 +436,7 @@ __global__ void __launch_bounds__(BS) post_kernel(int n, const int* __restrict__
 // damped Jacobi sweep (coarsest level without a dense inverse): out = x + omega D^-1 (b - A x)
 template <typename T>
 __global__ void smooth0_kernel(int n, T* x, const T* b, const T* dinv, T omega, const KState* S) {
+    pdlEnter();
     if (S && S->done) return;
     int i = blockIdx.x * BS + threadIdx.x;
     if (i < n) x[i] = omega * dinv[i] * b[i];
@@ -442,6 +447,7 @@ __global__ void __launch_bounds__(BS) jacobi_sweep_kernel(int n, const int* __re
                                                           const T* __restrict__ b, const T* __restrict__ x,
                                                           const T* __restrict__ dinv, T omega, T* __restrict__ out,
                                                           const KState* S) {
+    pdlEnter();
     if (S && S->done) return;
     const int gt = blockIdx.x * BS + threadIdx.x;
     const int row = gt / LPR, sub = gt % LPR;
@@ -476,6 +482,7 @@ int lanesPerRow(int n, int64_t nnz) {
 template <typename T>
 __global__ void coarse_solve_kernel(int n, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x,
                                     const KState* S) {
+    pdlEnter();
     if (S && S->done) return;
     int row = (blockIdx.x * BS + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (row >= n) return;
@@ -492,6 +499,7 @@ __global__ void __launch_bounds__(BS) jacobi_sweep_kernel(int nslices, int n, co
                                                           const T* __restrict__ b, const T* __restrict__ x,
                                                           const T* __restrict__ dinv, T omega, T* __restrict__ out,
                                                           const KState* S) {
+    pdlEnter();
     if (S && S->done) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
@@ -501,6 +509,190 @@ __global__ void __launch_bounds__(BS) jacobi_sweep_kernel(int nslices, int n, co
         for (int j = 0; j < width; ++j) sum += val[bo + 32 * j + lane] * x[col[bo + 32 * j + lane]];
         if (r < n) out[r] = x[r] + omega * dinv[r] * (b[r] - sum);
     }
+}
+
+// ---------------------------------------------------------------- fused coarse tail
+// The levels from the first one with at most tailMaxRows() rows down to the
+// coarsest run in one launch of a thread-block cluster: the pre-smoothing and
+// residual, restriction, coarsest solve and prolongation/post-smoothing phases
+// of all those levels are separated by cluster barriers instead of kernel
+// boundaries, which on levels this small cost more than the work itself. One
+// warp walks a 32-row slice at a time (one row per lane, slots in order, so the
+// sums round as in the single-lane kernels above). Vectors written inside the
+// launch are read through L2 (ld.global.cg); matrices with ordinary loads.
+constexpr int TAIL_MAX_LEVELS = 16;
+constexpr int TAIL_BS = 1024;
+
+template <typename T>
+struct TailLevel {
+    int n, nslices;
+    const int* sl_off;
+    const int* col;
+    const T* val;
+    const T* dinv;
+    const int* agg;    // row -> aggregate of the next level
+    const int* m_off;  // aggregate -> member rows (restriction to the next level)
+    const int* m_idx;
+    T *b, *x, *x2, *res;
+};
+template <typename T>
+struct TailParams {
+    int nlev;      // levels in the tail, the last being the coarsest
+    const T* b0;   // right-hand side of the first tail level (its result goes to L[0].x2)
+    const T* inv;  // dense inverse of the coarsest level, or null for Jacobi sweeps
+    T omega, scale;
+    const KState* S;
+    TailLevel<T> L[TAIL_MAX_LEVELS];
+};
+
+// Rows of a tail level, TAIL_LPR lanes per row (the lanes-per-row split of the
+// separate kernels on such levels): f(row, valid, sub) for every row, with a
+// loop bound uniform across each warp so that the row sums can shuffle.
+constexpr int TAIL_LPR = 8;
+template <typename F>
+__device__ __forceinline__ void tailRows(int n, int g, int nthreads, F f) {
+    constexpr int RPW = 32 / TAIL_LPR;  // rows per warp
+    const int lane = g & 31;
+    for (int rb = (g >> 5) * RPW; rb < n; rb += (nthreads >> 5) * RPW) {
+        const int row = rb + lane / TAIL_LPR;
+        f(row, row < n, lane % TAIL_LPR);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TAIL_BS) tail_kernel(const __grid_constant__ TailParams<T> P) {
+    pdlEnter();
+    if (P.S && P.S->done) return;  // uniform: the state does not change during this launch
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int nthreads = (int)cl.num_blocks() * TAIL_BS;
+    const int g = (int)cl.block_rank() * TAIL_BS + threadIdx.x;
+    const int lane = threadIdx.x & 31, gw = g >> 5, nw = nthreads >> 5;
+    const T omega = P.omega, scale = P.scale;
+    // down: pre-smoothing from zero with the residual, then restriction
+    for (int l = 0; l + 1 < P.nlev; ++l) {
+        const TailLevel<T>& L = P.L[l];
+        const T* b = l == 0 ? P.b0 : L.b;
+        tailRows(L.n, g, nthreads, [&](int row, bool valid, int sub) {
+            const T sum = rowSum<T, TAIL_LPR>(L.sl_off, L.col, L.val, row, valid, sub,
+                                              [&](int c) { return omega * L.dinv[c] * __ldcg(b + c); });
+            if (valid && sub == 0) {
+                const T br = __ldcg(b + row);
+                L.x[row] = omega * L.dinv[row] * br;
+                L.res[row] = br - sum;
+            }
+        });
+        cl.sync();
+        const TailLevel<T>& N = P.L[l + 1];
+        tailRows(N.n, g, nthreads, [&](int c, bool valid, int sub) {
+            T sum = 0;
+            if (valid)
+                for (int q = L.m_off[c] + sub; q < L.m_off[c + 1]; q += TAIL_LPR) sum += __ldcg(L.res + L.m_idx[q]);
+#pragma unroll
+            for (int o = TAIL_LPR / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if (valid && sub == 0) N.b[c] = sum;
+        });
+        cl.sync();
+    }
+    // coarsest level
+    {
+        const TailLevel<T>& C = P.L[P.nlev - 1];
+        const T* b = P.nlev == 1 ? P.b0 : C.b;
+        if (P.inv) {
+            for (int row = gw; row < C.n; row += nw) {
+                T sum = 0;
+                for (int c = lane; c < C.n; c += 32) sum += P.inv[(size_t)row * C.n + c] * __ldcg(b + c);
+                for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+                if (lane == 0) C.x2[row] = sum;
+            }
+        } else {
+            for (int r = g; r < C.n; r += nthreads) C.x[r] = omega * C.dinv[r] * __ldcg(b + r);
+            T* cur = C.x;
+            T* nxt = C.res;
+            for (int k = 0; k < 8; ++k) {
+                cl.sync();
+                T* dst = k == 7 ? C.x2 : nxt;
+                tailRows(C.n, g, nthreads, [&](int row, bool valid, int sub) {
+                    const T sum = rowSum<T, TAIL_LPR>(C.sl_off, C.col, C.val, row, valid, sub,
+                                                      [&](int c) { return __ldcg(cur + c); });
+                    if (valid && sub == 0) dst[row] = __ldcg(cur + row) + omega * C.dinv[row] * (__ldcg(b + row) - sum);
+                });
+                nxt = cur;
+                cur = dst;
+            }
+        }
+        cl.sync();
+    }
+    // up: prolongation and post-smoothing
+    for (int l = P.nlev - 2; l >= 0; --l) {
+        const TailLevel<T>& L = P.L[l];
+        const T* xc = P.L[l + 1].x2;
+        const T* b = l == 0 ? P.b0 : L.b;
+        tailRows(L.n, g, nthreads, [&](int row, bool valid, int sub) {
+            const T sum = rowSum<T, TAIL_LPR>(L.sl_off, L.col, L.val, row, valid, sub,
+                                              [&](int c) { return __ldcg(L.x + c) + scale * __ldcg(xc + L.agg[c]); });
+            if (valid && sub == 0) {
+                const T xp = __ldcg(L.x + row) + scale * __ldcg(xc + L.agg[row]);
+                L.x2[row] = xp + omega * L.dinv[row] * (__ldcg(b + row) - sum);
+            }
+        });
+        if (l > 0) cl.sync();
+    }
+}
+
+// rows of the largest level run in the fused tail (PRISM_AMG_TAIL_ROWS; 0 disables it)
+int tailMaxRows() {
+    static const int v = [] {
+        const char* e = std::getenv("PRISM_AMG_TAIL_ROWS");
+        return e && e[0] ? std::max(0, std::atoi(e)) : 4096;
+    }();
+    return v;
+}
+
+// CTAs per tail cluster: 16 (a non-portable size) where the device can place
+// such a cluster, else the portable 8
+template <typename T>
+int tailCluster() {
+    static const int c = [] {
+        int cl = 8;
+        if (cudaFuncSetAttribute(tail_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(16);
+            cfg.blockDim = dim3(TAIL_BS);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = 16;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int n = 0;
+            if (cudaOccupancyMaxActiveClusters(&n, tail_kernel<T>, &cfg) == cudaSuccess && n >= 1) cl = 16;
+        }
+        cudaGetLastError();  // a refused query leaves no sticky error
+        return cl;
+    }();
+    return c;
+}
+
+template <typename T>
+void launchTail(const TailParams<T>& P, cudaStream_t s) {
+    const int cl = tailCluster<T>();
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)cl);
+    cfg.blockDim = dim3(TAIL_BS);
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = pdlEnabled() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    PB_CUDA(cudaLaunchKernelEx(&cfg, tail_kernel<T>, P));
+    countLaunch();
 }
 
 // ---------------------------------------------------------------- structure builders
@@ -723,11 +915,18 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
         }
         coarse_n = levels.back()->n;
         for (auto& L : levels) L->lpr = lanesPerRow(L->n, L->nnz);
+        tail = -1;
+        for (size_t l = 1; l + 1 < levels.size(); ++l)
+            if (levels[l]->n <= tailMaxRows() && levels.size() - l <= (size_t)TAIL_MAX_LEVELS) {
+                tail = (int)l;
+                break;
+            }
         if (verbose()) {
             std::fprintf(stderr, "[prism amg] hierarchy:");
             for (auto& L : levels) std::fprintf(stderr, " %d/%lld/%d", L->n, (long long)L->nnz, L->lpr);
-            std::fprintf(stderr, " (rows/entries/lanes per row), coarsest %s; matching %.1f ms, galerkin %.1f ms, members %.1f ms\n",
-                         coarse_n <= DENSE_MAX ? "dense" : "Jacobi", t_match, t_gal, t_mem);
+            std::fprintf(stderr, " (rows/entries/lanes per row), coarsest %s, fused tail from level %d; matching %.1f ms, "
+                         "galerkin %.1f ms, members %.1f ms\n",
+                         coarse_n <= DENSE_MAX ? "dense" : "Jacobi", tail, t_match, t_gal, t_mem);
         }
         trimScratch(s);
         if (coarse_n <= DENSE_MAX) {
@@ -802,6 +1001,38 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
         if constexpr (sizeof(T) == 8) return bufs64(X);
         else return bufs32(X);
     };
+    if (A.tail > 0 && (int)l == A.tail) {
+        TailParams<T> P{};
+        P.nlev = (int)(A.levels.size() - l);
+        P.b0 = b;
+        if (A.coarse_inv.p) {
+            if constexpr (sizeof(T) == 8) P.inv = A.coarse_inv.p;
+            else P.inv = A.coarse_inv32.p;
+        }
+        P.omega = (T)A.omega;
+        P.scale = (T)A.scale;
+        P.S = S;
+        for (int k = 0; k < P.nlev; ++k) {
+            AmgLevel& X = *A.levels[l + k];
+            Bufs<T> xb = B(X);
+            TailLevel<T>& t = P.L[k];
+            t.n = X.n;
+            t.nslices = X.nslices;
+            t.sl_off = X.sl_off;
+            t.col = X.sl_col;
+            t.val = CycleData<T>::vals(X);
+            t.dinv = xb.dinv;
+            t.agg = X.agg.p;
+            t.m_off = X.m_off.p;
+            t.m_idx = X.m_idx.p;
+            t.b = xb.b;
+            t.x = xb.x;
+            t.x2 = k == 0 ? out : xb.x2;
+            t.res = xb.res;
+        }
+        launchTail<T>(P, s);
+        return;
+    }
     Bufs<T> lb = B(L);
     const T omega = (T)A.omega;
     const T* vals = CycleData<T>::vals(L);
@@ -810,20 +1041,19 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
             const T* inv;
             if constexpr (sizeof(T) == 8) inv = A.coarse_inv.p;
             else inv = A.coarse_inv32.p;
-            coarse_solve_kernel<T><<<grid((int64_t)L.n * 32), BS, 0, s>>>(L.n, inv, b, out, S); countLaunch();
+            launchPdl(coarse_solve_kernel<T>, grid((int64_t)L.n * 32), BS, s, L.n, inv, b, out, S);
         } else {
             // ping-pong between x and res (out is this level's x2 or a caller vector)
-            smooth0_kernel<T><<<grid(L.n), BS, 0, s>>>(L.n, lb.x, b, lb.dinv, omega, S); countLaunch();
+            launchPdl(smooth0_kernel<T>, grid(L.n), BS, s, L.n, lb.x, b, lb.dinv, omega, S);
             T* cur = lb.x;
             T* nxt = lb.res;
             for (int k = 0; k < 8; ++k) {
                 T* dst = (k == 7) ? out : nxt;
                 withLpr(L.lpr, [&](auto c) {
                     constexpr int P = decltype(c)::value;
-                    jacobi_sweep_kernel<T, P><<<grid((int64_t)L.n * P), BS, 0, s>>>(L.n, L.sl_off, L.sl_col, vals, b,
-                                                                                   cur, lb.dinv, omega, dst, S);
+                    launchPdl(jacobi_sweep_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals,
+                              b, cur, lb.dinv, omega, dst, S);
                 });
-                countLaunch();
                 nxt = cur;
                 cur = dst;
             }
@@ -837,22 +1067,21 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
     int slot = fine ? profBegin(PROF_AMG_PRE, sizeof(T) == 4, mat_bytes + 4.0 * sizeof(T) * L.n, s) : -1;
     withLpr(L.lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
-        pre_kernel<T, P><<<grid((int64_t)L.n * P), BS, 0, s>>>(L.n, L.sl_off, L.sl_col, vals, b, lb.dinv, omega, lb.x,
-                                                               lb.res, S);
+        launchPdl(pre_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, lb.dinv, omega,
+                  lb.x, lb.res, S);
     });
-    countLaunch();
     profEnd(slot, s);
-    restrict_kernel<T><<<grid(N.n), BS, 0, s>>>(N.n, L.m_off.p, L.m_idx.p, lb.res, nb.b, S); countLaunch();
+    launchPdl(restrict_kernel<T>, grid(N.n), BS, s, N.n, (const int*)L.m_off.p, (const int*)L.m_idx.p,
+              (const T*)lb.res, nb.b, S);
     vcycle<T>(A, l + 1, nb.b, nb.x2, S, s, false);
     slot = fine ? profBegin(PROF_AMG_POST, sizeof(T) == 4,
                             mat_bytes + (4.0 * sizeof(T) + 4.0) * L.n + (double)sizeof(T) * N.n, s)
                 : -1;
     withLpr(L.lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
-        post_kernel<T, P><<<grid((int64_t)L.n * P), BS, 0, s>>>(L.n, L.sl_off, L.sl_col, vals, b, lb.x, nb.x2,
-                                                                L.agg.p, (T)A.scale, lb.dinv, omega, out, S);
+        launchPdl(post_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, lb.x, nb.x2,
+                  L.agg.p, (T)A.scale, lb.dinv, omega, out, S);
     });
-    countLaunch();
     profEnd(slot, s);
 }
 

@@ -49,6 +49,7 @@ struct Amg {
     bool built = false;
     bool has32 = false;
     uint64_t generation = 0;  // new process-wide value whenever a buffer of the hierarchy is (re)allocated
+    int tail = -1;            // first level of the fused coarse tail (-1: every level launches its own kernels)
     double omega = 0.67, scale = 1.5;
 
     // Build the hierarchy (first call) or refresh its values (later calls) for

@@ -138,6 +138,41 @@ inline bool verbose() {
     return v;
 }
 
+// Programmatic dependent launch (sm_90 and later). Kernels of the solver
+// iteration are launched with launchPdl(): the next kernel in the stream may be
+// scheduled while this one drains, and waits in pdlEnter() until this one has
+// completed and its writes are visible. PRISM_NO_PDL=1 launches them plainly.
+inline bool pdlEnabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("PRISM_NO_PDL");
+        return !(e && e[0] && e[0] != '0');
+    }();
+    return on;
+}
+template <typename... KArgs, typename... Args>
+void launchPdl(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = pdlEnabled() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    PB_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+    countLaunch();
+}
+#ifdef __CUDACC__
+// First statement of a kernel launched by launchPdl(): release the next kernel's
+// launch, then wait for the previous kernel (no-ops without the attribute).
+__device__ __forceinline__ void pdlEnter() {
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+#endif
+
 constexpr double EPSILON = 2.220446049250313080847263336181640625e-16; // std::numeric_limits<double>::epsilon()
 constexpr int SLICE = 32;  // SELL slice height: one warp of rows
 constexpr int NUM_SMS = 148;

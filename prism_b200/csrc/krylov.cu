@@ -139,21 +139,36 @@ int waveGrid(K kernel, int needed) {
 // coalesced loads; the matrix is read with evict-first (streaming) loads so
 // that L2 keeps the gathered x.
 // STAGE 0: plain; 1: alpha = rho / (u.y); 2: w = (u.y)/(y.y)
+// The columns and values of up to 8 slots are loaded before their gathers, so
+// a row's loads are all in flight at once; the sum runs over the slots in order.
 template <typename T>
 __device__ __forceinline__ T sliceRow(const int* __restrict__ col, const T* __restrict__ val,
                                       const T* __restrict__ x, int b, int width, int lane) {
+    constexpr int W = 8;
     T sum = 0;
-#pragma unroll 4
-    for (int j = 0; j < width; ++j) sum += __ldcs(val + b + 32 * j + lane) * x[__ldcs(col + b + 32 * j + lane)];
+    for (int j0 = 0; j0 < width; j0 += W) {
+        int c[W];
+        T v[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            if (j0 + k < width) {
+                c[k] = __ldcs(col + b + 32 * (j0 + k) + lane);
+                v[k] = __ldcs(val + b + 32 * (j0 + k) + lane);
+            }
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            if (j0 + k < width) sum += v[k] * __ldg(x + c[k]);
+    }
     return sum;
 }
 
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(BS) spmv_kernel(int nslices, int n, const int* __restrict__ sl_off,
+__global__ void __launch_bounds__(BS, 5) spmv_kernel(int nslices, int n, const int* __restrict__ sl_off,
                                                   const int* __restrict__ col, const T* __restrict__ val,
                                                   const T* __restrict__ x, T* __restrict__ y,
                                                   const T* __restrict__ u, double* partials,
                                                   unsigned int* counter, KState* S) {
+    pdlEnter();
     if (STAGE != 0 && S->done) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double d0 = 0.0, d1 = 0.0;
@@ -184,6 +199,7 @@ __global__ void __launch_bounds__(BS) spmv_kernel(int nslices, int n, const int*
 template <typename T>
 __global__ void __launch_bounds__(BS) p_kernel(int n, T* __restrict__ p, const T* __restrict__ r,
                                                const T* __restrict__ v, const KState* S) {
+    pdlEnter();
     if (S->done) return;
     const double beta = S->beta, w = S->w;
     for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS)
@@ -193,6 +209,7 @@ __global__ void __launch_bounds__(BS) p_kernel(int n, T* __restrict__ p, const T
 template <typename T>
 __global__ void __launch_bounds__(BS) s_kernel(int n, T* __restrict__ s, const T* __restrict__ r,
                                                const T* __restrict__ v, const KState* S) {
+    pdlEnter();
     if (S->done) return;
     const double alpha = S->alpha;
     for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS)
@@ -205,6 +222,7 @@ __global__ void __launch_bounds__(BS) xr_kernel(int n, T* __restrict__ x, T* __r
                                                 const T* __restrict__ q, const T* __restrict__ s,
                                                 const T* __restrict__ t, const T* __restrict__ r0, double* partials,
                                                 unsigned int* counter, KState* S) {
+    pdlEnter();
     if (S->done) return;
     const double alpha = S->alpha, w = S->w;
     double d0 = 0.0, d1 = 0.0;
@@ -450,7 +468,7 @@ void KrylovWork::ensure(int n_pad, int64_t nnz_padded, bool mixed) {
         nnz = nnz_padded;
         for (auto* b : {&r, &r0, &p, &v, &s, &t, &xs, &dinv, &tmp}) b->alloc(n_pad);
         As.alloc(nnz_padded);
-        partials.alloc((size_t)std::max(sliceGrid(n_pad / 32), std::max(NUM_SMS, smCount()) * 16) * 4);
+        partials.alloc((size_t)std::max(ceil_div(n_pad / 32, WARPS), std::max(NUM_SMS, smCount()) * 16) * 4);
         counter.alloc(1);
         PB_CUDA(cudaMemset(counter.p, 0, sizeof(unsigned int)));
         scal.alloc(8);
@@ -583,25 +601,25 @@ void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T*
     const int sg1 = waveGrid(spmv_kernel<T, 1>, ceil_div(A.nslices, WARPS));
     const int sg2 = waveGrid(spmv_kernel<T, 2>, ceil_div(A.nslices, WARPS));
     for (long long it = 0; it < count; ++it) {
-        p_kernel<T><<<vg, BS, 0, s>>>(n, V.p, V.r, V.v, S); countLaunch();
+        launchPdl(p_kernel<T>, vg, BS, s, n, V.p, V.r, V.v, S);
         const T* dp = V.p;
         if (amg) {
             precApply(amg, V.p, y, S, s, sample);
             dp = y;
         }
         const int slot = sample ? profBegin(PROF_SPMV, sizeof(T) == 4, spmvBytes<T>(A), s) : -1;
-        spmv_kernel<T, 1><<<sg1, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, dp, V.v, V.r0, w.partials.p,
-                                            w.counter.p, S); countLaunch();
+        launchPdl(spmv_kernel<T, 1>, sg1, BS, s, A.nslices, n, A.sl_off, A.col, M, dp, V.v, V.r0, w.partials.p,
+                  w.counter.p, S);
         profEnd(slot, s);
-        s_kernel<T><<<vg, BS, 0, s>>>(n, V.s, V.r, V.v, S); countLaunch();
+        launchPdl(s_kernel<T>, vg, BS, s, n, V.s, V.r, V.v, S);
         const T* ds = V.s;
         if (amg) {
             precApply(amg, V.s, z, S, s, sample);
             ds = z;
         }
-        spmv_kernel<T, 2><<<sg2, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, ds, V.t, V.s, w.partials.p,
-                                            w.counter.p, S); countLaunch();
-        xr_kernel<T><<<vg, BS, 0, s>>>(n, V.x, V.r, dp, ds, V.s, V.t, V.r0, w.partials.p, w.counter.p, S); countLaunch();
+        launchPdl(spmv_kernel<T, 2>, sg2, BS, s, A.nslices, n, A.sl_off, A.col, M, ds, V.t, V.s, w.partials.p,
+                  w.counter.p, S);
+        launchPdl(xr_kernel<T>, vg, BS, s, n, V.x, V.r, dp, ds, V.s, V.t, V.r0, w.partials.p, w.counter.p, S);
     }
 }
 

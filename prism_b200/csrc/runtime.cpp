@@ -604,6 +604,24 @@ PrismSolveOpts inner(const PrismSolveOpts& so, int64_t n_iter, double eps, int64
     return o;
 }
 
+// PRISM_VERBOSE: wall time of a scope, the stream drained at both ends
+struct PhaseTimer {
+    std::string what;
+    cudaStream_t s;
+    std::chrono::steady_clock::time_point t0;
+    PhaseTimer(std::string w, cudaStream_t st) : what(std::move(w)), s(st) {
+        if (!verbose()) return;
+        cudaStreamSynchronize(s);
+        t0 = std::chrono::steady_clock::now();
+    }
+    ~PhaseTimer() {
+        if (!verbose()) return;
+        cudaStreamSynchronize(s);
+        std::fprintf(stderr, "[prism] phase %s: %.3f ms\n", what.c_str(),
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+};
+
 void setURF(Transport& eq, double f) {  // transport.cpp:38-52: out-of-range values are ignored
     if (f < 0.0 || f > 1.0) return;
     eq.urf = f;
@@ -614,6 +632,7 @@ void solveImplicitMomentum(const PrismSIMPLEControls& c, std::vector<Transport*>
                            std::vector<Report>& rep) {
     for (auto* eq : mom) {
         setURF(*eq, c.momentum_urf);
+        PhaseTimer pt("momentum " + eq->phi->name, eq->phi->m->stream);
         auto r = solve(*eq, inner(so, c.momentum_max_iter, c.momentum_residual, -1, 0.0, false));
         rep.push_back({eq->phi->name, r.iterations, r.initial_residual, r.final_residual, r.converged != 0});
     }
@@ -709,6 +728,7 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
     if (!m.p_amg) m.p_amg = std::make_shared<Amg>();
     pEqn.amg = m.p_amg;
     for (int64_t i = 0; i <= c.non_ortho_correctors; ++i) {
+        PhaseTimer pt("pressure corrector " + std::to_string(i), m.stream);
         auto r = solve(pEqn, inner(so, c.pressure_max_iter, c.pressure_residual, c.p_ref_cell, c.p_ref_value, true));
         rep.push_back({pp->name + "_corr_" + std::to_string(i), r.iterations, r.initial_residual, r.final_residual,
                        r.converged != 0});
@@ -754,8 +774,10 @@ bool needsPressureReference(const Scalar& p) {  // SIMPLE.cpp:110-122
 void simpleStep(const PrismSIMPLEControls& c, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
                 const PrismSolveOpts& so, std::vector<Report>& rep) {
     if (mom.size() != 2 && mom.size() != 3) fail(PRISM_BAD_ARG, "SIMPLE expects 2 or 3 momentum predictors");
+    PhaseTimer pt("SIMPLE step", p.m->stream);
     solveImplicitMomentum(c, mom, so, rep);
     auto r = solvePressureEquation(c, mom, U, mdot, p, so, rep);
+    PhaseTimer pc("correct fields", p.m->stream);
     correctFields(U, mdot, p, *r.D, *r.pp, c.pressure_urf);
 }
 
