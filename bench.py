@@ -201,7 +201,8 @@ def transport_exact(mesh):
 def transport_time_to_tol(mesh, precision, ref, tol=1e-8, preconditioner="auto"):
     """Seconds (CUDA events) for one solve() step from T = 0 (assembly included) to reach
     ||T - x*|| / ||x*|| <= tol: the loosest Krylov tolerance of a 10^-0.5 ladder that meets
-    the error is timed (second of two identical runs)."""
+    the error is timed (the fastest of three identical runs, so that a one-off host stall in
+    one run does not decide the figure)."""
     import numpy as np
     import torch
     from prism_b200 import api
@@ -211,7 +212,8 @@ def transport_time_to_tol(mesh, precision, ref, tol=1e-8, preconditioner="auto")
         ktol = 10.0 ** (-e)
         solver = api.BiCGSTAB(precision=precision, krylov_tol=ktol, krylov_max_iter=100000,
                               preconditioner=preconditioner)
-        for rep in range(2):
+        best = None
+        for rep in range(3):
             T, keep, eqn = transport_eqn(mesh)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -220,6 +222,8 @@ def transport_time_to_tol(mesh, precision, ref, tol=1e-8, preconditioner="auto")
             e1.record()
             torch.cuda.synchronize()
             secs = e0.elapsed_time(e1) / 1000.0
+            best = secs if best is None else min(best, secs)
+        secs = best
         err = float(np.linalg.norm(T.values() - ref) / nref)
         last = {"seconds": secs, "krylov_tol": ktol, "krylov_iterations": r.krylov_iterations, "error": err}
         if err <= tol:
