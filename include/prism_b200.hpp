@@ -93,6 +93,8 @@ class PMesh {
     auto boundaryFaceCount() const -> size_t { return (size_t)_info.n_boundary_faces; }
     auto patchCount() const -> size_t { return (size_t)_info.n_patches; }
     auto vertexCount() const -> size_t { return (size_t)_info.n_vertices; }
+    // mesh::CuthillMckee(mesh).reorder(reverse) (reorder.cpp:8-130); before any field exists
+    void reorder(bool reverse = false) { check(prism_mesh_reorder(_h.get(), reverse ? 1 : 0)); }
     auto handle() const -> PrismMesh* { return _h.get(); }
     // output::cellToPoint (export.cpp:73-111): interleaved cell data -> interleaved vertex data
     auto cellToPoint(const std::vector<double>& cell_data, size_t n_components) const -> std::vector<double> {
