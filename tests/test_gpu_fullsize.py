@@ -9,8 +9,8 @@ itself and against the physics:
     face flux is zero and the continuity residual has fallen;
   * the 128^3 jittered-hex transport (2,097,152 cells): FP64 and mixed
     precision agree and the field stays finite and near the boundary values
-    (LinearUpwind's weights are not bounded, so a few percent of over- and
-    undershoot is the scheme's, not a solver error)."""
+    (LinearUpwind's weights are not bounded: the ~11% overshoot near the hot
+    wall is the scheme's, not a solver error)."""
 import numpy as np
 import pytest
 
