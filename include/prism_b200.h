@@ -320,6 +320,12 @@ typedef struct {
     int64_t krylov_max_iter; /* 0: default 2*n_cells */
     double inner_tol;        /* mixed precision: residual reduction between FP64 reliable updates (0: default 0.1) */
     int32_t preconditioner;  /* PRISM_PC_* (BiCGSTAB only) */
+    int32_t graph;           /* 1: prism_solve, and the SIMPLE/PRIME/PISO steps given these options, run as
+                                one CUDA graph launch whose solver loops (Krylov batches, restarts,
+                                accurate-residual passes, outer steps) are device-side conditional
+                                nodes, with no host round trip until the end. FP64 BiCGSTAB only; the
+                                first call on new equations runs as usual (it builds the AMG
+                                hierarchies and work buffers the graph then uses). 0: default. */
 } PrismSolveOpts;
 
 typedef struct {
@@ -421,6 +427,7 @@ typedef struct {
     int64_t amg_post_launches;
     double amg_post_ms;
     double amg_post_bytes;
+    int64_t graph_launches; /* solves and steps run as one CUDA graph launch (PrismSolveOpts.graph) */
 } PrismProfile;
 int prism_profile_start(int32_t max_samples);
 int prism_profile_stop(PrismProfile* out);

@@ -76,7 +76,7 @@ class SolveOpts(C.Structure):
     _fields_ = [("method", i32), ("precision", i32), ("n_iter", i64), ("eps", f64),
                 ("ref_cell", i64), ("ref_value", f64), ("clear_coeffs", i32),
                 ("krylov_tol", f64), ("krylov_max_iter", i64), ("inner_tol", f64),
-                ("preconditioner", i32)]
+                ("preconditioner", i32), ("graph", i32)]
 
 
 class SolveResult(C.Structure):
@@ -116,7 +116,8 @@ class Profile(C.Structure):
                 ("fp32_launches", i64), ("fp32_ms", f64), ("fp32_bytes", f64),
                 ("kernel_launches", i64),
                 ("amg_pre_launches", i64), ("amg_pre_ms", f64), ("amg_pre_bytes", f64),
-                ("amg_post_launches", i64), ("amg_post_ms", f64), ("amg_post_bytes", f64)]
+                ("amg_post_launches", i64), ("amg_post_ms", f64), ("amg_post_bytes", f64),
+                ("graph_launches", i64)]
 
 
 PP = C.POINTER(P)

@@ -561,7 +561,7 @@ class SolverResult:
 
 
 def _solve_opts(lib, method, precision, n_iter, eps, ref_cell, ref_value, clear, krylov_tol,
-                krylov_max_iter, inner_tol, preconditioner=A.PC_AUTO):
+                krylov_max_iter, inner_tol, preconditioner=A.PC_AUTO, graph=False):
     o = A.SolveOpts()
     lib.solve_opts_default(C.byref(o))
     o.method, o.precision, o.n_iter, o.eps = method, precision, n_iter, eps
@@ -574,6 +574,7 @@ def _solve_opts(lib, method, precision, n_iter, eps, ref_cell, ref_value, clear,
     if inner_tol:
         o.inner_tol = inner_tol
     o.preconditioner = preconditioner
+    o.graph = 1 if graph else 0
     return o
 
 
@@ -581,7 +582,11 @@ class _Solver:
     method = A.SOLVER_BICGSTAB
 
     def __init__(self, precision=A.PREC_FP64, krylov_tol=0.0, krylov_max_iter=0, inner_tol=0.0,
-                 preconditioner="auto"):
+                 preconditioner="auto", graph=False):
+        """graph=True: solves, and the SIMPLE/PRIME/PISO steps driven by this solver, run as one
+        CUDA graph launch with device-side solver loops (FP64 BiCGSTAB; the first call on new
+        equations runs as usual and builds what the graph uses)."""
+        self.graph = graph
         self.precision, self.krylov_tol = precision, krylov_tol
         self.krylov_max_iter, self.inner_tol = krylov_max_iter, inner_tol
         if isinstance(preconditioner, str):
@@ -591,7 +596,7 @@ class _Solver:
     def opts(self, lib, n_iter=10, eps=1e-7, ref_cell=None, ref_value=0.0, clear_coeffs=True):
         return _solve_opts(lib, self.method, self.precision, n_iter, eps, ref_cell, ref_value,
                            clear_coeffs, self.krylov_tol, self.krylov_max_iter, self.inner_tol,
-                           self.preconditioner)
+                           self.preconditioner, self.graph)
 
     def solve(self, eqn: Transport, n_iter=10, eps=1e-7, ref_cell=None, ref_value=0.0,
               clear_coeffs=True) -> SolverResult:

@@ -965,7 +965,7 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
         gauss_jordan_kernel<<<1, 1024, (size_t)n * n * sizeof(double), s>>>(n, coarse_a.p, coarse_inv.p,
                                                                             mixed ? coarse_inv32.p : nullptr,
                                                                             coarse_bad.p); countLaunch();
-        if (verbose()) {
+        if (verbose() && !capturing(s)) {
             int ns = 0;
             PB_CUDA(cudaMemcpyAsync(&ns, coarse_bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
             PB_CUDA(cudaStreamSynchronize(s));

@@ -320,5 +320,16 @@ void launchPin(double* A, double* b, int pos, int row, double ref_value, cudaStr
     pin_kernel<<<1, 1, 0, s>>>(A, b, pos, row, ref_value); countLaunch();
     PB_LAUNCH("pin_kernel");
 }
+// the same, with the diagonal's position read on the device (for graph capture)
+__global__ void pin_dev_kernel(double* A, double* b, const int* diag_pos, int row, double ref_value) {
+    const int pos = diag_pos[row];
+    double diag = A[pos];
+    A[pos] += diag;
+    b[row] += diag * ref_value;
+}
+void launchPinDev(double* A, double* b, const int* diag_pos, int row, double ref_value, cudaStream_t s) {
+    pin_dev_kernel<<<1, 1, 0, s>>>(A, b, diag_pos, row, ref_value); countLaunch();
+    PB_LAUNCH("pin_dev_kernel");
+}
 
 }  // namespace pb

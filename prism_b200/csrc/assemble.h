@@ -55,5 +55,6 @@ struct AssembleParams {
 void launchAssemble(const AssembleParams& P, cudaStream_t s);
 void launchRelax(double* A, double* b, const int* diag_pos, const double* phi, double alpha, int n, cudaStream_t s);
 void launchPin(double* A, double* b, int pos, int row, double ref_value, cudaStream_t s);
+void launchPinDev(double* A, double* b, const int* diag_pos, int row, double ref_value, cudaStream_t s);
 
 }  // namespace pb

@@ -727,7 +727,8 @@ API void prism_solve_opts_default(PrismSolveOpts* o) {
 API int prism_solve(PrismTransport* pt, const PrismSolveOpts* o, PrismSolveResult* r) {
     return guard([&] {
         ARG(pt && o && r, "null argument");
-        *r = solve(pt->eq, *o);
+        if (o->graph && graphReady(pt->eq, *o)) *r = solveAsGraph(pt->eq, *o);
+        else *r = solve(pt->eq, *o);
         sync(*pt->eq.phi->m);
     });
 }
@@ -838,7 +839,11 @@ API int prism_simple_step(const PrismSIMPLEControls* c, PrismTransport* const* m
         ARG(c && U && mdot && p, "null argument");
         auto v = momVec(mom, n_mom);
         std::vector<Report> r;
-        simpleStep(*c, v, *U->v, *mdot->v, *p->s, optsOrDefault(so), r);
+        const PrismSolveOpts opts = optsOrDefault(so);
+        if (opts.graph && stepGraphReady(v, *U->v, *p->s, opts, true))
+            stepAsGraph(*p->s->m, [&] { simpleStep(*c, v, *U->v, *mdot->v, *p->s, opts, r); }, r);
+        else
+            simpleStep(*c, v, *U->v, *mdot->v, *p->s, opts, r);
         sync(*p->s->m);
         writeReports(r, rep, max, n);
     });
@@ -850,7 +855,11 @@ API int prism_prime_step(const PrismSIMPLEControls* c, PrismTransport* const* mo
         ARG(c && U && mdot && p, "null argument");
         auto v = momVec(mom, n_mom);
         std::vector<Report> r;
-        primeStep(*c, v, *U->v, *mdot->v, *p->s, optsOrDefault(so), r);
+        const PrismSolveOpts opts = optsOrDefault(so);
+        if (opts.graph && stepGraphReady(v, *U->v, *p->s, opts, false))
+            stepAsGraph(*p->s->m, [&] { primeStep(*c, v, *U->v, *mdot->v, *p->s, opts, r); }, r);
+        else
+            primeStep(*c, v, *U->v, *mdot->v, *p->s, opts, r);
         sync(*p->s->m);
         writeReports(r, rep, max, n);
     });
@@ -862,7 +871,11 @@ API int prism_piso_step(const PrismPISOControls* c, PrismTransport* const* mom, 
         ARG(c && U && mdot && p, "null argument");
         auto v = momVec(mom, n_mom);
         std::vector<Report> r;
-        pisoStep(*c, v, *U->v, *mdot->v, *p->s, optsOrDefault(so), r);
+        const PrismSolveOpts opts = optsOrDefault(so);
+        if (opts.graph && stepGraphReady(v, *U->v, *p->s, opts, true))
+            stepAsGraph(*p->s->m, [&] { pisoStep(*c, v, *U->v, *mdot->v, *p->s, opts, r); }, r);
+        else
+            pisoStep(*c, v, *U->v, *mdot->v, *p->s, opts, r);
         sync(*p->s->m);
         writeReports(r, rep, max, n);
     });

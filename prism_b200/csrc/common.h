@@ -125,6 +125,11 @@ inline std::atomic<long long>& launchCounter() {
     return c;
 }
 inline void countLaunch() { launchCounter().fetch_add(1, std::memory_order_relaxed); }
+// Number of solves and steps this library has run as one CUDA graph launch.
+inline std::atomic<long long>& graphLaunchCounter() {
+    static std::atomic<long long> c{0};
+    return c;
+}
 
 inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 

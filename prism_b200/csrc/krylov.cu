@@ -535,6 +535,7 @@ struct Sample {
 struct Profiler {
     bool on = false;
     long long launches0 = 0;
+    long long graphs0 = 0;
     int max_samples = 0;
     std::vector<Sample> samples;
     std::vector<cudaEvent_t> pool;
@@ -890,6 +891,7 @@ void profileStart(int max_samples) {
     g_prof.samples.clear();
     g_prof.max_samples = max_samples > 0 ? max_samples : 4096;
     g_prof.launches0 = launchCounter().load();
+    g_prof.graphs0 = graphLaunchCounter().load();
     g_prof.on = true;
 }
 
@@ -897,6 +899,7 @@ void profileStop(PrismProfile* out) {
     std::memset(out, 0, sizeof(*out));
     g_prof.on = false;
     out->kernel_launches = launchCounter().load() - g_prof.launches0;
+    out->graph_launches = graphLaunchCounter().load() - g_prof.graphs0;
     for (auto& smp : g_prof.samples) {
         if (!smp.closed) continue;
         PB_CUDA(cudaEventSynchronize(smp.b));
@@ -948,6 +951,254 @@ double scaledResidual(const SellMatrix& A, const double* b, const double* x, Kry
     PB_CUDA(cudaStreamSynchronize(s));
     if (h[2] != 0.0) return NAN;
     return h[0] / (h[1] + EPSILON);
+}
+
+// ---------------------------------------------------------------- solves inside a CUDA graph
+namespace {
+
+enum { PH_INIT = 0, PH_ITER = 1, PH_CHECK = 2, PH_DONE = 3 };
+constexpr int GRAPH_UNROLL = 4;  // BiCGSTAB iterations per pass of the device loop
+
+__device__ __forceinline__ double nanValue() { return __longlong_as_double(0x7ff8000000000000LL); }
+
+__global__ void ctl_solve_begin_kernel(SolveCtl* c, long long n_iter, double eps, long long kmax, double tol,
+                                       cudaGraphConditionalHandle ho) {
+    if (threadIdx.x) return;
+    cudaGraphSetConditional(ho, 1u);
+    SolveCtl z{};
+    z.n_iter = n_iter;
+    z.eps = eps;
+    z.kmax = kmax;
+    z.tol = tol;
+    z.status = PRISM_OK;
+    z.kstatus = PRISM_OK;
+    z.phase = PH_DONE;
+    *c = z;
+}
+
+__global__ void ctl_init_res_kernel(SolveCtl* c, const double* scal) {
+    if (threadIdx.x) return;
+    c->init_res = scal[2] != 0.0 ? nanValue() : scal[0] / (scal[1] + EPSILON);
+}
+
+// a fresh KState for one pass (runBicgstab's initial state: zeros, the iteration cap)
+__device__ void resetState(KState* S, long long maxit) {
+    KState z{};
+    z.maxit = maxit;
+    *S = z;
+}
+
+// start of one bicgstab() call: its first pass, and the device loop switched on
+__global__ void ctl_krylov_begin_kernel(SolveCtl* c, KState* S, cudaGraphConditionalHandle hk) {
+    if (threadIdx.x) return;
+    c->maxit_left = c->kmax;
+    c->pass = 0;
+    c->restarts = 0;
+    c->kstatus = PRISM_OK;
+    c->krylov_rel = 0.0;
+    c->guard = 0;
+    c->phase = PH_INIT;
+    resetState(S, c->kmax);
+    cudaGraphSetConditional(hk, 1u);
+}
+
+// first node of a loop pass: which phase body runs
+__global__ void ctl_phase_kernel(const SolveCtl* c, cudaGraphConditionalHandle hi, cudaGraphConditionalHandle ht,
+                                 cudaGraphConditionalHandle hc) {
+    if (threadIdx.x) return;
+    cudaGraphSetConditional(hi, c->phase == PH_INIT ? 1u : 0u);
+    cudaGraphSetConditional(ht, c->phase == PH_ITER ? 1u : 0u);
+    cudaGraphSetConditional(hc, c->phase == PH_CHECK ? 1u : 0u);
+}
+
+// One transition of bicgstab()'s control flow (runBicgstab's batches, restarts
+// and accurate-residual passes), after the body of the current phase has run.
+__global__ void ctl_krylov_step_kernel(SolveCtl* c, KState* S, const double* scal, long long guard_max,
+                                       cudaGraphConditionalHandle hk) {
+    if (threadIdx.x) return;
+    if (c->phase == PH_INIT) {
+        c->phase = PH_ITER;
+    } else if (c->phase == PH_ITER) {
+        const int d = S->done;
+        if (d == 3) {  // restart from the current x
+            if (++c->restarts > 20) {
+                c->kstatus = PRISM_BREAKDOWN;
+                c->phase = PH_CHECK;
+            } else {
+                c->phase = PH_INIT;
+            }
+        } else if (d != 0) {
+            c->kstatus = d == 2 ? PRISM_NOT_CONVERGED : d == 5 ? PRISM_NONFINITE : PRISM_OK;
+            c->phase = PH_CHECK;
+        }
+    } else if (c->phase == PH_CHECK) {
+        const double rb0 = scal[0], rb1 = scal[1];
+        c->krylov_rel = rb1 > 0 ? sqrt(rb0 / rb1) : 0.0;
+        c->krylov_iterations += S->iter;
+        c->maxit_left -= S->iter;
+        c->pass += 1;
+        if (c->kstatus != PRISM_OK || c->krylov_rel <= 10 * c->tol || c->maxit_left <= 0 || rb1 == 0 || c->pass >= 4) {
+            c->phase = PH_DONE;
+        } else {
+            resetState(S, c->maxit_left);
+            c->restarts = 0;
+            c->kstatus = PRISM_OK;
+            c->phase = PH_INIT;
+        }
+    }
+    if (++c->guard > guard_max && c->phase != PH_DONE) {  // safety net: the caps above end every solve first
+        c->kstatus = PRISM_NOT_CONVERGED;
+        c->phase = PH_DONE;
+    }
+    cudaGraphSetConditional(hk, c->phase != PH_DONE ? 1u : 0u);
+}
+
+// b = 0 ends a pass with x = 0 (bicgstab()'s memset on done == 4)
+__global__ void zero_if_rhs_zero_kernel(int n, double* x, const KState* S) {
+    if (S->done != 4) return;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS) x[i] = 0.0;
+}
+
+__global__ void ctl_outer_step_kernel(SolveCtl* c, const double* scal, cudaGraphConditionalHandle ho) {
+    if (threadIdx.x) return;
+    const double cur = scal[2] != 0.0 ? nanValue() : scal[0] / (scal[1] + EPSILON);
+    c->cur_res = cur;
+    if (c->kstatus != PRISM_OK && c->status == PRISM_OK) c->status = c->kstatus;
+    if (isnan(cur)) c->status = PRISM_NONFINITE;
+    c->outer += 1;
+    const bool conv = cur < c->eps;
+    if (conv) c->converged = 1;
+    cudaGraphSetConditional(ho, (!conv && c->outer < c->n_iter) ? 1u : 0u);
+}
+
+}  // namespace
+
+cudaStream_t CaptureStreams::at(int depth) {
+    if (depth < 0 || depth >= 3) fail(PRISM_INTERNAL, "conditional nodes nested too deep");
+    if (!s[depth]) PB_CUDA(cudaStreamCreateWithFlags(&s[depth], cudaStreamNonBlocking));
+    return s[depth];
+}
+CaptureStreams::~CaptureStreams() {
+    for (auto& x : s)
+        if (x) cudaStreamDestroy(x);
+}
+
+bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) return false;
+    return st == cudaStreamCaptureStatusActive;
+}
+
+cudaGraphConditionalHandle createConditional(cudaStream_t s, unsigned dflt) {
+    cudaStreamCaptureStatus st;
+    unsigned long long id;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps;
+    size_t nd;
+    PB_CUDA(cudaStreamGetCaptureInfo(s, &st, &id, &g, &deps, &nd));
+    if (st != cudaStreamCaptureStatusActive) fail(PRISM_INTERNAL, "conditional handle outside a capture");
+    cudaGraphConditionalHandle h;
+    PB_CUDA(cudaGraphConditionalHandleCreate(&h, g, dflt, cudaGraphCondAssignDefault));
+    return h;
+}
+
+void beginConditional(cudaStream_t s, cudaGraphConditionalNodeType type, cudaGraphConditionalHandle h,
+                      cudaStream_t body) {
+    cudaStreamCaptureStatus st;
+    unsigned long long id;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps;
+    size_t nd;
+    PB_CUDA(cudaStreamGetCaptureInfo(s, &st, &id, &g, &deps, &nd));
+    if (st != cudaStreamCaptureStatusActive) fail(PRISM_INTERNAL, "conditional node outside a capture");
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    PB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+    PB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    PB_CUDA(cudaStreamBeginCaptureToGraph(body, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed));
+}
+
+void endConditional(cudaStream_t body) {
+    cudaGraph_t g;
+    PB_CUDA(cudaStreamEndCapture(body, &g));
+}
+
+void emitSolveBegin(SolveCtl* ctl, long long n_iter, double eps, long long kmax, double tol,
+                    cudaGraphConditionalHandle outer, cudaStream_t s) {
+    ctl_solve_begin_kernel<<<1, 32, 0, s>>>(ctl, n_iter, eps, kmax, tol, outer); countLaunch();
+}
+
+void emitResidual(const SellMatrix& A, const double* b, const double* x, KrylovWork& w, cudaStream_t s) {
+    resid_kernel<<<waveGrid(resid_kernel, ceil_div(A.nslices, WARPS)), BS, 0, s>>>(
+        A.nslices, A.n, A.sl_off, A.col, A.vals, A.diag_pos, b, x, w.partials.p, w.counter.p, w.scal.p); countLaunch();
+}
+
+void emitInitResidual(SolveCtl* ctl, KrylovWork& w, cudaStream_t s) {
+    ctl_init_res_kernel<<<1, 32, 0, s>>>(ctl, w.scal.p); countLaunch();
+}
+
+void emitOuterStep(SolveCtl* ctl, KrylovWork& w, cudaGraphConditionalHandle outer, cudaStream_t s) {
+    ctl_outer_step_kernel<<<1, 32, 0, s>>>(ctl, w.scal.p, outer); countLaunch();
+}
+
+// bicgstab() (FP64) with its host loops turned into a device loop:
+//   WHILE (phase != DONE) { IF INIT {r = b - A x; init} IF ITER {GRAPH_UNROLL iterations}
+//                           IF CHECK {x = 0 if b = 0; unscale; accurate residual} controller }
+// The kernels and their order are those of the eager path, so the results are the same.
+void emitBicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, KrylovWork& w,
+                  cudaStream_t s, Amg* amg, const int* rowptr, const int* col, SolveCtl* ctl, CaptureStreams& cs,
+                  int depth) {
+    w.ensure(A.nslices * 32, A.nnz_padded, false);
+    const int n = A.n, gn = ceil_div(n, BS);
+    const bool scaled = amg == nullptr;
+    SellMatrix A64 = A;
+    double* X = x;
+    if (scaled) {
+        dinv_kernel<<<gn, BS, 0, s>>>(n, A.diag_pos, A.vals, w.dinv.p, x, w.xs.p); countLaunch();
+        int sgrid = std::min<int64_t>((A.nnz_padded + BS - 1) / BS, NUM_SMS * 32);
+        scale_kernel<double><<<sgrid, BS, 0, s>>>(A.nnz_padded, A.col, A.vals, w.dinv.p, w.As.p); countLaunch();
+        A64.vals = w.As.p;
+        X = w.xs.p;
+    } else {
+        if (!rowptr || !col) fail(PRISM_INTERNAL, "AMG preconditioner without a CSR pattern");
+        w.ensurePrec(false);
+        amg->setup(A, rowptr, col, false, s);
+    }
+    KState* S = w.state.p;
+    Vecs<double> V{X, w.r.p, w.r0.p, w.p.p, w.v.p, w.s.p, w.t.p};
+    const int vg = vecGrid(n), sg = sliceGrid(A.nslices);
+    const long long guard_max = 4 * (maxit / GRAPH_UNROLL + 64) + 256;
+    cudaStream_t body = cs.at(depth), sub = cs.at(depth + 1);
+    cudaGraphConditionalHandle hk = createConditional(s, 0);
+    ctl_krylov_begin_kernel<<<1, 32, 0, s>>>(ctl, S, hk); countLaunch();
+    beginConditional(s, cudaGraphCondTypeWhile, hk, body);
+    cudaGraphConditionalHandle hi = createConditional(body, 0), ht = createConditional(body, 0),
+                               hc = createConditional(body, 0);
+    ctl_phase_kernel<<<1, 32, 0, body>>>(ctl, hi, ht, hc); countLaunch();
+    beginConditional(body, cudaGraphCondTypeIf, hi, sub);
+    spmv_kernel<double, 0><<<sg, BS, 0, sub>>>(A.nslices, n, A.sl_off, A.col, A64.vals, V.x, V.r, nullptr, nullptr,
+                                               nullptr, nullptr); countLaunch();
+    init_kernel<double><<<vg, BS, 0, sub>>>(n, V.r, b, V.r0, V.p, V.v, 0, tol, w.partials.p, w.counter.p, S); countLaunch();
+    endConditional(sub);
+    beginConditional(body, cudaGraphCondTypeIf, ht, sub);
+    iterateEager<double>(A, A64.vals, V, amg, w.y.p, w.z.p, GRAPH_UNROLL, false, w, sub);
+    endConditional(sub);
+    beginConditional(body, cudaGraphCondTypeIf, hc, sub);
+    zero_if_rhs_zero_kernel<<<vg, BS, 0, sub>>>(n, X, S); countLaunch();
+    if (scaled) {
+        unscale_kernel<<<gn, BS, 0, sub>>>(n, w.dinv.p, w.xs.p, x); countLaunch();
+    }
+    spmv(A, x, w.tmp.p, sub);
+    refine_residual_kernel<<<vg, BS, 0, sub>>>(n, w.tmp.p, b, reinterpret_cast<float*>(w.s.p), w.partials.p,
+                                               w.counter.p, w.scal.p); countLaunch();
+    endConditional(sub);
+    ctl_krylov_step_kernel<<<1, 32, 0, body>>>(ctl, S, w.scal.p, guard_max, hk); countLaunch();
+    endConditional(body);
 }
 
 }  // namespace pb

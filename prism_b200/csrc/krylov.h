@@ -94,4 +94,54 @@ void spmv(const SellMatrix& A, const double* x, double* y, cudaStream_t s);
 // H-operator of the explicit momentum step: x_new = (b - (A x - diag x)) / diag  (PRIME.cpp:39-56)
 void explicitUpdate(const SellMatrix& A, const double* b, const double* x, double* xnew, cudaStream_t s);
 
+// ---- solves inside a CUDA graph ------------------------------------------
+// A solve captured into a graph runs its loops on the device: conditional
+// WHILE/IF graph nodes repeat the BiCGSTAB iteration, the restarts and the
+// accurate-residual passes of bicgstab() and the outer steps of ISolver::solve,
+// decided by one-thread controller kernels that read the solver state, so the
+// replayed graph needs no host round trip. SolveCtl is the device record of one
+// such solve (read back after the graph ran).
+struct SolveCtl {
+    long long n_iter, outer;       // ISolver::solve: steps allowed / done
+    double eps, init_res, cur_res;
+    int converged, status;
+    long long kmax, maxit_left, krylov_iterations;
+    double tol, krylov_rel;
+    int phase, pass, restarts, kstatus;
+    long long guard;  // controller passes of the current BiCGSTAB solve
+};
+
+// Helper streams for the bodies of nested conditional nodes (one per depth).
+struct CaptureStreams {
+    cudaStream_t s[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t at(int depth);
+    ~CaptureStreams();
+};
+// A conditional handle of the graph being captured on s (reset to dflt at every launch).
+cudaGraphConditionalHandle createConditional(cudaStream_t s, unsigned dflt);
+// Adds a conditional node (cudaGraphCondTypeWhile / If) on handle h after the
+// current capture frontier of s and starts capturing its body on body.
+void beginConditional(cudaStream_t s, cudaGraphConditionalNodeType type, cudaGraphConditionalHandle h,
+                      cudaStream_t body);
+void endConditional(cudaStream_t body);
+bool capturing(cudaStream_t s);
+
+// Device-controlled pieces of solve(), emitted into the capture on s:
+// ctl := ISolver::solve bookkeeping for n_iter steps, eps, kmax, tol
+// (and switches on the outer loop's condition)
+void emitSolveBegin(SolveCtl* ctl, long long n_iter, double eps, long long kmax, double tol,
+                    cudaGraphConditionalHandle outer, cudaStream_t s);
+// w.scal := max|A x - b|, max|diag(A) x|, non-finite flag (the scaled residual's parts)
+void emitResidual(const SellMatrix& A, const double* b, const double* x, KrylovWork& w, cudaStream_t s);
+// ctl->init_res := the scaled residual in w.scal
+void emitInitResidual(SolveCtl* ctl, KrylovWork& w, cudaStream_t s);
+// one ISolver::solve step's end: ctl->cur_res from w.scal, status, converged,
+// outer count; sets the outer loop's condition (continue while not converged
+// and outer < n_iter)
+void emitOuterStep(SolveCtl* ctl, KrylovWork& w, cudaGraphConditionalHandle outer, cudaStream_t s);
+// the FP64 bicgstab() of one step, as device-controlled nodes (streams: helpers for the bodies)
+void emitBicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, KrylovWork& w,
+                  cudaStream_t s, Amg* amg, const int* rowptr, const int* col, SolveCtl* ctl, CaptureStreams& cs,
+                  int depth);
+
 }  // namespace pb

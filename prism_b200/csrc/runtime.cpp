@@ -87,10 +87,10 @@ void checkVectorFlux(const Vector& U, const std::string& who, int only = -1) {
 
 // ------------------------------------------------------------------ mesh
 Mesh::~Mesh() {
-    if (stream) {
-        cudaStreamSynchronize(stream);
-        cudaStreamDestroy(stream);
-    }
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph_host) cudaFreeHost(graph_host);
+    if (stream) cudaStreamDestroy(stream);
 }
 
 MeshView Mesh::view() const {
@@ -504,8 +504,20 @@ int choosePreconditioner(int pc, int64_t n) {
     return pc;
 }
 
+namespace {
+// set while a solve or step is being captured into a graph (graph_capture below)
+struct GraphCapture {
+    Mesh* m = nullptr;
+    int used = 0;
+};
+thread_local GraphCapture* g_capture = nullptr;
+constexpr int GRAPH_SLOTS = 256;  // captured solves per graph
+PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o);
+}  // namespace
+
 // ISolver::solve (numerics/solver.cpp:27-82)
 PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
+    if (g_capture) return solveCaptured(eq, o);
     Scalar& phi = *eq.phi;
     Mesh& m = *phi.m;
     updateCoeffs(eq);
@@ -609,13 +621,15 @@ struct PhaseTimer {
     std::string what;
     cudaStream_t s;
     std::chrono::steady_clock::time_point t0;
+    bool on = false;
     PhaseTimer(std::string w, cudaStream_t st) : what(std::move(w)), s(st) {
-        if (!verbose()) return;
+        on = verbose() && !capturing(st);
+        if (!on) return;
         cudaStreamSynchronize(s);
         t0 = std::chrono::steady_clock::now();
     }
     ~PhaseTimer() {
-        if (!verbose()) return;
+        if (!on) return;
         cudaStreamSynchronize(s);
         std::fprintf(stderr, "[prism] phase %s: %.3f ms\n", what.c_str(),
                      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
@@ -1070,6 +1084,170 @@ void cellToPoint(Mesh& m, const double* const* comp, int ncomp, int64_t stride, 
     pc.stride = stride;
     pc.ncomp = ncomp;
     launchCellToPoint(m.view(), pm, pc, out, m.stream);
+}
+
+// ------------------------------------------------------------------ solves and steps as one graph
+namespace {
+
+// solve() with its loops as device-side conditional nodes (ISolver::solve's
+// outer steps around bicgstab()'s passes, restarts and batches): the same
+// kernels in the same order as the ordinary path, decided on the device.
+PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o) {
+    Scalar& phi = *eq.phi;
+    Mesh& m = *phi.m;
+    if (g_capture->m != &m) fail(PRISM_BAD_ARG, "a graph step spans more than one mesh");
+    if (o.method != PRISM_SOLVER_BICGSTAB || o.precision != PRISM_PREC_FP64)
+        fail(PRISM_BAD_ARG, "graph mode runs FP64 BiCGSTAB only");
+    if (g_capture->used >= GRAPH_SLOTS) fail(PRISM_BAD_ARG, "too many solves in one graph step");
+    const int slot = g_capture->used++;
+    SolveCtl* ctl = m.graph_ctl.p + slot;
+    cudaStream_t s = m.stream;
+    updateCoeffs(eq);
+    relax(eq);
+    if (o.ref_cell >= 0 && o.ref_cell < m.nc)
+        launchPinDev(eq.A.p, eq.b.p, m.pat.diag_pos.p, (int)o.ref_cell, o.ref_value, s);
+    SellMatrix A = m.matrix(eq.A.p);
+    const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
+    const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
+    Amg* amg = nullptr;
+    if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
+        if (!eq.amg) eq.amg = std::make_shared<Amg>();
+        amg = eq.amg.get();
+    }
+    const long long n_iter = std::max<long long>(o.n_iter, 0);
+    cudaGraphConditionalHandle outer = createConditional(s, 0);
+    emitSolveBegin(ctl, n_iter, o.eps, kmax, ktol, outer, s);
+    if (n_iter > 0) {
+        ++phi.event;
+        emitResidual(A, eq.b.p, phi.v.p, m.kw, s);
+        emitInitResidual(ctl, m.kw, s);
+        cudaStream_t body = m.cs.at(0);
+        beginConditional(s, cudaGraphCondTypeWhile, outer, body);
+        phi.event += 2;
+        emitBicgstab(A, eq.b.p, phi.v.p, ktol, kmax, m.kw, body, amg, m.pat.rowptr.p, m.pat.col.p, ctl, m.cs, 1);
+        ++phi.event;
+        emitResidual(A, eq.b.p, phi.v.p, m.kw, body);
+        emitOuterStep(ctl, m.kw, outer, body);
+        endConditional(body);
+    }
+    if (o.clear_coeffs) zeroOutCoeffs(eq);
+    PrismSolveResult r{};
+    r.iterations = -(slot + 1);  // the device record of this solve, read after the launch
+    return r;
+}
+
+PrismSolveResult fromCtl(const SolveCtl& c) {
+    PrismSolveResult r{};
+    r.iterations = c.outer;
+    r.initial_residual = c.init_res;
+    r.final_residual = c.cur_res;
+    r.converged = c.converged;
+    r.status = c.status;
+    r.krylov_iterations = c.krylov_iterations;
+    r.krylov_rel_residual = c.krylov_rel;
+    return r;
+}
+
+// Captures f (host code issuing the work of solves and steps on m's stream)
+// into one graph, launches it (updating the previous call's executable graph
+// in place when only parameters changed) and reads the solves' records back.
+int runAsGraph(Mesh& m, const std::function<void()>& f) {
+    // least-squares operators are built on the host at first use: build them now, outside the capture
+    m.ensureLeastSquares();
+    if (!m.graph_ctl) m.graph_ctl.alloc(GRAPH_SLOTS);
+    if (!m.graph_host) PB_CUDA(cudaMallocHost(&m.graph_host, GRAPH_SLOTS * sizeof(SolveCtl)));
+    for (int d = 0; d < 3; ++d) m.cs.at(d);
+    GraphCapture ctx;
+    ctx.m = &m;
+    PB_CUDA(cudaStreamBeginCapture(m.stream, cudaStreamCaptureModeRelaxed));
+    g_capture = &ctx;
+    cudaGraph_t graph = nullptr;
+    try {
+        f();
+    } catch (...) {
+        g_capture = nullptr;
+        cudaStreamEndCapture(m.stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        throw;
+    }
+    g_capture = nullptr;
+    PB_CUDA(cudaStreamEndCapture(m.stream, &graph));
+    bool updated = false;
+    if (m.graph_exec) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(m.graph_exec, graph, &info) == cudaSuccess;
+        if (!updated) {
+            cudaGetLastError();
+            cudaGraphExecDestroy(m.graph_exec);
+            m.graph_exec = nullptr;
+        }
+    }
+    if (!updated) {
+        cudaError_t e = cudaGraphInstantiate(&m.graph_exec, graph, 0);
+        if (e != cudaSuccess) m.graph_exec = nullptr;
+        cudaGraphDestroy(graph);
+        PB_CUDA(e);
+    } else {
+        cudaGraphDestroy(graph);
+    }
+    PB_CUDA(cudaGraphLaunch(m.graph_exec, m.stream));
+    graphLaunchCounter().fetch_add(1, std::memory_order_relaxed);
+    if (ctx.used)
+        PB_CUDA(cudaMemcpyAsync(m.graph_host, m.graph_ctl.p, ctx.used * sizeof(SolveCtl), cudaMemcpyDeviceToHost,
+                                m.stream));
+    PB_CUDA(cudaStreamSynchronize(m.stream));
+    return ctx.used;
+}
+
+}  // namespace
+
+bool graphReady(const Transport& eq, const PrismSolveOpts& o) {
+    const Mesh& m = *eq.phi->m;
+    if (o.method != PRISM_SOLVER_BICGSTAB || o.precision != PRISM_PREC_FP64) return false;
+    if (!eq.A || !eq.b || m.kw.n != m.n_pad) return false;
+    if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
+        if (!eq.amg || !eq.amg->built || !m.kw.y) return false;
+        for (auto& L : eq.amg->levels)
+            if (!L->b || !L->dinv) return false;
+    }
+    return true;
+}
+
+bool stepGraphReady(const std::vector<Transport*>& mom, const Vector& U, const Scalar& p, const PrismSolveOpts& so,
+                    bool momentum_solved) {
+    const Mesh& m = *p.m;
+    for (auto* eq : mom) {
+        if (momentum_solved && !graphReady(*eq, so)) return false;
+        if (!eq->A || !eq->b) return false;
+    }
+    if (!m.p_eq || !m.p_corr || !m.p_D || !m.p_eq->phi) return false;
+    (void)U;
+    return graphReady(*m.p_eq, so);
+}
+
+PrismSolveResult solveAsGraph(Transport& eq, const PrismSolveOpts& o) {
+    Mesh& m = *eq.phi->m;
+    PrismSolveResult out{};
+    const int used = runAsGraph(m, [&] { out = solve(eq, o); });
+    if (used != 1) fail(PRISM_INTERNAL, "graph solve recorded no solve");
+    return fromCtl(m.graph_host[0]);
+}
+
+void stepAsGraph(Mesh& m, const std::function<void()>& step, std::vector<Report>& rep) {
+    const size_t first = rep.size();
+    const int used = runAsGraph(m, step);
+    for (size_t i = first; i < rep.size(); ++i) {
+        Report& r = rep[i];
+        if (r.n >= 0) continue;
+        const int slot = (int)(-r.n - 1);
+        if (slot >= used) fail(PRISM_INTERNAL, "graph step report without a record");
+        const SolveCtl& c = m.graph_host[slot];
+        r.n = c.outer;
+        r.init = c.init_res;
+        r.fin = c.cur_res;
+        r.conv = c.converged != 0;
+    }
 }
 
 }  // namespace pb

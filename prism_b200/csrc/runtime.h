@@ -3,6 +3,7 @@
 #pragma once
 
 #include <limits>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -51,6 +52,11 @@ struct Mesh {
     DevBuf<int> v2c_cell;
     bool points_ready = false;
     bool frozen = false;  // fields exist: the cells can no longer be renumbered
+    // solves and steps run as one CUDA graph launch (PrismSolveOpts.graph)
+    CaptureStreams cs;
+    DevBuf<SolveCtl> graph_ctl;
+    SolveCtl* graph_host = nullptr;  // pinned copy of graph_ctl
+    cudaGraphExec_t graph_exec = nullptr;
 
     ~Mesh();
     MeshView view() const;
@@ -161,6 +167,18 @@ void primeStep(const PrismSIMPLEControls& c, std::vector<Transport*>& mom, Vecto
 void pisoStep(const PrismPISOControls& c, std::vector<Transport*>& mom, Vector& U, Vector& mdot, Scalar& p,
               const PrismSolveOpts& so, std::vector<Report>& rep);
 bool needsPressureReference(const Scalar& p);
+
+// PrismSolveOpts.graph: a solve or a SIMPLE/PRIME/PISO step captured into one
+// CUDA graph and launched once. Ready when the solver is FP64 BiCGSTAB and the
+// equations' coefficient and work buffers, AMG hierarchies and least-squares
+// operators exist (built by an earlier ordinary call), since a capture may not
+// allocate or wait on the host.
+bool graphReady(const Transport& eq, const PrismSolveOpts& o);
+// momentum_solved: the step solves the momentum equations (SIMPLE, PISO), not only applies them (PRIME)
+bool stepGraphReady(const std::vector<Transport*>& mom, const Vector& U, const Scalar& p, const PrismSolveOpts& so,
+                    bool momentum_solved);
+PrismSolveResult solveAsGraph(Transport& eq, const PrismSolveOpts& o);
+void stepAsGraph(Mesh& m, const std::function<void()>& step, std::vector<Report>& rep);
 
 // Steady fixed point of repeated solve() calls and its discrete adjoint (pure
 // diffusion with a scalar kappa). steadySolve repeats solve(eq, o) until the
