@@ -1,8 +1,8 @@
 """CPU oracle of the Prism hot path -- TEST INFRASTRUCTURE, not product code.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load this
-package, and only as the checker (or, for the timed CPU baseline, as the
-restated reference implementation). It exposes the same C-ABI as the sm_100a
+package, and only to check the GPU results against (or, for the timed CPU
+baseline, as the restated reference implementation). It exposes the same C-ABI as the sm_100a
 library with the prefix ``orc_``.
 """
 import ctypes

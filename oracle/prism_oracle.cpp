@@ -1,6 +1,6 @@
 // prism_oracle.cpp -- CPU oracle for the Prism hot path. TEST INFRASTRUCTURE ONLY.
 //
-// This file is the checker, not the product: only tests/, __graft_entry__.smoke()
+// This file checks the product and is not part of it: only tests/, __graft_entry__.smoke()
 // and bench.py's cpu_baseline / --impl reference leg load it. It restates, in
 // plain single-threaded FP64 C++, the algorithms of eigemx/prism's hot path:
 // the UNV -> PMesh conversion and face reordering, field face values and
