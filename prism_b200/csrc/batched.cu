@@ -22,6 +22,7 @@
 
 #include <chrono>
 #include <cmath>
+#include <cstring>
 
 #include "batched.h"
 
@@ -620,6 +621,30 @@ __global__ void fill_int_kernel(int n, int value, int* out) {
     if (i < n) out[i] = value;
 }
 // D^-1 of every row (1 on padding rows)
+// one system's buffers and its place in the concatenated ones
+struct CopyEntry {
+    const double* vals;
+    const double* b;
+    double* x;
+    long long nnz, nnz_off, row_off;
+    int n;
+};
+// gather (dir 0: systems -> concatenated values, b, x) or scatter (dir 1: x back);
+// blockIdx.y is the system, blockIdx.x strides within it
+__global__ void batch_copy_kernel(const CopyEntry* tab, int dir, double* A64, double* b64, double* x64) {
+    const CopyEntry e = tab[blockIdx.y];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    if (dir == 0) {
+        for (long long i = t; i < e.nnz; i += stride) A64[e.nnz_off + i] = e.vals[i];
+        for (long long i = t; i < e.n; i += stride) {
+            b64[e.row_off + i] = e.b[i];
+            x64[e.row_off + i] = e.x[i];
+        }
+    } else {
+        for (long long i = t; i < e.n; i += stride) e.x[i] = x64[e.row_off + i];
+    }
+}
+
 __global__ void batch_dinv_kernel(int nrows, const int* diag, const double* A64, double* dinv) {
     int r = blockIdx.x * BS + threadIdx.x;
     if (r >= nrows) return;
@@ -733,20 +758,37 @@ std::vector<BatchOut> runBatch(const std::vector<BatchSystem>& sys, BatchPlan& p
         for (auto* b : {&pl.r64b, &pl.r064, &pl.p64, &pl.v64, &pl.s64, &pl.t64, &pl.d64}) ensure(*b, nrows);
     }
     InnerBufs<T> ib = innerBufs(pl, T{});
-    // values of this solve
+    // the systems' buffers, for the gather and scatter kernels
+    std::vector<CopyEntry> tab(sys.size());
     for (size_t i = 0; i < sys.size(); ++i) {
         const BatchSystem& q = sys[i];
-        PB_CUDA(cudaMemcpyAsync(pl.A64.p + pl.nnz_off[i], q.vals, q.nnz_padded * sizeof(double),
-                                cudaMemcpyDeviceToDevice, s));
-        PB_CUDA(cudaMemcpyAsync(pl.b64.p + 32 * (int64_t)pl.slice0[i], q.b, q.n * sizeof(double),
-                                cudaMemcpyDeviceToDevice, s));
-        PB_CUDA(cudaMemcpyAsync(pl.x64.p + 32 * (int64_t)pl.slice0[i], q.x, q.n * sizeof(double),
-                                cudaMemcpyDeviceToDevice, s));
+        tab[i] = {q.vals, q.b, q.x, (long long)q.nnz_padded, (long long)pl.nnz_off[i], 32LL * pl.slice0[i], q.n};
     }
-    batch_dinv_kernel<<<grid(nrows), BS, 0, s>>>(nrows, pl.diag.p, pl.A64.p, pl.dinv.p); countLaunch();
-    const int sg = (int)std::min<int64_t>(grid(pl.nnz), NUM_SMS * 32);
-    batch_scale_kernel<T><<<sg, BS, 0, s>>>(pl.nnz, pl.col.p, pl.A64.p, pl.dinv.p, ib.A); countLaunch();
-    PB_LAUNCH("batched setup");
+    std::vector<uintptr_t> key = {sizeof(T), (uintptr_t)max_inner, (uintptr_t)max_pass, (uintptr_t)maxit};
+    for (double v : {tol, itol}) {
+        uint64_t bits;
+        std::memcpy(&bits, &v, sizeof bits);
+        key.push_back((uintptr_t)bits);
+    }
+    for (const auto& e : tab)
+        for (uintptr_t v : {(uintptr_t)e.vals, (uintptr_t)e.b, (uintptr_t)e.x}) key.push_back(v);
+    const size_t tab_bytes = tab.size() * sizeof(CopyEntry);
+    // graph_key = this prefix (6 entries) + the systems' pointers + the launch shape (2 entries)
+    const bool same_systems = pl.graph_key.size() == key.size() + 2 &&
+                              std::equal(key.begin() + 6, key.end(), pl.graph_key.begin() + 6);
+    if (!same_systems) {
+        if (pl.copy_tab.n < tab_bytes) pl.copy_tab.alloc(tab_bytes);
+        pl.copy_tab.upload(reinterpret_cast<const unsigned char*>(tab.data()), tab_bytes, s);
+    }
+    const CopyEntry* dtab = reinterpret_cast<const CopyEntry*>(pl.copy_tab.p);
+    const dim3 copy_grid(64, (unsigned)sys.size());
+    auto gather = [&] {
+        batch_copy_kernel<<<copy_grid, BS, 0, s>>>(dtab, 0, pl.A64.p, pl.b64.p, pl.x64.p); countLaunch();
+        batch_dinv_kernel<<<grid(nrows), BS, 0, s>>>(nrows, pl.diag.p, pl.A64.p, pl.dinv.p); countLaunch();
+        const int sg = (int)std::min<int64_t>(grid(pl.nnz), NUM_SMS * 32);
+        batch_scale_kernel<T><<<sg, BS, 0, s>>>(pl.nnz, pl.col.p, pl.A64.p, pl.dinv.p, ib.A); countLaunch();
+        PB_LAUNCH("batched setup");
+    };
 
     BP<T> P{};
     P.nprob = pl.nprob;
@@ -790,6 +832,7 @@ std::vector<BatchOut> runBatch(const std::vector<BatchSystem>& sys, BatchPlan& p
     // autotune the launch shape on this batch: a few steps of every candidate from the same start
     BatchTuning& tune = pl.tune[sizeof(T) == 4 ? 1 : 0];
     if (tune.block == 0) {
+        gather();
         DevBuf<double> xsave(nrows);
         PB_CUDA(cudaMemcpyAsync(xsave.p, pl.x64.p, nrows * sizeof(double), cudaMemcpyDeviceToDevice, s));
         cudaEvent_t e0, e1;
@@ -820,21 +863,55 @@ std::vector<BatchOut> runBatch(const std::vector<BatchSystem>& sys, BatchPlan& p
             std::fprintf(stderr, "[prism] batched solver tuned: block %d, %d lanes per row (%.3f ms for 8 steps)\n",
                          tune.block, tune.lpr, tune.ms);
     }
-    init();
     // every step is one iteration (plus at most one refinement) of every active system
     P.max_steps = (int)std::min<long long>(maxit + (long long)max_pass + 2, (long long)1 << 30);
+    key.push_back((uintptr_t)tune.block);
+    key.push_back((uintptr_t)tune.lpr);
+    // the call: gather, set-up, the persistent solve and the scatter of the solutions
+    auto call = [&] {
+        gather();
+        init();
+        launchBatch(P, tune.block, tune.lpr, s);
+        PB_LAUNCH("batched solve");
+        batch_copy_kernel<<<copy_grid, BS, 0, s>>>(dtab, 1, pl.A64.p, pl.b64.p, pl.x64.p); countLaunch();
+    };
     const auto t0 = std::chrono::steady_clock::now();
-    launchBatch(P, tune.block, tune.lpr, s);
-    PB_LAUNCH("batched solve");
+    if (pl.graph.g && key == pl.graph_key) {
+        PB_CUDA(cudaGraphLaunch(pl.graph.g, s));
+        graphLaunchCounter().fetch_add(1, std::memory_order_relaxed);
+    } else {
+        pl.graph.reset();
+        pl.graph_key.clear();
+        // a capture that the runtime refuses leaves nothing executed: run the call directly
+        cudaGraph_t g = nullptr;
+        bool captured = false;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+            try {
+                call();
+                captured = cudaStreamEndCapture(s, &g) == cudaSuccess && g != nullptr;
+            } catch (...) {
+                cudaStreamEndCapture(s, &g);
+            }
+            if (captured && cudaGraphInstantiate(&pl.graph.g, g, 0) != cudaSuccess) {
+                pl.graph.g = nullptr;
+                captured = false;
+            }
+            if (g) cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+        if (captured) {
+            pl.graph_key = key;
+            PB_CUDA(cudaGraphLaunch(pl.graph.g, s));
+            graphLaunchCounter().fetch_add(1, std::memory_order_relaxed);
+        } else {
+            call();
+        }
+    }
     if (verbose()) {
         PB_CUDA(cudaStreamSynchronize(s));
-        std::fprintf(stderr, "[prism] batched solve of %d systems (%d rows): %.3f ms in one launch\n", pl.nprob,
+        std::fprintf(stderr, "[prism] batched solve of %d systems (%d rows): %.3f ms in one graph launch\n", pl.nprob,
                      nrows, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     }
-    // solutions back, per-system results
-    for (size_t i = 0; i < sys.size(); ++i)
-        PB_CUDA(cudaMemcpyAsync(sys[i].x, pl.x64.p + 32 * (int64_t)pl.slice0[i], sys[i].n * sizeof(double),
-                                cudaMemcpyDeviceToDevice, s));
     std::vector<BState> hs(pl.nprob);
     PB_CUDA(cudaMemcpyAsync(hs.data(), P.st, pl.nprob * sizeof(BState), cudaMemcpyDeviceToHost, s));
     PB_CUDA(cudaStreamSynchronize(s));

@@ -46,6 +46,30 @@ struct BatchPlan {
     DevBuf<unsigned char> state;  // per-problem solver state
     DevBuf<int> ctl;
     BatchTuning tune[2];  // [0] FP64 inner, [1] FP32 inner
+    // per call: the systems' values, right-hand sides and guesses gathered into the
+    // concatenated buffers by one kernel (table of source pointers), and the whole
+    // call -- gather, set-up, the persistent solve, scatter of the solutions -- kept
+    // as one CUDA graph, replayed while the systems' buffers and options are the same
+    DevBuf<unsigned char> copy_tab;
+    std::vector<uintptr_t> graph_key;
+    struct Exec {  // owned executable graph (movable with the plan)
+        cudaGraphExec_t g = nullptr;
+        Exec() = default;
+        Exec(Exec&& o) noexcept : g(o.g) { o.g = nullptr; }
+        Exec& operator=(Exec&& o) noexcept {
+            if (this != &o) {
+                reset();
+                g = o.g;
+                o.g = nullptr;
+            }
+            return *this;
+        }
+        ~Exec() { reset(); }
+        void reset() {
+            if (g) cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    } graph;
 };
 
 // Solves every system to ||b - Ax|| <= tol ||b|| (FP64 residual): BiCGSTAB

@@ -56,3 +56,25 @@ def test_batch_zero_rhs_and_bad_args(gpu):
     assert res[1].status == A.OK
     with pytest.raises(PrismError):
         api.BatchSolver(api.Jacobi(), lib=gpu).solve([q["eqn"]])
+
+
+def test_batch_call_is_one_graph_launch(gpu):
+    # each call (gather, set-up, the persistent solve, scatter) is one CUDA graph launch,
+    # captured on the first call and replayed while the systems' buffers stay the same
+    import ctypes
+    sizes = [6, 11, 4, 9]
+    probs = [cases.diffusion_box(N, gpu, seed=40 + i) for i, N in enumerate(sizes)]
+    bs = api.BatchSolver(api.BiCGSTAB(precision=A.PREC_MIXED, krylov_tol=1e-12), lib=gpu)
+    sols = []
+    gpu.check(gpu.profile_start(16))
+    for _ in range(3):
+        for p in probs:
+            p["T"].set_values(np.zeros(p["mesh"].n_cells))
+        res = bs.solve([p["eqn"] for p in probs])
+        assert all(r.status == A.OK for r in res)
+        sols.append(np.concatenate([p["T"].values() for p in probs]))
+    prof = A.Profile()
+    gpu.check(gpu.profile_stop(ctypes.byref(prof)))
+    assert prof.graph_launches == 3
+    np.testing.assert_array_equal(sols[1], sols[0])
+    np.testing.assert_array_equal(sols[2], sols[0])
