@@ -18,6 +18,7 @@
 #include <cstring>
 #include <map>
 #include <numeric>
+#include <thread>
 
 #include "mesh_build.h"
 
@@ -61,6 +62,25 @@ int faceVerts(const PrismUnvMesh* d, int64_t e, int l, int64_t* out) {
     int n = kWedgeFaces[l][3] < 0 ? 3 : 4;
     for (int i = 0; i < n; ++i) out[i] = en[kWedgeFaces[l][i]];
     return n;
+}
+
+// f(begin, end) over [0, n) split across host threads; f must not throw
+template <typename F>
+void parallelFor(int64_t n, F&& f) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const unsigned nt = std::min<unsigned>(hw ? hw : 1, 32);
+    if (n < 200000 || nt == 1) {
+        f(int64_t(0), n);
+        return;
+    }
+    const int64_t chunk = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < nt; ++t) {
+        const int64_t b = t * chunk, e = std::min<int64_t>(n, b + chunk);
+        if (b >= e) break;
+        th.emplace_back([&f, b, e] { f(b, e); });
+    }
+    for (auto& x : th) x.join();
 }
 
 struct Key {
@@ -113,9 +133,10 @@ std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
         int32_t local;  // -1: boundary element
         int32_t cell;   // -1: boundary element
     };
-    std::vector<Occ> occ;
+    // validation and counts (serial), then the keys of every occurrence (threads)
     std::vector<int64_t> cell_elem;
-    std::vector<int64_t> bface_of_elem(ne, -1);  // later: face id of a boundary element
+    std::vector<int64_t> occ_off(ne + 1, 0);
+    std::vector<int32_t> cell_of_elem(ne, -1);
     int64_t tmp[8];
     for (int64_t e = 0; e < ne; ++e) {
         int k = d->elem_kind[e];
@@ -123,34 +144,64 @@ std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
         const int64_t* en = d->elem_nodes + d->elem_offsets[e];
         for (int64_t i = 0; i < nn; ++i)
             if (en[i] < 0 || en[i] >= d->n_nodes) fail(PRISM_INVALID_MESH, "element node index out of range");
-        if (k == PRISM_ELEM_LINE) continue;
-        if (k == PRISM_ELEM_TRIANGLE || k == PRISM_ELEM_QUAD) {
+        int cnt = 0;
+        if (k == PRISM_ELEM_LINE) {
+        } else if (k == PRISM_ELEM_TRIANGLE || k == PRISM_ELEM_QUAD) {
             int n = faceVerts(d, e, -1, tmp);
             if (n != (k == PRISM_ELEM_QUAD ? 4 : 3)) fail(PRISM_INVALID_MESH, "bad boundary element");
-            occ.push_back({makeKey(tmp, n), e, -1, -1});
+            cnt = 1;
         } else if (k == PRISM_ELEM_HEX || k == PRISM_ELEM_TETRA || k == PRISM_ELEM_WEDGE) {
             int need = k == PRISM_ELEM_HEX ? 8 : k == PRISM_ELEM_TETRA ? 4 : 6;
             if (nn != need) fail(PRISM_INVALID_MESH, "cell element with a wrong node count");
-            int32_t c = (int32_t)cell_elem.size();
+            cell_of_elem[e] = (int32_t)cell_elem.size();
             cell_elem.push_back(e);
-            for (int l = 0; l < nLocalFaces(k); ++l) {
-                int n = faceVerts(d, e, l, tmp);
-                occ.push_back({makeKey(tmp, n), e, l, c});
-            }
+            cnt = nLocalFaces(k);
         } else {
             fail(PRISM_INVALID_MESH, "unsupported element type");
         }
+        occ_off[e + 1] = occ_off[e] + cnt;
     }
+    std::vector<Occ> occ(occ_off[ne]);
+    parallelFor(ne, [&](int64_t e0, int64_t e1) {
+        int64_t t[8];
+        for (int64_t e = e0; e < e1; ++e) {
+            const int64_t o0 = occ_off[e], cnt = occ_off[e + 1] - o0;
+            if (cnt == 0) continue;
+            if (cell_of_elem[e] < 0) {
+                int n = faceVerts(d, e, -1, t);
+                occ[o0] = {makeKey(t, n), e, -1, -1};
+            } else {
+                for (int l = 0; l < (int)cnt; ++l) {
+                    int n = faceVerts(d, e, l, t);
+                    occ[o0 + l] = {makeKey(t, n), e, l, cell_of_elem[e]};
+                }
+            }
+        }
+    });
     if (cell_elem.empty()) fail(PRISM_INVALID_MESH, "mesh is empty or two dimensional");
     if (cell_elem.size() >= (size_t(1) << 31)) fail(PRISM_INVALID_MESH, "too many cells");
 
-    // ---- match occurrences: sort by (key, reading order)
+    // ---- match occurrences: order by (key, reading order). A stable counting sort
+    // on the smallest node id groups the occurrences into small buckets (the faces
+    // around one node), each then sorted by the full key: O(n) instead of a global sort.
     std::vector<int64_t> ord(occ.size());
-    std::iota(ord.begin(), ord.end(), 0);
-    std::sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) {
-        if (occ[a].key == occ[b].key) return a < b;
-        return occ[a].key < occ[b].key;
-    });
+    {
+        std::vector<int64_t> start((size_t)d->n_nodes + 1, 0);
+        for (const Occ& o : occ) start[(o.key.hi >> 32) + 1]++;
+        for (int64_t v = 0; v < d->n_nodes; ++v) start[v + 1] += start[v];
+        std::vector<int64_t> fill(start.begin(), start.end() - 1);
+        for (size_t o = 0; o < occ.size(); ++o) ord[fill[occ[o].key.hi >> 32]++] = (int64_t)o;
+        parallelFor(d->n_nodes, [&](int64_t v0, int64_t v1) {
+            for (int64_t v = v0; v < v1; ++v) {
+                auto b = ord.begin() + start[v], e = ord.begin() + start[v + 1];
+                if (e - b > 1)
+                    std::sort(b, e, [&](int64_t a, int64_t c) {
+                        if (occ[a].key == occ[c].key) return a < c;
+                        return occ[a].key < occ[c].key;
+                    });
+            }
+        });
+    }
     struct Run {
         int64_t first;   // occurrence index of creation
         int64_t owner_occ;
@@ -179,12 +230,6 @@ std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
         runs.push_back(r);
         i = j;
     }
-    // converter face id = rank of creation
-    std::vector<int64_t> by_creation(runs.size());
-    std::iota(by_creation.begin(), by_creation.end(), 0);
-    std::sort(by_creation.begin(), by_creation.end(), [&](int64_t a, int64_t b) { return runs[a].first < runs[b].first; });
-    std::vector<int64_t> conv_id(runs.size());
-    for (size_t k = 0; k < by_creation.size(); ++k) conv_id[by_creation[k]] = (int64_t)k;
     const int64_t nf = (int64_t)runs.size();
 
     // ---- groups -> patches (unv.cpp:298-371, 84-97)
@@ -233,8 +278,20 @@ std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
     for (size_t r = 0; r < runs.size(); ++r) (runs[r].bface ? bruns : iruns).push_back((int64_t)r);
     for (auto r : bruns)
         if (run_patch[r] < 0) fail(PRISM_INVALID_MESH, "boundary face without a patch");
-    std::sort(bruns.begin(), bruns.end(), [&](int64_t a, int64_t b) { return runs[a].owner_occ < runs[b].owner_occ; });
-    std::sort(iruns.begin(), iruns.end(), [&](int64_t a, int64_t b) { return runs[a].first < runs[b].first; });
+    // boundary faces in the order their owners were assigned, interior faces in creation
+    // order; both orders are by distinct occurrence indices, so a placement by index sorts them
+    {
+        std::vector<int64_t> at(occ.size(), -1);
+        for (auto r : bruns) at[runs[r].owner_occ] = r;
+        bruns.clear();
+        for (auto r : at)
+            if (r >= 0) bruns.push_back(r);
+        std::fill(at.begin(), at.end(), -1);
+        for (auto r : iruns) at[runs[r].first] = r;
+        iruns.clear();
+        for (auto r : at)
+            if (r >= 0) iruns.push_back(r);
+    }
     int64_t nb = (int64_t)bruns.size(), nne = 0;
     for (auto r : bruns)
         if (!hm->patches[run_patch[r]].empty) ++nne;
@@ -242,7 +299,6 @@ std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
     int64_t pos_ne = 0, pos_e = nne, pos_i = nb;
     for (auto r : bruns) new_id[r] = hm->patches[run_patch[r]].empty ? pos_e++ : pos_ne++;
     for (auto r : iruns) new_id[r] = pos_i++;
-    (void)conv_id;
 
     // ---- flatten
     const int64_t nc = (int64_t)cell_elem.size();
@@ -260,22 +316,25 @@ std::unique_ptr<HostMesh> buildHostMesh(const PrismUnvMesh* d) {
         hm->cc[k].assign(nc, 0.0);
     }
     hm->vol.assign(nc, 0.0);
-    V3 fv[8];
-    for (size_t r = 0; r < runs.size(); ++r) {
-        int64_t f = new_id[r];
-        const Occ& o = occ[runs[r].first];
-        int n = faceVerts(d, o.elem, o.local, tmp);
-        for (int i = 0; i < n; ++i) fv[i] = X[tmp[i]];
-        double a;
-        V3 nrm, ctr;
-        faceGeometry(fv, n, a, nrm, ctr);
-        hm->area[f] = a;
-        hm->normal[0][f] = nrm.x; hm->normal[1][f] = nrm.y; hm->normal[2][f] = nrm.z;
-        hm->fc[0][f] = ctr.x; hm->fc[1][f] = ctr.y; hm->fc[2][f] = ctr.z;
-        hm->owner[f] = runs[r].owner;
-        hm->nbr[f] = runs[r].nbr;
-        hm->patch[f] = run_patch[r];
-    }
+    parallelFor((int64_t)runs.size(), [&](int64_t r0, int64_t r1) {
+        V3 fv[8];
+        int64_t t[8];
+        for (int64_t r = r0; r < r1; ++r) {
+            int64_t f = new_id[r];
+            const Occ& o = occ[runs[r].first];
+            int n = faceVerts(d, o.elem, o.local, t);
+            for (int i = 0; i < n; ++i) fv[i] = X[t[i]];
+            double a;
+            V3 nrm, ctr;
+            faceGeometry(fv, n, a, nrm, ctr);
+            hm->area[f] = a;
+            hm->normal[0][f] = nrm.x; hm->normal[1][f] = nrm.y; hm->normal[2][f] = nrm.z;
+            hm->fc[0][f] = ctr.x; hm->fc[1][f] = ctr.y; hm->fc[2][f] = ctr.z;
+            hm->owner[f] = runs[r].owner;
+            hm->nbr[f] = runs[r].nbr;
+            hm->patch[f] = run_patch[r];
+        }
+    });
     for (int32_t p = 0; p < d->n_patches; ++p)
         for (auto r : patch_runs[p]) hm->patches[p].faces.push_back((int32_t)new_id[r]);
 
