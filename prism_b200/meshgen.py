@@ -19,23 +19,23 @@ PATCHES = ("left", "right", "bottom", "top", "back", "front")
 
 
 def _assemble(xyz, faces_by_patch, cells, cell_kind):
-    kinds, offs, conn = [], [0], []
-    groups = []
+    kinds, counts, conn, groups = [], [], [], []
+    start = 0
     for name in PATCHES:
         fl = faces_by_patch[name]
-        start = len(kinds)
         nverts = fl.shape[1]
-        kinds.extend([A.ELEM_QUAD if nverts == 4 else A.ELEM_TRIANGLE] * fl.shape[0])
+        kinds.append(np.full(fl.shape[0], A.ELEM_QUAD if nverts == 4 else A.ELEM_TRIANGLE, dtype=np.int32))
+        counts.append(np.full(fl.shape[0], nverts, dtype=np.int64))
         conn.append(fl.reshape(-1))
         groups.append((name, False, np.arange(start, start + fl.shape[0], dtype=np.int64)))
-    nb = len(kinds)
-    kinds = np.array(kinds + [cell_kind] * cells.shape[0], dtype=np.int32)
-    counts = np.array([4 if k == A.ELEM_QUAD else 3 for k in kinds[:nb]]
-                      + [cells.shape[1]] * cells.shape[0], dtype=np.int64)
-    offs = np.zeros(len(kinds) + 1, dtype=np.int64)
-    np.cumsum(counts, out=offs[1:])
+        start += fl.shape[0]
+    kinds.append(np.full(cells.shape[0], cell_kind, dtype=np.int32))
+    counts.append(np.full(cells.shape[0], cells.shape[1], dtype=np.int64))
     conn.append(cells.reshape(-1))
-    return UnvData(xyz, kinds, offs, np.concatenate(conn).astype(np.int64), groups)
+    counts = np.concatenate(counts)
+    offs = np.zeros(len(counts) + 1, dtype=np.int64)
+    np.cumsum(counts, out=offs[1:])
+    return UnvData(xyz, np.concatenate(kinds), offs, np.concatenate(conn).astype(np.int64), groups)
 
 
 def _grid_nodes(nx, ny, nz, lengths, origin, jitter, seed):
