@@ -357,6 +357,10 @@ typedef struct {
     double pressure_residual;
     int64_t p_ref_cell; /* -1: none */
     double p_ref_value;
+    int32_t batched_momentum; /* 1: the momentum predictors of a step are solved together in one
+                                 persistent launch (prism_batch_*: Jacobi-preconditioned BiCGSTAB
+                                 on every component at once) instead of one solve each; not a
+                                 reference control, default 0 */
 } PrismSIMPLEControls;
 
 typedef struct {
@@ -373,6 +377,7 @@ typedef struct {
     double pressure_residual;
     int64_t p_ref_cell;
     double p_ref_value;
+    int32_t batched_momentum; /* as in PrismSIMPLEControls */
 } PrismPISOControls;
 
 typedef struct {

@@ -1345,6 +1345,7 @@ inline void simpleDefaults(PrismSIMPLEControls* c) {
     c->pressure_residual = 1e-7;
     c->p_ref_cell = -1;
     c->p_ref_value = 0.0;
+    c->batched_momentum = 0;
 }
 inline void pisoDefaults(PrismPISOControls* c) {
     c->outer_iterations = 1;
@@ -1360,6 +1361,7 @@ inline void pisoDefaults(PrismPISOControls* c) {
     c->pressure_residual = 1e-4;
     c->p_ref_cell = -1;
     c->p_ref_value = 0.0;
+    c->batched_momentum = 0;
 }
 
 struct Report {

@@ -89,7 +89,7 @@ class SIMPLEControls(C.Structure):
     _fields_ = [("momentum_urf", f64), ("momentum_max_iter", i64), ("momentum_residual", f64),
                 ("momentum_residual_stop", f64), ("non_ortho_correctors", i64),
                 ("pressure_urf", f64), ("pressure_max_iter", i64), ("pressure_residual", f64),
-                ("p_ref_cell", i64), ("p_ref_value", f64)]
+                ("p_ref_cell", i64), ("p_ref_value", f64), ("batched_momentum", i32)]
 
 
 class PISOControls(C.Structure):
@@ -98,7 +98,7 @@ class PISOControls(C.Structure):
                 ("momentum_max_iter", i64), ("momentum_residual", f64),
                 ("momentum_residual_stop", f64), ("non_ortho_correctors", i64),
                 ("pressure_urf", f64), ("pressure_max_iter", i64), ("pressure_residual", f64),
-                ("p_ref_cell", i64), ("p_ref_value", f64)]
+                ("p_ref_cell", i64), ("p_ref_value", f64), ("batched_momentum", i32)]
 
 
 class Report(C.Structure):

@@ -642,6 +642,7 @@ class SIMPLEControls:
     pressure_residual: float = 1e-7
     p_ref_cell: Optional[int] = None
     p_ref_value: float = 0.0
+    batched_momentum: bool = False  # momentum components solved together in one persistent launch
 
     def to_c(self):
         c = A.SIMPLEControls()
@@ -666,6 +667,7 @@ class PISOControls:
     pressure_residual: float = 1e-4
     p_ref_cell: Optional[int] = None
     p_ref_value: float = 0.0
+    batched_momentum: bool = False
 
     def to_c(self):
         c = A.PISOControls()

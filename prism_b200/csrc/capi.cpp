@@ -840,7 +840,7 @@ API int prism_simple_step(const PrismSIMPLEControls* c, PrismTransport* const* m
         auto v = momVec(mom, n_mom);
         std::vector<Report> r;
         const PrismSolveOpts opts = optsOrDefault(so);
-        if (opts.graph && stepGraphReady(v, *U->v, *p->s, opts, true))
+        if (opts.graph && !c->batched_momentum && stepGraphReady(v, *U->v, *p->s, opts, true))
             stepAsGraph(*p->s->m, [&] { simpleStep(*c, v, *U->v, *mdot->v, *p->s, opts, r); }, r);
         else
             simpleStep(*c, v, *U->v, *mdot->v, *p->s, opts, r);
@@ -872,7 +872,7 @@ API int prism_piso_step(const PrismPISOControls* c, PrismTransport* const* mom, 
         auto v = momVec(mom, n_mom);
         std::vector<Report> r;
         const PrismSolveOpts opts = optsOrDefault(so);
-        if (opts.graph && stepGraphReady(v, *U->v, *p->s, opts, true))
+        if (opts.graph && !c->batched_momentum && stepGraphReady(v, *U->v, *p->s, opts, true))
             stepAsGraph(*p->s->m, [&] { pisoStep(*c, v, *U->v, *mdot->v, *p->s, opts, r); }, r);
         else
             pisoStep(*c, v, *U->v, *mdot->v, *p->s, opts, r);

@@ -586,6 +586,7 @@ void simpleDefaults(PrismSIMPLEControls* c) {  // SIMPLEControls, SIMPLE.h:14-43
     c->pressure_residual = 1e-7;
     c->p_ref_cell = -1;
     c->p_ref_value = 0.0;
+    c->batched_momentum = 0;
 }
 void pisoDefaults(PrismPISOControls* c) {  // PISOControls, PISO.h:11-49
     c->outer_iterations = 1;
@@ -601,6 +602,7 @@ void pisoDefaults(PrismPISOControls* c) {  // PISOControls, PISO.h:11-49
     c->pressure_residual = 1e-4;
     c->p_ref_cell = -1;
     c->p_ref_value = 0.0;
+    c->batched_momentum = 0;
 }
 
 namespace {
@@ -641,9 +643,22 @@ void setURF(Transport& eq, double f) {  // transport.cpp:38-52: out-of-range val
     eq.urf = f;
 }
 
-// solveImplicitMomentum, SIMPLE.cpp:19-41
+// solveImplicitMomentum, SIMPLE.cpp:19-41. With batched_momentum every component
+// is assembled and relaxed as usual and the systems are then solved together in
+// one persistent launch (one step each, to the Krylov tolerance).
 void solveImplicitMomentum(const PrismSIMPLEControls& c, std::vector<Transport*>& mom, const PrismSolveOpts& so,
                            std::vector<Report>& rep) {
+    if (c.batched_momentum) {
+        for (auto* eq : mom) setURF(*eq, c.momentum_urf);
+        Mesh& m = *mom[0]->phi->m;
+        if (!m.mom_batch) m.mom_batch = std::make_unique<BatchHandle>();
+        PhaseTimer pt("momentum (batched)", m.stream);
+        auto res = solveBatch(*m.mom_batch, mom, inner(so, c.momentum_max_iter, c.momentum_residual, -1, 0.0, false));
+        for (size_t i = 0; i < mom.size(); ++i)
+            rep.push_back({mom[i]->phi->name, res[i].iterations, res[i].initial_residual, res[i].final_residual,
+                           res[i].converged != 0});
+        return;
+    }
     for (auto* eq : mom) {
         setURF(*eq, c.momentum_urf);
         PhaseTimer pt("momentum " + eq->phi->name, eq->phi->m->stream);
@@ -825,6 +840,7 @@ void pisoStep(const PrismPISOControls& pc, std::vector<Transport*>& mom, Vector&
     sc.pressure_residual = pc.pressure_residual;
     sc.p_ref_cell = pc.p_ref_cell;
     sc.p_ref_value = pc.p_ref_value;
+    sc.batched_momentum = pc.batched_momentum;
     for (int64_t i = 0; i < pc.outer_iterations; ++i) {
         for (int64_t j = 0; j < pc.momentum_implicit_steps; ++j) simpleStep(sc, mom, U, mdot, p, so, rep);
         for (int64_t j = 1; j < pc.pressure_correction_steps; ++j) primeStep(sc, mom, U, mdot, p, so, rep);

@@ -22,6 +22,7 @@ namespace pb {
 struct Scalar;
 struct Tensor;
 struct Transport;
+struct BatchHandle;
 
 struct Mesh {
     std::unique_ptr<HostMesh> h;
@@ -57,6 +58,7 @@ struct Mesh {
     DevBuf<SolveCtl> graph_ctl;
     SolveCtl* graph_host = nullptr;  // pinned copy of graph_ctl
     cudaGraphExec_t graph_exec = nullptr;
+    std::unique_ptr<BatchHandle> mom_batch;  // momentum predictors solved together (batched_momentum)
 
     ~Mesh();
     MeshView view() const;
