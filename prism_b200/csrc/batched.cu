@@ -758,7 +758,8 @@ std::vector<BatchOut> runBatch(const std::vector<BatchSystem>& sys, BatchPlan& p
         for (auto* b : {&pl.r64b, &pl.r064, &pl.p64, &pl.v64, &pl.s64, &pl.t64, &pl.d64}) ensure(*b, nrows);
     }
     InnerBufs<T> ib = innerBufs(pl, T{});
-    // the systems' buffers, for the gather and scatter kernels
+    // the systems' buffers, for the gather and scatter kernels (one grid row per system)
+    if (sys.size() > 65535) fail(PRISM_BAD_ARG, "batched solve: at most 65535 systems per call");
     std::vector<CopyEntry> tab(sys.size());
     for (size_t i = 0; i < sys.size(); ++i) {
         const BatchSystem& q = sys[i];
