@@ -15,8 +15,8 @@
 //     built by sorting the fine entries by (aggregate row, aggregate column)
 //     once, after which refreshing the values for a new matrix is one
 //     segmented sum per coarse entry in a fixed order;
-//   * cycle: V(1,1), damped Jacobi (omega = 0.67) smoothing, coarse correction
-//     scaled by 1.5 (unsmoothed aggregation under-corrects), dense inverse
+//   * cycle: V(1,1), damped Jacobi (omega = 0.85) smoothing, coarse correction
+//     scaled by 1.7 (unsmoothed aggregation under-corrects), dense inverse
 //     (single-block Gauss-Jordan with partial pivoting) on the coarsest level.
 // The hierarchy's structure is built once per matrix pattern and reused; every
 // solve refreshes the values from the current matrix.
@@ -26,6 +26,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <type_traits>
 
 #include "amg.h"
@@ -936,6 +937,9 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
             PB_CUDA(cudaFuncSetAttribute(gauss_jordan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          DENSE_MAX * DENSE_MAX * (int)sizeof(double)));
         }
+        // smoother weight and coarse-correction factor (PRISM_AMG_OMEGA / PRISM_AMG_SCALE override them)
+        if (const char* e = std::getenv("PRISM_AMG_OMEGA")) omega = std::atof(e);
+        if (const char* e = std::getenv("PRISM_AMG_SCALE")) scale = std::atof(e);
         built = true;
         generation = nextGeneration();
     } else if (levels[0]->vals != A.vals) {

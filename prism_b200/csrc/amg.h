@@ -50,7 +50,7 @@ struct Amg {
     bool has32 = false;
     uint64_t generation = 0;  // new process-wide value whenever a buffer of the hierarchy is (re)allocated
     int tail = -1;            // first level of the fused coarse tail (-1: every level launches its own kernels)
-    double omega = 0.67, scale = 1.5;
+    double omega = 0.85, scale = 1.7;
 
     // Build the hierarchy (first call) or refresh its values (later calls) for
     // the matrix A, whose CSR pattern (device rowptr/col) lists each row's
