@@ -534,7 +534,10 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
     const double itol = o.inner_tol > 0 ? o.inner_tol : 0.1;
     Amg* amg = nullptr;
     if (o.method != PRISM_SOLVER_JACOBI && choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
-        if (!eq.amg) eq.amg = std::make_shared<Amg>();
+        if (!eq.amg) {
+            eq.amg = std::make_shared<Amg>();
+            if (!eq.has_conv) eq.amg->forDiffusion();
+        }
         amg = eq.amg.get();
     }
     PrismSolveResult r{};
@@ -754,7 +757,10 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
     pEqn.urf = 1.0;
     pEqn.ensure();
     zeroOutCoeffs(pEqn);
-    if (!m.p_amg) m.p_amg = std::make_shared<Amg>();
+    if (!m.p_amg) {
+        m.p_amg = std::make_shared<Amg>();
+        m.p_amg->forDiffusion();
+    }
     pEqn.amg = m.p_amg;
     for (int64_t i = 0; i <= c.non_ortho_correctors; ++i) {
         PhaseTimer pt("pressure corrector " + std::to_string(i), m.stream);
@@ -934,7 +940,10 @@ FixedPointOut adjointBackward(Transport& eq, const double* dJ, double* gk, doubl
 
     Amg* amg = nullptr;
     if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
-        if (!eq.amg_adj) eq.amg_adj = std::make_shared<Amg>();
+        if (!eq.amg_adj) {
+            eq.amg_adj = std::make_shared<Amg>();
+            eq.amg_adj->forDiffusion();
+        }
         amg = eq.amg_adj.get();
     }
     const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
@@ -1127,7 +1136,10 @@ PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o) {
     const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
     Amg* amg = nullptr;
     if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
-        if (!eq.amg) eq.amg = std::make_shared<Amg>();
+        if (!eq.amg) {
+            eq.amg = std::make_shared<Amg>();
+            if (!eq.has_conv) eq.amg->forDiffusion();
+        }
         amg = eq.amg.get();
     }
     const long long n_iter = std::max<long long>(o.n_iter, 0);
