@@ -16,7 +16,7 @@
 //     once, after which refreshing the values for a new matrix is one
 //     segmented sum per coarse entry in a fixed order;
 //   * cycle: V(1,1), damped Jacobi (omega = 0.9) smoothing, coarse correction
-//     scaled by 1.8, or 2.0 without convection (unsmoothed aggregation
+//     scaled by 1.8, or 2.0 for the pressure correction (unsmoothed aggregation
 //     under-corrects), dense inverse
 //     (single-block Gauss-Jordan with partial pivoting) on the coarsest level.
 // The hierarchy's structure is built once per matrix pattern and reused; every

@@ -50,11 +50,11 @@ struct Amg {
     bool has32 = false;
     uint64_t generation = 0;  // new process-wide value whenever a buffer of the hierarchy is (re)allocated
     int tail = -1;            // first level of the fused coarse tail (-1: every level launches its own kernels)
-    // V-cycle smoother weight and coarse-correction factor: forDiffusion() for
-    // equations without convection (pressure correction, Poisson), where a
-    // larger over-correction pays; PRISM_AMG_OMEGA / PRISM_AMG_SCALE override both
+    // V-cycle smoother weight and coarse-correction factor; the pressure-correction
+    // equation of SIMPLE/PRIME/PISO gains from a larger over-correction
+    // (forPressure). PRISM_AMG_OMEGA / PRISM_AMG_SCALE override both.
     double omega = 0.9, scale = 1.8;
-    void forDiffusion() { scale = 2.0; }
+    void forPressure() { scale = 2.0; }
 
     // Build the hierarchy (first call) or refresh its values (later calls) for
     // the matrix A, whose CSR pattern (device rowptr/col) lists each row's

@@ -534,10 +534,7 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
     const double itol = o.inner_tol > 0 ? o.inner_tol : 0.1;
     Amg* amg = nullptr;
     if (o.method != PRISM_SOLVER_JACOBI && choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
-        if (!eq.amg) {
-            eq.amg = std::make_shared<Amg>();
-            if (!eq.has_conv) eq.amg->forDiffusion();
-        }
+        if (!eq.amg) eq.amg = std::make_shared<Amg>();
         amg = eq.amg.get();
     }
     PrismSolveResult r{};
@@ -759,7 +756,7 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
     zeroOutCoeffs(pEqn);
     if (!m.p_amg) {
         m.p_amg = std::make_shared<Amg>();
-        m.p_amg->forDiffusion();
+        m.p_amg->forPressure();
     }
     pEqn.amg = m.p_amg;
     for (int64_t i = 0; i <= c.non_ortho_correctors; ++i) {
@@ -940,10 +937,7 @@ FixedPointOut adjointBackward(Transport& eq, const double* dJ, double* gk, doubl
 
     Amg* amg = nullptr;
     if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
-        if (!eq.amg_adj) {
-            eq.amg_adj = std::make_shared<Amg>();
-            eq.amg_adj->forDiffusion();
-        }
+        if (!eq.amg_adj) eq.amg_adj = std::make_shared<Amg>();
         amg = eq.amg_adj.get();
     }
     const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
@@ -1136,10 +1130,7 @@ PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o) {
     const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
     Amg* amg = nullptr;
     if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
-        if (!eq.amg) {
-            eq.amg = std::make_shared<Amg>();
-            if (!eq.has_conv) eq.amg->forDiffusion();
-        }
+        if (!eq.amg) eq.amg = std::make_shared<Amg>();
         amg = eq.amg.get();
     }
     const long long n_iter = std::max<long long>(o.n_iter, 0);
