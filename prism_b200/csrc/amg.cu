@@ -726,7 +726,7 @@ int matchPairs(const AmgLevel& L, int* agg, cudaStream_t s) {
 
 // Galerkin structure of P^T A P for the aggregate map `agg` (nc aggregates):
 // fills the restriction data of L and creates the coarse level C (pattern + SELL).
-void galerkinStructure(AmgLevel& L, const int* agg, int nc, AmgLevel& C, cudaStream_t s) {
+void galerkinStructure(DevArena& ar, AmgLevel& L, const int* agg, int nc, AmgLevel& C, cudaStream_t s) {
     const int n = L.n;
     const int64_t m = L.nnz;
     TmpBuf<long long> keys(m, s), keys_s(m, s);
@@ -748,12 +748,12 @@ void galerkinStructure(AmgLevel& L, const int* agg, int nc, AmgLevel& C, cudaStr
     PB_CUDA(cudaMemcpyAsync(&nnz_c, mid.p + m, sizeof(int), cudaMemcpyDeviceToHost, s));
     PB_CUDA(cudaStreamSynchronize(s));
     // restriction data + coarse CSR
-    L.gal_seg.alloc(nnz_c + 1);
-    L.gal_src.alloc(m);
+    L.gal_seg.alloc(ar, nnz_c + 1, s);
+    L.gal_src.alloc(ar, m, s);
     C.n = nc;
     C.nnz = nnz_c;
-    C.o_rowptr.alloc(nc + 1);
-    C.o_col.alloc(nnz_c);
+    C.o_rowptr.alloc(ar, nc + 1, s);
+    C.o_col.alloc(ar, nnz_c, s);
     coarse_csr_kernel<<<grid(m), BS, 0, s>>>(m, keys_s.p, head.p, mid.p, idx_s.p, L.csr_pos, nc, L.gal_seg.p,
                                              C.o_col.p, C.o_rowptr.p, L.gal_src.p); countLaunch();
     int hm = (int)m;
@@ -764,7 +764,7 @@ void galerkinStructure(AmgLevel& L, const int* agg, int nc, AmgLevel& C, cudaStr
     TmpBuf<int> se(C.nslices + 1, s);
     PB_CUDA(cudaMemsetAsync(se.p + C.nslices, 0, sizeof(int), s));
     rowlen_slice_kernel<<<grid(C.nslices), BS, 0, s>>>(nc, C.nslices, C.o_rowptr.p, se.p); countLaunch();
-    C.o_sl_off.alloc(C.nslices + 1);
+    C.o_sl_off.alloc(ar, C.nslices + 1, s);
     size_t tb3 = 0;
     PB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb3, se.p, C.o_sl_off.p, C.nslices + 1, s));
     TmpBuf<unsigned char> tmp3(std::max<size_t>(tb3, 1), s);
@@ -773,9 +773,9 @@ void galerkinStructure(AmgLevel& L, const int* agg, int nc, AmgLevel& C, cudaStr
     PB_CUDA(cudaMemcpyAsync(&sell, C.o_sl_off.p + C.nslices, sizeof(int), cudaMemcpyDeviceToHost, s));
     PB_CUDA(cudaStreamSynchronize(s));
     C.sell_nnz = sell;
-    C.o_sl_col.alloc(std::max(sell, 1));
-    C.o_csr_pos.alloc(std::max(nnz_c, 1));
-    C.o_diag_pos.alloc(nc);
+    C.o_sl_col.alloc(ar, std::max(sell, 1), s);
+    C.o_csr_pos.alloc(ar, std::max(nnz_c, 1), s);
+    C.o_diag_pos.alloc(ar, nc, s);
     sell_fill_kernel<<<grid((int64_t)C.nslices * 32), BS, 0, s>>>(nc, C.nslices, C.o_rowptr.p, C.o_col.p,
                                                                    C.o_sl_off.p, C.o_sl_col.p, C.o_csr_pos.p,
                                                                    C.o_diag_pos.p); countLaunch();
@@ -785,7 +785,7 @@ void galerkinStructure(AmgLevel& L, const int* agg, int nc, AmgLevel& C, cudaStr
     C.sl_off = C.o_sl_off.p;
     C.sl_col = C.o_sl_col.p;
     C.diag_pos = C.o_diag_pos.p;
-    C.o_vals.alloc(std::max(sell, 1));
+    C.o_vals.alloc(ar, std::max(sell, 1), s);
     C.o_vals.zero(s);
     C.vals = C.o_vals.p;
     PB_LAUNCH("amg galerkin structure");
@@ -797,18 +797,18 @@ void galerkinValues(const AmgLevel& L, AmgLevel& C, cudaStream_t s) {
 }
 
 // aggregate -> member rows (rows sorted by aggregate, stable)
-void members(AmgLevel& L, int nc, cudaStream_t s) {
+void members(DevArena& ar, AmgLevel& L, int nc, cudaStream_t s) {
     const int n = L.n;
     TmpBuf<int> rows(n, s), agg_s(n, s);
     iota_kernel<<<grid(n), BS, 0, s>>>(n, rows.p); countLaunch();
-    L.m_idx.alloc(n);
+    L.m_idx.alloc(ar, n, s);
     int end_bit = 1;
     while (end_bit < 31 && (1 << end_bit) < nc) ++end_bit;
     size_t tb = 0;
     PB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, L.agg.p, agg_s.p, rows.p, L.m_idx.p, n, 0, end_bit, s));
     TmpBuf<unsigned char> tmp(std::max<size_t>(tb, 1), s);
     PB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, L.agg.p, agg_s.p, rows.p, L.m_idx.p, n, 0, end_bit, s));
-    L.m_off.alloc(nc + 1);
+    L.m_off.alloc(ar, nc + 1, s);
     member_heads_kernel<<<grid(n), BS, 0, s>>>(n, agg_s.p, L.m_off.p); countLaunch();
     PB_CUDA(cudaMemcpyAsync(L.m_off.p + nc, &n, sizeof(int), cudaMemcpyHostToDevice, s));
     PB_CUDA(cudaStreamSynchronize(s));
@@ -816,24 +816,24 @@ void members(AmgLevel& L, int nc, cudaStream_t s) {
 }
 
 // returns true if a buffer was allocated
-bool allocCycle(AmgLevel& L, bool mixed, cudaStream_t s) {
+bool allocCycle(DevArena& ar, AmgLevel& L, bool mixed, cudaStream_t s) {
     bool fresh = false;
     int np = L.nslices * 32;
     for (auto* b : {&L.b, &L.x, &L.x2, &L.res, &L.dinv})
         if (!b->p) {
-            b->alloc(np);
+            b->alloc(ar, np, s);
             b->zero(s);
             fresh = true;
         }
     if (mixed) {
         for (auto* b : {&L.b32, &L.x32, &L.x232, &L.res32, &L.dinv32})
             if (!b->p) {
-                b->alloc(np);
+                b->alloc(ar, np, s);
                 b->zero(s);
                 fresh = true;
             }
         if (!L.vals32.p) {
-            L.vals32.alloc(std::max<int64_t>(L.sell_nnz, 1));
+            L.vals32.alloc(ar, std::max<int64_t>(L.sell_nnz, 1), s);
             L.vals32.zero(s);
             fresh = true;
         }
@@ -859,6 +859,7 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
         coarse_inv.release();
         coarse_inv32.release();
         coarse_bad.release();
+        arena.reset();  // stream order keeps earlier work on the old hierarchy ahead of its reuse
         auto L0 = std::make_unique<AmgLevel>();
         L0->n = A.n;
         L0->nslices = A.nslices;
@@ -866,7 +867,7 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
         L0->sell_nnz = A.nnz_padded;
         L0->rowptr = rowptr;
         L0->col = col;
-        L0->o_csr_pos.alloc(std::max<int64_t>(A.nnz_csr, 1));
+        L0->o_csr_pos.alloc(arena, std::max<int64_t>(A.nnz_csr, 1), s);
         csr_pos_kernel<<<grid(A.n), BS, 0, s>>>(A.n, rowptr, A.sl_off, L0->o_csr_pos.p); countLaunch();
         L0->csr_pos = L0->o_csr_pos.p;
         L0->sl_off = A.sl_off;
@@ -892,25 +893,29 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
             TmpBuf<int> agg1(L.n, s);
             int n1 = timed(t_match, [&] { return matchPairs(L, agg1.p, s); });
             if (n1 > (int)(0.9 * L.n)) break;
+            L.agg.alloc(arena, L.n, s);
+            // the pass-1 operator T and the pass-1 restriction data of L are
+            // intermediates: their arena space is given back once L.agg is composed
+            const DevArena::Mark pass1 = arena.mark();
             AmgLevel T;
             timed(t_gal, [&] {
-                galerkinStructure(L, agg1.p, n1, T, s);
+                galerkinStructure(arena, L, agg1.p, n1, T, s);
                 galerkinValues(L, T, s);
                 return 0;
             });
             // pass 2 on the pass-1 operator
             TmpBuf<int> agg2(n1, s);
             int n2 = timed(t_match, [&] { return matchPairs(T, agg2.p, s); });
-            L.agg.alloc(L.n);
             compose_kernel<<<grid(L.n), BS, 0, s>>>(L.n, agg1.p, agg2.p, L.agg.p); countLaunch();
+            arena.rewind(pass1);
             auto C = std::make_unique<AmgLevel>();
             timed(t_gal, [&] {
-                galerkinStructure(L, L.agg.p, n2, *C, s);
+                galerkinStructure(arena, L, L.agg.p, n2, *C, s);
                 galerkinValues(L, *C, s);
                 return 0;
             });
             timed(t_mem, [&] {
-                members(L, n2, s);
+                members(arena, L, n2, s);
                 return 0;
             });
             levels.push_back(std::move(C));
@@ -930,11 +935,10 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
                          "galerkin %.1f ms, members %.1f ms\n",
                          coarse_n <= DENSE_MAX ? "dense" : "Jacobi", tail, t_match, t_gal, t_mem);
         }
-        trimScratch(s);
         if (coarse_n <= DENSE_MAX) {
-            coarse_a.alloc((size_t)coarse_n * coarse_n);
-            coarse_inv.alloc((size_t)coarse_n * coarse_n);
-            coarse_bad.alloc(1);
+            coarse_a.alloc(arena, (size_t)coarse_n * coarse_n, s);
+            coarse_inv.alloc(arena, (size_t)coarse_n * coarse_n, s);
+            coarse_bad.alloc(arena, 1, s);
             PB_CUDA(cudaFuncSetAttribute(gauss_jordan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          DENSE_MAX * DENSE_MAX * (int)sizeof(double)));
         }
@@ -948,9 +952,9 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
         generation = nextGeneration();
     }
     for (auto& L : levels)
-        if (allocCycle(*L, mixed, s)) generation = nextGeneration();
+        if (allocCycle(arena, *L, mixed, s)) generation = nextGeneration();
     if (mixed && coarse_inv.p && !coarse_inv32.p) {
-        coarse_inv32.alloc(coarse_inv.n);
+        coarse_inv32.alloc(arena, coarse_inv.n, s);
         generation = nextGeneration();
     }
     has32 = mixed;

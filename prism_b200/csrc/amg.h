@@ -11,7 +11,8 @@ namespace pb {
 
 // One level of the hierarchy. Level 0 borrows the equation's matrix (pattern of
 // the mesh, values of the equation); coarser levels own theirs. Matrices are
-// kept both as CSR (setup) and SELL-32 (cycle kernels).
+// kept both as CSR (setup) and SELL-32 (cycle kernels). Every buffer lives in
+// the hierarchy's arena (Amg::arena).
 struct AmgLevel {
     int n = 0, nslices = 0;
     int lpr = 1;  // lanes per row of the cycle kernels
@@ -23,29 +24,30 @@ struct AmgLevel {
     const int* sl_off = nullptr;
     const int* sl_col = nullptr;
     const int* diag_pos = nullptr;
-    DevBuf<int> o_rowptr, o_col, o_csr_pos, o_sl_off, o_sl_col, o_diag_pos;
+    ArenaBuf<int> o_rowptr, o_col, o_csr_pos, o_sl_off, o_sl_col, o_diag_pos;
     // values (SELL layout): level 0 borrows vals64; FP32 copy for mixed precision
     const double* vals = nullptr;
-    DevBuf<double> o_vals;
-    DevBuf<float> vals32;
-    DevBuf<double> dinv;
-    DevBuf<float> dinv32;
+    ArenaBuf<double> o_vals;
+    ArenaBuf<float> vals32;
+    ArenaBuf<double> dinv;
+    ArenaBuf<float> dinv32;
     // restriction to the next level
-    DevBuf<int> agg;            // fine row -> aggregate
-    DevBuf<int> m_off, m_idx;   // aggregate -> member rows
-    DevBuf<int> gal_seg;        // coarse CSR entry m sums sorted fine entries [gal_seg[m], gal_seg[m+1])
-    DevBuf<int> gal_src;        // SELL position (this level) of each sorted fine entry
+    ArenaBuf<int> agg;            // fine row -> aggregate
+    ArenaBuf<int> m_off, m_idx;   // aggregate -> member rows
+    ArenaBuf<int> gal_seg;        // coarse CSR entry m sums sorted fine entries [gal_seg[m], gal_seg[m+1])
+    ArenaBuf<int> gal_src;        // SELL position (this level) of each sorted fine entry
     // cycle vectors (FP64 and FP32)
-    DevBuf<double> b, x, x2, res;
-    DevBuf<float> b32, x32, x232, res32;
+    ArenaBuf<double> b, x, x2, res;
+    ArenaBuf<float> b32, x32, x232, res32;
 };
 
 struct Amg {
+    DevArena arena;  // memory of every level (declared first: released last)
     std::vector<std::unique_ptr<AmgLevel>> levels;
     int coarse_n = 0;
-    DevBuf<double> coarse_a, coarse_inv;
-    DevBuf<float> coarse_inv32;
-    DevBuf<int> coarse_bad;
+    ArenaBuf<double> coarse_a, coarse_inv;
+    ArenaBuf<float> coarse_inv32;
+    ArenaBuf<int> coarse_bad;
     bool built = false;
     bool has32 = false;
     uint64_t generation = 0;  // new process-wide value whenever a buffer of the hierarchy is (re)allocated

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
@@ -78,9 +79,28 @@ struct DevBuf {
     explicit operator bool() const { return p != nullptr; }
 };
 
-// Library-owned stream-ordered memory pool of the current device, for
-// temporaries of setup phases: freed blocks are reused by later temporaries
-// without a device synchronisation; trimScratch() returns them to the device.
+// Non-owning slice of a device allocation (several arrays carved from one
+// allocation, which costs one cudaMalloc instead of one per array).
+template <typename T>
+struct DevSlice {
+    T* p = nullptr;
+    size_t n = 0;
+    void zero(cudaStream_t s) {
+        if (n) PB_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    }
+    void download(T* h, size_t count, cudaStream_t s) const {
+        if (count > n) fail(PRISM_INTERNAL, "download beyond allocation");
+        if (count) PB_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+    }
+    explicit operator bool() const { return p != nullptr; }
+};
+
+// Library-owned stream-ordered memory pool of the current device, for the
+// temporaries and hierarchies of setup phases. A cudaMalloc / cudaFree pair
+// costs milliseconds here, so blocks freed to the pool stay reserved (up to
+// SCRATCH_KEEP bytes) and are handed to later allocations without a call into
+// the driver.
+constexpr uint64_t SCRATCH_KEEP = uint64_t(2) << 30;
 inline cudaMemPool_t scratchPool() {
     static cudaMemPool_t pools[64] = {};
     int dev = 0;
@@ -92,14 +112,10 @@ inline cudaMemPool_t scratchPool() {
         props.location.type = cudaMemLocationTypeDevice;
         props.location.id = dev;
         PB_CUDA(cudaMemPoolCreate(&pools[dev], &props));
-        uint64_t keep = ~0ull;
+        uint64_t keep = SCRATCH_KEEP;
         PB_CUDA(cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep));
     }
     return pools[dev];
-}
-inline void trimScratch(cudaStream_t s) {
-    PB_CUDA(cudaStreamSynchronize(s));
-    PB_CUDA(cudaMemPoolTrimTo(scratchPool(), 0));
 }
 
 // Temporary device buffer in stream order on stream s (scratchPool()).
@@ -117,6 +133,84 @@ struct TmpBuf {
     ~TmpBuf() {
         if (p) cudaFreeAsync(p, s);
     }
+};
+
+// Device memory handed out in bump order from a few large chunks of
+// scratchPool() and returned all at once, for objects made of many buffers
+// (the AMG hierarchy): one pool call per chunk instead of one cudaMalloc per
+// buffer. Chunks grow geometrically (at least MIN_CHUNK, at least the total so
+// far). mark()/rewind() give back everything taken after the mark, for
+// intermediates of a build; reset() gives back everything. Chunks are
+// allocated in order on the stream of the call, so work on that stream may use
+// them at once; the destructor waits for the device before freeing them.
+class DevArena {
+public:
+    struct Mark {
+        size_t chunk = 0, off = 0;
+    };
+    DevArena() = default;
+    DevArena(const DevArena&) = delete;
+    DevArena& operator=(const DevArena&) = delete;
+    ~DevArena() {
+        if (chunks_.empty()) return;
+        cudaDeviceSynchronize();
+        for (auto& c : chunks_) cudaFree(c.p);
+    }
+    template <typename T>
+    T* take(size_t count, cudaStream_t s) {
+        if (!count) return nullptr;
+        const size_t bytes = (count * sizeof(T) + ALIGN - 1) & ~(ALIGN - 1);
+        for (; cur_ < chunks_.size(); ++cur_, off_ = 0)
+            if (off_ + bytes <= chunks_[cur_].size) {
+                char* p = chunks_[cur_].p + off_;
+                off_ += bytes;
+                return reinterpret_cast<T*>(p);
+            }
+        size_t size = std::max(std::max(bytes, MIN_CHUNK), total_);
+        char* p = nullptr;
+        PB_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), size, scratchPool(), s));
+        chunks_.push_back({p, size});
+        total_ += size;
+        cur_ = chunks_.size() - 1;
+        off_ = bytes;
+        return reinterpret_cast<T*>(p);
+    }
+    Mark mark() const { return {cur_, off_}; }
+    void rewind(const Mark& m) {
+        cur_ = m.chunk;
+        off_ = m.off;
+    }
+    void reset() { rewind(Mark{}); }
+
+private:
+    struct Chunk {
+        char* p;
+        size_t size;
+    };
+    static constexpr size_t ALIGN = 256;
+    static constexpr size_t MIN_CHUNK = size_t(64) << 20;
+    std::vector<Chunk> chunks_;
+    size_t cur_ = 0, off_ = 0, total_ = 0;
+};
+
+// A buffer inside a DevArena: the arena owns the memory, so release() only
+// forgets it.
+template <typename T>
+struct ArenaBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(DevArena& a, size_t count, cudaStream_t s) {
+        p = a.take<T>(count, s);
+        n = count;
+    }
+    void release() {
+        p = nullptr;
+        n = 0;
+    }
+    void zero(cudaStream_t s) {
+        if (n) PB_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+    }
+    explicit operator bool() const { return p != nullptr; }
 };
 
 // Number of kernels this library has launched (read by the profiling window).

@@ -351,14 +351,15 @@ void updatePrevTimeSteps(Scalar& s) {
 void Transport::ensure() {
     Mesh& m = *phi->m;
     if (!A) {
-        A.alloc(m.pat.sell_nnz);
-        b.alloc(m.n_pad);
-        bconv.alloc(m.n_pad);
-        bdiff.alloc(m.n_pad);
-        A.zero(m.stream);
-        b.zero(m.stream);
-        bconv.zero(m.stream);
-        bdiff.zero(m.stream);
+        // each array starts on a 256-byte boundary
+        auto up = [](size_t k) { return (k + 31) / 32 * 32; };
+        const size_t na = up(m.pat.sell_nnz), nv = up(m.n_pad);
+        store.alloc(na + 3 * nv);
+        store.zero(m.stream);
+        A = {store.p, (size_t)m.pat.sell_nnz};
+        b = {store.p + na, (size_t)m.n_pad};
+        bconv = {store.p + na + nv, (size_t)m.n_pad};
+        bdiff = {store.p + na + 2 * nv, (size_t)m.n_pad};
     }
 }
 

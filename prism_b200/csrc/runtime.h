@@ -133,7 +133,8 @@ struct Transport {
     bool symmetry = false;
     double urf = 1.0;
     bool clean = true;
-    DevBuf<double> A, b, bconv, bdiff;
+    DevBuf<double> store;  // A, b, bconv and bdiff in one allocation
+    DevSlice<double> A, b, bconv, bdiff;
     std::shared_ptr<Amg> amg;  // AMG hierarchy (PRISM_PC_AMG), built on the first solve
     // adjoint: A^T values and the AMG hierarchy of A^T
     DevBuf<double> AT;
