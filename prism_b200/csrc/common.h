@@ -188,7 +188,7 @@ private:
         size_t size;
     };
     static constexpr size_t ALIGN = 256;
-    static constexpr size_t MIN_CHUNK = size_t(64) << 20;
+    static constexpr size_t MIN_CHUNK = size_t(2) << 20;
     std::vector<Chunk> chunks_;
     size_t cur_ = 0, off_ = 0, total_ = 0;
 };
