@@ -53,9 +53,24 @@ def test_needs_pressure_reference_pin(orc, name, expected):
     assert api.needs_pressure_reference(p) == expected
 
 
+def test_simple_duct_symmetry_pin(orc):
+    # tests/test_simple_duct_symmetry.cpp:38-53: duct with a symmetry plane against OpenFOAM
+    unv, case, extra = cases.load_golden("duct_simple")
+    r = cases.run_reference_test("duct_simple", orc)
+    assert cases.rel_l2(r["p"], extra["foam_p"]) < 0.025
+    assert cases.rel_l2(r["U"][0], extra["foam_U"][:, 0]) < 0.07
+    assert cases.rel_l2(r["U"][1], extra["foam_U"][:, 1]) < 0.007
+    assert not r["needs_ref"]
+    # the stored oracle result (compared with the GPU path on the B200) is this run, bit for bit
+    ref = cases.load_oracle_results("duct_simple")
+    for k in ref:
+        np.testing.assert_array_equal(r[k], ref[k], err_msg=f"duct_simple:{k}")
+
+
 def test_golden_files_match_oracle(orc):
     # the stored oracle results are reproduced bit for bit by the current oracle
-    for name in ("poisson_hex", "versteeg_advection_1d", "cavity_hex"):
+    for name in ("poisson_hex", "poisson_wedge", "versteeg_advection_1d", "versteeg_trans_1d", "cavity_hex",
+                 "coarse_pipe"):
         ref = cases.load_oracle_results(name)
         got = cases.run_reference_test(name, orc)
         for k in ref:
