@@ -212,8 +212,23 @@ std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d) {
     auto mesh = std::make_unique<Mesh>();
     mesh->h = buildHostMesh(d);
     const HostMesh& h = *mesh->h;
-    if (h.nc >= (int64_t(1) << 31) || h.nf >= (int64_t(1) << 31) || (int64_t)h.cf_face.size() >= (int64_t(1) << 31))
+    constexpr int64_t LIMIT = int64_t(1) << 31;
+    if (h.nc >= LIMIT || h.nf >= LIMIT || (int64_t)h.cf_face.size() >= LIMIT)
         fail(PRISM_INVALID_MESH, "mesh too large for 32-bit indices");
+    // the CSR and SELL-32 patterns number their entries with 32-bit ints: bound both
+    // (a row holds the cell and at most one entry per interior face of the cell)
+    int64_t nnz = 0, sell = 0;
+    for (int64_t s0 = 0; s0 < h.nc; s0 += 32) {
+        int64_t width = 0;
+        for (int64_t c = s0; c < std::min(s0 + 32, h.nc); ++c) {
+            int64_t len = 1;
+            for (int64_t k = h.cf_off[c]; k < h.cf_off[c + 1]; ++k) len += h.cf_face[k] >= h.nb;
+            nnz += len;
+            width = std::max(width, len);
+        }
+        sell += 32 * width;
+    }
+    if (nnz >= LIMIT || sell >= LIMIT) fail(PRISM_INVALID_MESH, "matrix pattern too large for 32-bit indices");
     PB_CUDA(cudaStreamCreateWithFlags(&mesh->stream, cudaStreamNonBlocking));
     setupDevice(*mesh);
     return mesh;

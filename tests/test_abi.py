@@ -43,3 +43,23 @@ def test_status_strings(orc):
     orc.lib.orc_status_string.restype = ctypes.c_char_p
     assert orc.lib.orc_status_string(0) == b"OK"
     assert orc.lib.orc_status_string(7) == b"NO_BC_HANDLER"
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+def test_mesh_host_build_and_index_checks(kind):
+    # prism_mesh_create builds the PMesh on the host and checks that every index
+    # (cells, faces, CSR and SELL-32 entries) fits 32 bits before it touches the
+    # device: without a GPU the call gets exactly as far as creating the mesh's stream
+    import prism_b200
+    import torch
+    from prism_b200 import api, io, meshgen
+    if not os.path.exists(prism_b200.LIB_PATH):
+        pytest.skip("library not built")
+    unv = meshgen.box_hex(6, 5, 4, jitter=0.2, seed=1) if kind == "hex" else meshgen.box_tet(4, 3, 3)
+    case = io.Case.from_dict(meshgen.PATCHES, {"T": {p: ("fixed", 0.0) for p in meshgen.PATCHES}}, {"T": {}})
+    if torch.cuda.is_available():
+        assert api.Mesh(unv, case, lib=prism_b200.lib()).n_cells > 0
+        return
+    with pytest.raises(_abi.PrismError) as err:
+        api.Mesh(unv, case, lib=prism_b200.lib())
+    assert err.value.status == _abi.CUDA_ERROR and "cudaStreamCreate" in str(err.value)
