@@ -37,7 +37,6 @@ namespace pb {
 namespace {
 
 constexpr int BS = 256;
-constexpr int WARPS = BS / 32;
 constexpr int COARSE_MAX = 128;   // stop coarsening at this many rows
 constexpr int DENSE_MAX = 160;    // dense inverse of the coarsest level up to this many rows (fits shared memory)
 constexpr int MAX_LEVELS = 20;
@@ -275,7 +274,6 @@ __global__ void __launch_bounds__(1024) gauss_jordan_kernel(int n, const double*
     extern __shared__ double a[];
     __shared__ double fac[DENSE_MAX];
     __shared__ int perm[DENSE_MAX];
-    __shared__ double red_v[32];
     __shared__ int red_i[32];
     __shared__ double amax;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -308,7 +306,6 @@ __global__ void __launch_bounds__(1024) gauss_jordan_kernel(int n, const double*
                 }
             }
             if (lane == 0) {
-                red_v[0] = bv;
                 red_i[0] = bi;
                 perm[k] = bi;
             }
@@ -495,24 +492,6 @@ __global__ void coarse_solve_kernel(int n, const T* __restrict__ inv, const T* _
 }
 
 // coarsest level too large for a dense inverse: a few damped Jacobi sweeps
-template <typename T>
-__global__ void __launch_bounds__(BS) jacobi_sweep_kernel(int nslices, int n, const int* __restrict__ sl_off,
-                                                          const int* __restrict__ col, const T* __restrict__ val,
-                                                          const T* __restrict__ b, const T* __restrict__ x,
-                                                          const T* __restrict__ dinv, T omega, T* __restrict__ out,
-                                                          const KState* S) {
-    pdlEnter();
-    if (S && S->done) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
-        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
-        const int r = sl * 32 + lane;
-        T sum = 0;
-        for (int j = 0; j < width; ++j) sum += val[bo + 32 * j + lane] * x[col[bo + 32 * j + lane]];
-        if (r < n) out[r] = x[r] + omega * dinv[r] * (b[r] - sum);
-    }
-}
-
 // ---------------------------------------------------------------- fused coarse tail
 // The levels from the first one with at most tailMaxRows() rows down to the
 // coarsest run in one launch of a thread-block cluster: the pre-smoothing and
