@@ -11,6 +11,10 @@ that uses the case (tests/test_poisson.cpp, test_advection_1d.cpp,
 test_simple_coarse_pipe.cpp, test_needs_pressure_ref.cpp, test_transient_1d.cpp). The GPU tests
 compare the sm_100a path with these arrays; the CPU tests re-run the oracle and
 check it against the reference tests' own thresholds.
+
+The case name "boundary" bundles the fields.json / <field>.json files of the
+reference's boundary-file tests (tests/test_boundary.cpp, cases/boundary/*)
+into boundary_cases.json: {case: {file name: file text}}.
 """
 import json
 import os
@@ -36,8 +40,24 @@ CASES = {
 }
 
 
+def boundary_files(src, out_dir):
+    base = os.path.join(src, "boundary")
+    bundle = {}
+    for case in sorted(os.listdir(base)):
+        d = os.path.join(base, case)
+        bundle[case] = {}
+        for f in sorted(os.listdir(d)):
+            with open(os.path.join(d, f)) as fh:
+                bundle[case][f] = fh.read()
+    with open(os.path.join(out_dir, "boundary_cases.json"), "w") as fh:
+        json.dump(bundle, fh, indent=1, sort_keys=True)
+    print("boundary", {c: sorted(v) for c, v in bundle.items()})
+
+
 def main(src, only=None):
     out_dir = os.path.dirname(os.path.abspath(__file__))
+    if not only or "boundary" in only:
+        boundary_files(src, out_dir)
     for name, (case_dir, mesh_file) in CASES.items():
         if only and name not in only:
             continue
