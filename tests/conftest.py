@@ -22,3 +22,18 @@ def orc():
 def gpu():
     import prism_b200
     return prism_b200.lib()
+
+
+@pytest.fixture(scope="session")
+def ref():
+    """The reference's own code compiled here (oracle/_ref/libprism_ref.so), built on first use
+    when the reference tree is present; tests that need it are skipped where it is absent."""
+    from oracle import ref_build, ref_lib
+    if not ref_lib.available():
+        try:
+            ref_build.build()
+        except RuntimeError as e:
+            pytest.skip(f"reference build failed: {e}")
+    if not ref_lib.available():
+        pytest.skip("oracle/_ref/libprism_ref.so is not built and the reference tree is absent")
+    return ref_lib

@@ -1,8 +1,9 @@
 """Generate tests/golden/*.npz from the reference's own test cases.
 
-Run in a container where the reference checkout is available:
+Run in a container where the reference checkout is available, giving the path of its
+tests/cases directory:
 
-    python tests/golden/make_golden.py /root/reference/tests/cases [case names]
+    python tests/golden/make_golden.py <reference>/tests/cases [case names]
 
 For each case it stores the mesh in converter form (nodes, element list,
 groups; re-encoded from the case's mesh.unv), the parsed fields.json and
@@ -97,4 +98,6 @@ def main(src, only=None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests/cases", sys.argv[2:])
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference tests/cases directory> [case names]")
+    main(sys.argv[1], sys.argv[2:])
