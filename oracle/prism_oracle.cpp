@@ -1122,15 +1122,18 @@ double diagOf(const CSR& A, int64_t i) {
     return 0.0;
 }
 
-// residual(), numerics/solver.cpp:8-24
+// residual(), numerics/solver.cpp:8-24. Each maxCoeff() is a reduction seeded with the first
+// coefficient and folded with std::max, so a NaN in the first position propagates and a NaN
+// further on is dropped (Eigen's scalar max keeps its first argument when either is NaN).
 double scaledResidual(const CSR& A, const std::vector<double>& x, const std::vector<double>& b) {
     std::vector<double> Ax;
     spmv(A, x, Ax);
-    double denom = 0.0;
-    for (int64_t i = 0; i < A.n; ++i) denom = std::max(denom, std::abs(diagOf(A, i) * x[i]));
+    if (A.n == 0) return 0.0;
+    double denom = std::abs(diagOf(A, 0) * x[0]);
+    for (int64_t i = 1; i < A.n; ++i) denom = std::max(denom, std::abs(diagOf(A, i) * x[i]));
     denom += EPSILON;
-    double r = 0.0;
-    for (int64_t i = 0; i < A.n; ++i) r = std::max(r, std::abs(Ax[i] - b[i]) / denom);
+    double r = std::abs(Ax[0] - b[0]) / denom;
+    for (int64_t i = 1; i < A.n; ++i) r = std::max(r, std::abs(Ax[i] - b[i]) / denom);
     return r;
 }
 
