@@ -439,10 +439,9 @@ int prism_profile_stop(PrismProfile* out);
 
 /* ---- allocation-free Jacobi sweep ------------------------------------------ */
 /* For callers that cannot allocate device memory when they need a solver step
- * (work recorded into a CUDA graph, where allocating during stream capture is an
- * error; host applications that own a fixed device-memory budget; time loops
- * that must not synchronize on cudaMalloc/cudaFree). No counterpart in the
- * reference.
+ * (host applications that own a fixed device-memory budget and allocate nothing
+ * after start-up; time loops that must not synchronize on cudaMalloc/cudaFree).
+ * No counterpart in the reference.
  *
  * One Jacobi sweep x <- x + D^-1 (b - A x) on an n x n CSR matrix whose arrays
  * the caller already holds in device memory: rowptr (n+1) and col (nnz) int32,
@@ -459,7 +458,8 @@ int prism_profile_stop(PrismProfile* out);
  * whose work overlaps on the GPU (different streams, or different host threads)
  * race; serialize them. Every scratch entry a call reads is written earlier in
  * the same call, so nothing has to be cleared between calls. A row without a
- * diagonal entry yields NaN. */
+ * diagonal entry follows numerics/jacobi.cpp:5-9 (1/0 = inf, so x + inf (b - Ax)
+ * there); prism_solve_csr rejects such a matrix with PRISM_BAD_ARG instead. */
 #define PRISM_NOALLOC_MAX_ROWS 1048576
 int prism_jacobi_step_noalloc(int64_t n, const int32_t* rowptr, const int32_t* col, const double* values,
                               const double* b, double* x, void* stream);

@@ -2,12 +2,11 @@
 // call cudaMalloc.
 //
 // Some callers cannot allocate device memory at the point where they need a
-// solver step: code that records work into a CUDA graph (an allocation during
-// stream capture is an error), solvers embedded in a host application that owns
-// a fixed device-memory budget and forbids allocation after start-up, or a
-// time-stepping loop where a cudaMalloc/cudaFree pair would synchronize the
-// device every step. prism_jacobi_step_noalloc gives them one Jacobi sweep,
-// x <- x + D^-1 (b - A x), on a CSR matrix they already hold in device memory.
+// solver step: solvers embedded in a host application that owns a fixed
+// device-memory budget and forbids allocation after start-up, or a time-stepping
+// loop where a cudaMalloc/cudaFree pair would synchronize the device every step.
+// prism_jacobi_step_noalloc gives them one Jacobi sweep, x <- x + D^-1 (b - A x),
+// on a CSR matrix they already hold in device memory.
 //
 // The sweep has to be computed out of place (every row reads the old x of its
 // neighbours), so it needs an n-double scratch vector. Here that scratch is a
@@ -48,8 +47,9 @@ double* scratchAddress() {
     return g_scratch_ptr[dev];
 }
 
-// scratch[i] = x[i] + (b[i] - sum_j a_ij x_j) / a_ii   (numerics/jacobi.cpp:5-9)
-// One warp per row; a row without a diagonal entry yields NaN.
+// scratch[i] = x[i] + (1 / a_ii) (b[i] - sum_j a_ij x_j)   (numerics/jacobi.cpp:5-9)
+// One warp per row. A row without a diagonal entry has a_ii = 0, so 1 / a_ii = inf as in
+// the reference's A.diagonal().cwiseInverse().
 __global__ void __launch_bounds__(256) jacobi_csr_kernel(int n, const int* __restrict__ rowptr,
                                                          const int* __restrict__ col,
                                                          const double* __restrict__ val,
@@ -68,10 +68,7 @@ __global__ void __launch_bounds__(256) jacobi_csr_kernel(int n, const int* __res
         sum += __shfl_down_sync(0xffffffffu, sum, o);
         diag += __shfl_down_sync(0xffffffffu, diag, o);
     }
-    if (lane == 0) {
-        const double d = diag != 0.0 ? diag : NAN;
-        out[row] = x[row] + (1.0 / d) * (b[row] - sum);
-    }
+    if (lane == 0) out[row] = x[row] + (1.0 / diag) * (b[row] - sum);
 }
 
 __global__ void copy_kernel(int n, const double* __restrict__ src, double* __restrict__ dst) {
