@@ -1,6 +1,8 @@
 """Cell gradients on the GPU vs the oracle: least squares and the level-scheduled
 in-place Green-Gauss sweep reproduce the reference's cell-order sweep bit for bit
-(including the sweep-to-sweep Gauss-Seidel seeding)."""
+(including the sweep-to-sweep Gauss-Seidel seeding). The small hex box has at most
+16 dependency levels and runs one launch per level; the other meshes have more and
+run the sweep as one cooperative launch."""
 import numpy as np
 import pytest
 
@@ -12,10 +14,14 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("grad", [A.GRAD_LEAST_SQUARES, A.GRAD_GREEN_GAUSS])
-@pytest.mark.parametrize("kind", ["hex", "tet", "wedge"])
+@pytest.mark.parametrize("kind", ["hex_small", "hex", "hex16", "tet", "wedge"])
 def test_gradients_bit_exact(gpu, orc, grad, kind):
-    if kind == "hex":
+    if kind == "hex_small":
+        unv, case = meshgen.box_hex(5, 4, 3, jitter=0.2, seed=10), cases.box_case({"T": {"left": ("fixed", 2.0)}})
+    elif kind == "hex":
         unv, case = meshgen.box_hex(9, 7, 5, jitter=0.2, seed=11), cases.box_case({"T": {"left": ("fixed", 2.0)}})
+    elif kind == "hex16":
+        unv, case = meshgen.box_hex(16, 16, 16, jitter=0.2, seed=13), cases.box_case({"T": {"right": ("fixed", 1.0)}})
     elif kind == "tet":
         unv, case = meshgen.box_tet(4, 4, 4, jitter=0.2, seed=12), cases.box_case({"T": {"top": ("no-slip", 1.0)}})
     else:
