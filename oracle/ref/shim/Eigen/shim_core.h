@@ -683,30 +683,52 @@ class SparseMatrix {
     // duplicates summed in insertion order; entries sorted by row inside each column
     template <typename It>
     void setFromTriplets(It begin, It end) {
-        std::vector<std::vector<std::pair<Index, S>>> cols(static_cast<size_t>(cols_));
-        std::vector<std::vector<Index>> slot(static_cast<size_t>(cols_));
+        std::vector<StorageIndex> start(static_cast<size_t>(cols_ + 1), 0);
+        size_t total = 0;
         for (It it = begin; it != end; ++it) {
             Index r = it->row(), c = it->col();
             if (r < 0 || r >= rows_ || c < 0 || c >= cols_)
                 throw std::out_of_range("SparseMatrix::setFromTriplets: index out of range");
-            cols[c].emplace_back(r, it->value());
+            ++start[c + 1];
+            ++total;
+        }
+        for (Index c = 0; c < cols_; ++c) start[c + 1] += start[c];
+        // scatter by column, keeping the insertion order inside each column
+        std::vector<StorageIndex> rows(total);
+        std::vector<S> vals(total);
+        std::vector<StorageIndex> fill(start.begin(), start.end() - 1);
+        for (It it = begin; it != end; ++it) {
+            StorageIndex p = fill[it->col()]++;
+            rows[p] = static_cast<StorageIndex>(it->row());
+            vals[p] = it->value();
         }
         outer_.assign(static_cast<size_t>(cols_ + 1), 0);
         inner_.clear();
         val_.clear();
+        inner_.reserve(total);
+        val_.reserve(total);
+        std::vector<std::pair<StorageIndex, S>> col;
         for (Index c = 0; c < cols_; ++c) {
-            auto& v = cols[c];
-            std::vector<Index> order(v.size());
-            for (size_t k = 0; k < v.size(); ++k) order[k] = static_cast<Index>(k);
-            std::stable_sort(order.begin(), order.end(), [&](Index a, Index b) { return v[a].first < v[b].first; });
-            Index last = -1;
-            for (Index k : order) {
-                if (v[k].first == last) {
-                    val_.back() = val_.back() + v[k].second;
+            col.assign(static_cast<size_t>(start[c + 1] - start[c]), {});
+            for (StorageIndex k = start[c]; k < start[c + 1]; ++k) col[k - start[c]] = {rows[k], vals[k]};
+            // stable sort by row (insertion sort: the columns of a cell matrix are short)
+            for (size_t a = 1; a < col.size(); ++a) {
+                auto e = col[a];
+                size_t b = a;
+                while (b > 0 && col[b - 1].first > e.first) {
+                    col[b] = col[b - 1];
+                    --b;
+                }
+                col[b] = e;
+            }
+            StorageIndex last = -1;
+            for (const auto& [r, v] : col) {
+                if (r == last) {
+                    val_.back() = val_.back() + v;
                 } else {
-                    inner_.push_back(static_cast<StorageIndex>(v[k].first));
-                    val_.push_back(v[k].second);
-                    last = v[k].first;
+                    inner_.push_back(r);
+                    val_.push_back(v);
+                    last = r;
                 }
             }
             outer_[c + 1] = static_cast<StorageIndex>(inner_.size());
