@@ -9,17 +9,26 @@ urf 0.7/0.3 (the 512x512 cavity recipe) on 1448x1448x1 hexes (2,096,704 cells): 
 the working set (~1 GB) is larger than L2, so no flush is needed.
 
 Also reported: time to 1e-8 relative error of the 128^3 jittered-hex transport
-solve (LinearUpwind + Corrected), FP64 vs FP32/FP64-reliable-update BiCGSTAB,
-both AMG-preconditioned, and FP64 with the Jacobi preconditioner ("s_to_1e8"),
-the same SIMPLE steps with every outer iteration run as one CUDA graph launch
-("simple_graph": PrismSolveOpts.graph, device-side solver loops, results identical
-to the ordinary path), the live bandwidth of the dominant kernel (the finest-level AMG
-post-smoothing SpMV) and of the BiCGSTAB SpMV (CUDA events around sampled
-launches in the timed region), the discrete adjoint of steady diffusion on
-64^3 x 6 tets ("adjoint": times and finite-difference agreement) and 256
-independent diffusion solves in one persistent launch ("batched").
---impl reference times the CPU restatement of the reference
-(single-threaded, like the reference) on a bounded sample.
+solve (MUSCL + Corrected + Green-Gauss, one step() of the system assembled at
+T = 0) against the FP64 reference solution computed on the CPU by the
+reference's own code (tests/golden/c3_128_solution.npy, made by
+tests/golden/make_c3_solution.py and checked against its committed summary),
+FP64 vs FP32/FP64-reliable-update BiCGSTAB, both AMG-preconditioned, and FP64
+with the Jacobi preconditioner ("s_to_1e8"); the same SIMPLE steps with every
+outer iteration run as one CUDA graph launch ("simple_graph": PrismSolveOpts.graph,
+device-side solver loops, results identical to the ordinary path); the live
+bandwidth of the dominant kernel (the finest-level AMG post-smoothing SpMV) and
+of the BiCGSTAB SpMV (CUDA events around sampled launches in the timed region);
+the discrete adjoint of steady diffusion on 64^3 x 6 tets ("adjoint": times and
+finite-difference agreement) and 256 independent diffusion solves in one
+persistent launch ("batched").
+
+--impl reference times the reference's own code (oracle/_ref/libprism_ref.so,
+compiled from the reference's sources; single-threaded, like the reference) on
+the same 1448x1448x1 cavity: one SIMPLE outer iteration after one untimed one
+(the reference takes minutes per iteration at this size, so one is timed
+whatever --steps says; the line says so). The CPU restatement (the oracle) stands
+in when the compiled reference is absent.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -38,7 +47,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "s-to-1e-8 err (FP32+refine vs FP64 GPU), 2M-cell SIMPLE it/s, SpMV HBM GB/s"
 N_CAVITY = 1448
-N_CPU = 362  # bounded CPU sample: 1/16 of the cells
+N_CPU = 362  # the bounded CPU sample of the GPU arm: 1/16 of the cells
 UNIT = "SIMPLE it/s"
 
 
@@ -130,40 +139,60 @@ def max_over_ranks(world, value):
     return float(t.item())
 
 
-def cpu_simple_sample(steps=1):
-    """The CPU restatement of the reference (oracle) on a 362^2 cavity: seconds per SIMPLE step."""
-    import oracle
+def cavity_case(n):
+    """Mesh and boundary conditions of the lid-driven cavity (the same case as tests/cases.cavity)."""
+    from prism_b200 import meshgen
     from tests import cases
+    unv = meshgen.box_hex(n, n, 1, (1.0, 1.0, 1.0 / n))
+    wall = ("no-slip", [0.0, 0.0, 0.0])
+    case = cases.box_case({"U": {"top": ("fixed", [1.0, 0.0, 0.0]), "left": wall, "right": wall, "bottom": wall,
+                                 "back": ("empty", None), "front": ("empty", None)},
+                           "P": {"back": ("empty", None), "front": ("empty", None)}})
+    return unv, case
+
+
+def cpu_simple(n, warm=1, timed=1):
+    """SIMPLE outer iterations of the n x n cavity on the CPU by the reference's own code
+    (oracle/_ref, "reference"), else by the oracle's restatement ("port"): seconds of each
+    timed iteration after `warm` untimed ones, single-threaded like the reference."""
+    from oracle import ref_lib
+    if ref_lib.available():
+        unv, case = cavity_case(n)
+        mesh = ref_lib.Mesh(unv, case)
+        r = ref_lib.simple(mesh, warm + timed, nu=0.01, conv="Upwind", timings=True)
+        return list(r["seconds"][warm:]), "reference"
+    import oracle
     from prism_b200 import api
-    lib = oracle.lib()
-    mesh, U, p, nu, mdot, eqs = cases.cavity(N_CPU, lib)
+    from tests import cases
+    mesh, U, p, nu, mdot, eqs = cases.cavity(n, oracle.lib())
     simple = api.IncompressibleSIMPLE(api.SIMPLEControls())
-    t0 = time.perf_counter()
-    for _ in range(steps):
+    out = []
+    for i in range(warm + timed):
+        t0 = time.perf_counter()
         simple.step(eqs, U, mdot, p)
-    dt = (time.perf_counter() - t0) / steps
-    scale = (N_CPU * N_CPU) / float(N_CAVITY * N_CAVITY)
-    return scale / dt, dt
+        if i >= warm:
+            out.append(time.perf_counter() - t0)
+    return out, "port"
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    times = []
-    for i in range(args.warmup + args.steps):
-        it_s, dt = cpu_simple_sample(1)
-        if i >= args.warmup:
-            times.append(dt)
-    dt = sum(times) / len(times)
-    scale = (N_CPU * N_CPU) / float(N_CAVITY * N_CAVITY)
-    value = scale / dt
-    sample = (f"one SIMPLE outer iteration of the {N_CPU}x{N_CPU}x1 cavity ({N_CPU * N_CPU} cells) per step, "
-              f"it/s scaled by cells ({N_CPU * N_CPU}/{N_CAVITY * N_CAVITY}); single-threaded like the reference")
+    n = args.ref_n
+    secs, kind = cpu_simple(n, warm=1, timed=1)
+    dt = sum(secs) / len(secs)
+    value = 1.0 / dt
+    who = "the reference's own code (oracle/_ref)" if kind == "reference" else "the oracle's restatement"
+    sample = (f"{len(secs)} SIMPLE outer iteration of the {n}x{n}x1 cavity ({n * n} "
+              f"cells) after 1 untimed one, by {who}, single-threaded like the reference; one iteration is timed "
+              f"whatever --steps asks ({args.steps}): the reference takes {dt:.0f} s per iteration at this size")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"cavity SIMPLE {N_CAVITY}x{N_CAVITY}x1 (bounded CPU sample, see cpu_baseline)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+            "steps": len(secs), "steps_requested": args.steps, "warmup": 1, "ms_per_step": 1000.0 * dt,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"cavity SIMPLE {n}x{n}x1 ({n * n} cells), Re=100, "
+                                   "Upwind + Corrected, urf 0.7/0.3, BiCGSTAB + ILUT to machine precision (the "
+                                   "reference's solver::BiCGSTAB)", "cells": n * n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -171,16 +200,13 @@ def run_reference(args, world, rank):
 def transport_mesh(lib, n):
     """The C3 mesh: n^3 hexes, interior nodes jittered by +-0.2h (seed 3)."""
     from tests import cases
-    mesh, T, U, eqn = cases.transport_c3(n, lib, conv="LinearUpwind")
+    mesh, T, U, eqn = cases.transport_c3(n, lib, conv="MUSCL")
     return mesh
 
 
 def transport_eqn(mesh):
-    """Fresh fields and equation on the C3 mesh (fresh Green-Gauss state, T = 0): the C3
-    physics with LinearUpwind ("SecondOrderUpwind") convection. The reference's MUSCL
-    weights give systems with negative diagonals that neither a Jacobi-preconditioned
-    Krylov method nor the outer iteration solves; LinearUpwind keeps the same mesh,
-    velocity, diffusion and boundary conditions."""
+    """Fresh fields and equation on the C3 mesh (fresh Green-Gauss state, T = 0): MUSCL
+    convection + Corrected diffusion, Green-Gauss gradients (the mesh's case sets them)."""
     import numpy as np
     from prism_b200 import api
     cc = mesh.export()["cell_center"]
@@ -188,12 +214,30 @@ def transport_eqn(mesh):
                                         -np.cos(np.pi * cc[0]) * np.sin(np.pi * cc[1]), np.zeros(mesh.n_cells)]))
     T = api.Scalar("T", mesh, 0.0)
     k = api.Scalar("kappa", mesh, 1e-3)
-    eqn = api.Transport(api.convection.LinearUpwind(U, T), api.diffusion.Corrected(k, T))
+    eqn = api.Transport(api.convection.MUSCL(U, T), api.diffusion.Corrected(k, T))
     return T, (U, k), eqn
 
 
+def cpu_reference_solution(n):
+    """x* of the system assembled at T = 0, solved on the CPU by the reference's own code
+    (BiCGSTAB + ILUT to machine precision), as written by tests/golden/make_c3_solution.py:
+    returned only when the stored vector matches its committed summary (checksum)."""
+    import hashlib
+    import numpy as np
+    npy = os.path.join(ROOT, "tests", "golden", f"c3_{n}_solution.npy")
+    js = os.path.join(ROOT, "tests", "golden", f"c3_{n}_solution.json")
+    if not (os.path.exists(npy) and os.path.exists(js)):
+        return None, None
+    with open(js) as fh:
+        summ = json.load(fh)
+    x = np.load(npy)
+    if hashlib.sha256(np.ascontiguousarray(x, np.float64).tobytes()).hexdigest() != summ["sha256"]:
+        return None, None
+    return x, summ
+
+
 def transport_exact(mesh):
-    """x* of the system assembled at T = 0: FP64 BiCGSTAB to ||b - Ax|| <= 1e-14 ||b||."""
+    """x* of the system assembled at T = 0 on the GPU: FP64 BiCGSTAB to ||b - Ax|| <= 1e-14 ||b||."""
     from prism_b200 import api
     T, keep, eqn = transport_eqn(mesh)
     api.BiCGSTAB(krylov_tol=1e-14, krylov_max_iter=100000, preconditioner="jacobi").solve(eqn, 1, 0.0)
@@ -458,18 +502,27 @@ def run_ours(args, world, rank, local):
     if rank == 0 and not args.skip_transport:
         nt = args.transport_n
         tmesh = transport_mesh(lib, nt)
-        ref = transport_exact(tmesh)
+        gpu_x = transport_exact(tmesh)
+        cpu_x, summ = cpu_reference_solution(nt)
+        ref = cpu_x if cpu_x is not None else gpu_x
         r64 = transport_time_to_tol(tmesh, A.PREC_FP64, ref, preconditioner="amg")
         r32 = transport_time_to_tol(tmesh, A.PREC_MIXED, ref, preconditioner="amg")
         rj = transport_time_to_tol(tmesh, A.PREC_FP64, ref, preconditioner="jacobi")
+        if cpu_x is not None:
+            refsol = (f"CPU FP64 solution by {summ['solver']} (BiCGSTAB + ILUT to machine precision), "
+                      f"tests/golden/c3_{nt}_solution.npy, checksum-verified")
+        else:
+            refsol = "GPU FP64 BiCGSTAB(Jacobi) to ||b-Ax|| <= 1e-14 ||b|| (no stored CPU solution for this size)"
         extra["s_to_1e8"] = {"workload": f"{nt}^3 hexes jittered +-0.2h (seed 3), U = (sin pi x cos pi y, "
-                                         f"-cos pi x sin pi y, 0), kappa 1e-3, LinearUpwind + Corrected, "
+                                         f"-cos pi x sin pi y, 0), kappa 1e-3, MUSCL + Corrected + Green-Gauss, "
                                          f"T fixed 1/0 at x=0/1; one step() of the system assembled at T=0 "
-                                         f"(assembly, AMG setup and iterations timed)",
+                                         f"(assembly, gradient sweep, AMG setup and iterations timed)",
                              "fp64": r64, "mixed": r32, "fp64_jacobi": rj,
                              "speedup": r64["seconds"] / r32["seconds"] if r32["seconds"] > 0 else None,
                              "speedup_vs_fp64_jacobi": rj["seconds"] / r32["seconds"] if r32["seconds"] > 0 else None,
-                             "reference_solution": "FP64 BiCGSTAB(Jacobi) to ||b-Ax|| <= 1e-14 ||b||"}
+                             "reference_solution": refsol,
+                             "gpu_fp64_1e-14_vs_reference_solution": float(
+                                 np.linalg.norm(gpu_x - ref) / np.linalg.norm(ref))}
 
     if rank == 0 and not args.skip_adjoint:
         extra["adjoint"] = adjoint_measure(lib)
@@ -478,10 +531,16 @@ def run_ours(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        it_s, dt = cpu_simple_sample(1)
-        cpu = {"value": it_s, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"one SIMPLE outer iteration of the {N_CPU}x{N_CPU}x1 cavity ({dt:.1f} s), "
-                         f"it/s scaled by the cell ratio {N_CPU * N_CPU}/{N_CAVITY * N_CAVITY}"}
+        # bounded sample: the full-size cavity takes the CPU minutes per iteration (the reference
+        # arm, --impl reference, times it); here one iteration of a 1/16-size cavity, scaled
+        secs, kind = cpu_simple(N_CPU, warm=1, timed=1)
+        dt = secs[0]
+        scale = (N_CPU * N_CPU) / float(N_CAVITY * N_CAVITY)
+        cpu = {"value": scale / dt, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"the second SIMPLE outer iteration of the {N_CPU}x{N_CPU}x1 cavity ({dt:.1f} s, "
+                         f"{'the reference' + chr(39) + 's own code' if kind == 'reference' else 'the oracle'}, "
+                         f"one core), it/s scaled by the cell ratio {N_CPU * N_CPU}/{N_CAVITY * N_CAVITY}; the "
+                         f"full-size iteration is timed by --impl reference"}
 
     if rank == 0:
         # kernel launches per step, counted from the solver's iteration counts
@@ -515,6 +574,7 @@ def main():
     ap.add_argument("--transport-n", type=int, default=128)
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--ref-n", type=int, default=N_CAVITY, help="cavity size of the reference arm (tests only)")
     args = ap.parse_args()
     world, rank, local = dist_init(args)
     try:

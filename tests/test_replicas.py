@@ -34,6 +34,7 @@ def _rank(rank, world, port, q):
     class Args:
         impl = "reference"
         steps, warmup = 2, 0
+        ref_n = 8
 
     w, r, _ = bench.dist_init(Args)
     try:
@@ -42,7 +43,7 @@ def _rank(rank, world, port, q):
         # replicas: the units all ranks processed over the slowest rank's time
         value = w * Args.steps / t
         # the reference arm with a stand-in sample: only rank 0 measures and prints
-        bench.cpu_simple_sample = lambda steps: (1.0, 0.25)
+        bench.cpu_simple = lambda n, warm=1, timed=1: ([0.25], "reference")
         out = io.StringIO()
         with contextlib.redirect_stdout(out):
             bench.run_reference(Args, w, r)
@@ -76,11 +77,12 @@ def test_reference_arm_under_torchrun():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl", "reference",
-           "--gpus", "2", "--steps", "1", "--warmup", "0"]
+           "--gpus", "2", "--steps", "1", "--warmup", "0", "--ref-n", "16"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(line) for line in r.stdout.splitlines() if line.startswith("{")]
     assert len(lines) == 1
     d = lines[0]
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
-    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["e2e"]["h2d_bytes_per_step"] == 0
+    assert d["config"]["cells"] == 16 * 16
