@@ -1,24 +1,32 @@
-// assemble.cu -- fused face-loop assembly of one eqn::Transport.
+// assemble.cu -- face-loop assembly of one eqn::Transport in two passes.
 //
-// One thread owns one matrix row (cell). It walks the cell's faces in the
-// reference's insertion order (boundary faces patch by patch as
-// applyBoundary visits them, then interior faces by face id as
-// IFullScheme::apply visits them, scheme.cpp:12-22) and evaluates, for its own
-// row only, every scheme of the equation:
+// Face pass: one thread per non-empty face evaluates, once, every scheme term
+// the face contributes to the rows of its cells:
 //   convection  IConvection::applyInterior + Upwind::interpolate + weightsNVF
-//               (convection.cpp:18-128, convection_hr.cpp:6-23) and the
-//               Fixed/Outlet/ZeroGradient handlers (convection_boundary.cpp:4-61);
+//               (convection.cpp:18-128, convection_hr.cpp:6-23) for the owner's
+//               row and, with the flux reversed, the neighbour's (both from the
+//               same pair of phi-tilde values) and the Fixed/Outlet/ZeroGradient
+//               handlers (convection_boundary.cpp:4-61);
 //   diffusion   NonCorrected / Corrected (diffusion.h:116-205) with the
 //               over-relaxed / minimum / orthogonal decomposition
-//               (nonortho.cpp:7-21) and Fixed/NoSlip/FixedGradient handlers
-//               (diffusion_boundary.h:113-234);
-//   sources     ConstantScalar / Divergence / Gradient (scheme/source/*.h);
-//   symmetry    eqn::boundary::Symmetry<Transport> (equation/symmetry.cpp:54-90).
-// Per-scheme partial sums are kept apart and combined in Transport::updateCoeffs
-// order (transport.cpp:4-21), so with FMA contraction disabled the result is
-// the reference's arithmetic, term for term. Each interior face is evaluated
-// by both of its cells; no value is written by two threads and no atomics are
-// used, so assembly is deterministic.
+//               (nonortho.cpp:7-21) and the Fixed/NoSlip/FixedGradient handlers
+//               (diffusion_boundary.h:113-234).
+// It writes the off-diagonal coefficients (each interior face owns the two
+// matrix entries it couples) and, per (cell, face) pair, a record of the terms
+// that the cell's diagonal and right-hand side sum: convection diagonal, its
+// rhs, diffusion diagonal, its rhs. The records sit in the cells' assembly-order
+// lists, so the cell pass reads each cell's records contiguously.
+// Cell pass: one thread per row sums its records in the reference's insertion
+// order (boundary faces patch by patch as applyBoundary visits them, then
+// interior faces by face id as IFullScheme::apply does, scheme.cpp:12-22),
+// then the sources (scheme/source/*.h), the temporal term and the symmetry
+// handler (equation/symmetry.cpp:54-90), and combines the per-scheme sums in
+// Transport::updateCoeffs order (transport.cpp:4-21). With FMA contraction
+// disabled the result is the reference's arithmetic, term for term; no value is
+// written by two threads and no atomics are used, so assembly is deterministic.
+// Empty-patch faces keep all-zero records: adding +0.0 to a sum that starts at
+// +0.0 changes no bit. Padding slots of the SELL rows are never written (the
+// matrix is zeroed on allocation and by zeroOutCoeffs).
 #include "assemble.h"
 #include "devmath.cuh"
 
@@ -85,144 +93,195 @@ __device__ __forceinline__ void decompose(int corr, D3 S, D3 e, D3& E, D3& T) {
     T = S - E;
 }
 
-__global__ void __launch_bounds__(256) assemble_kernel(const AssembleParams P) {
+__device__ __forceinline__ void putRec(double* rec, int q, double dc, double rc, double dd, double rd) {
+    double4* r = reinterpret_cast<double4*>(rec) + q;
+    *r = make_double4(dc, rc, dd, rd);
+}
+
+__global__ void __launch_bounds__(256) assemble_faces_kernel(const AssembleParams P) {
+    const MeshView& m = P.m;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m.nne + (m.nf - m.nb)) return;
+    const int f = i < m.nne ? i : m.nb + (i - m.nne);
+    const ScalarView& phi = P.phi;
+    if (f < m.nb) {
+        // boundary face of a non-empty patch: terms of the owner's row
+        const int c = m.owner[f];
+        const int p = m.bpatch[f];
+        const int k = phi.bc_kind[p];
+        const D3 Sf = areaVector(m, f);
+        double dc = 0.0, rc = 0.0, dd = 0.0, rd = 0.0;
+        if (P.has_conv) {
+            if (k == PRISM_BC_FIXED) {
+                double phi_wall = phi.bc_val[p];
+                double mdot = vectorFlux(m, P.conv.U, f);
+                dc = smax(mdot, 0.0);
+                rc = smax(-mdot, 0.0) * phi_wall;
+            } else if (k == PRISM_BC_OUTLET || k == PRISM_BC_ZERO_GRADIENT) {
+                D3 Uf = vectorFace(m, P.conv.U, f);
+                dc = dot(Uf, Sf);
+            }
+        }
+        if (P.has_diff) {
+            if (k == PRISM_BC_FIXED || k == PRISM_BC_NOSLIP) {
+                double phi_wall = scalarFace(m, phi, f);
+                D3 d_Cf = faceCenter(m, f) - cellCenter(m, c);
+                double dn = norm(d_Cf);
+                D3 Sp = kappaCell(P, c, Sf);
+                if (!P.diff.corrected) {
+                    double g = dot(Sp, d_Cf) / (dn * dn + EPSILON);
+                    dd = g;
+                    rd = g * phi_wall;
+                } else {
+                    D3 e = d_Cf / dn;
+                    D3 E, T;
+                    decompose(P.diff.corrector, Sp, e, E, T);
+                    double g = dot(E, d_Cf) / (dn * dn + EPSILON);
+                    dd = g;
+                    rd = (g * phi_wall) + dot(T, gradFace(m, phi, f));
+                }
+            } else if (k == PRISM_BC_FIXED_GRADIENT) {
+                D3 wg{phi.bc_vec[3 * p], phi.bc_vec[3 * p + 1], phi.bc_vec[3 * p + 2]};
+                D3 Sp = kappaCell(P, c, Sf);
+                rd = -dot(wg, Sp);
+            }
+        }
+        putRec(P.rec, P.face_slot[2 * f], dc, rc, dd, rd);
+        return;
+    }
+    // interior face: owner o, neighbour n
+    const int o = m.owner[f];
+    const int n = m.nbr[f];
+    const D3 xo = cellCenter(m, o), xn = cellCenter(m, n);
+    double aCo = 0.0, aNo = 0.0, bo = 0.0, aCn = 0.0, aNn = 0.0, bn = 0.0;
+    if (P.has_conv) {
+        const double mdot = vectorFlux(m, P.conv.U, f);
+        const double phio = phi.v[o], phin = phi.v[n];
+        D3 go{0, 0, 0}, gn{0, 0, 0};
+        if (P.need_grad) {
+            go = gradAt(phi, o);
+            gn = gradAt(phi, n);
+        }
+        // Upwind::interpolate from the owner's side (m_dot = mdot) and from the neighbour's
+        // (m_dot = -mdot): the neighbour's phi-tilde pair is the owner's, swapped
+        const double pu = phin - (2 * dot(go, xn - xo));
+        const double t = (phio - pu) / (phin - pu);
+        const NVF w = weightsNVF(P.conv.scheme, t);
+        const double pu2 = phio - (2 * dot(gn, xo - xn));
+        const double t2 = (phin - pu2) / (phio - pu2);
+        const NVF w2 = weightsNVF(P.conv.scheme, t2);
+        aCo = smax(mdot, 0.0) * w.l;
+        aNo = smax(mdot, 0.0) * w.k;
+        bo = -smax(mdot, 0.0) * (1 - w.l - w.k) * pu;
+        aCo += -smax(-mdot, 0.0) * w2.k;
+        aNo += -smax(-mdot, 0.0) * w2.l;
+        bo += smax(-mdot, 0.0) * (1 - w2.l - w2.k) * pu2;
+        const double mn = -mdot;
+        aCn = smax(mn, 0.0) * w2.l;
+        aNn = smax(mn, 0.0) * w2.k;
+        bn = -smax(mn, 0.0) * (1 - w2.l - w2.k) * pu2;
+        aCn += -smax(-mn, 0.0) * w.k;
+        aNn += -smax(-mn, 0.0) * w.l;
+        bn += smax(-mn, 0.0) * (1 - w.l - w.k) * pu;
+    }
+    double g = 0.0, tf = 0.0;
+    if (P.has_diff) {
+        const D3 d_CF = xn - xo;
+        const double dn = norm(d_CF);
+        const D3 Sf = areaVector(m, f);
+        if (!P.diff.corrected) {
+            D3 Sp = kappaFace(P, f, Sf);
+            g = dot(Sp, d_CF) / (dn * dn + EPSILON);
+        } else {
+            D3 e = d_CF / dn;
+            D3 Sp = kappaFace(P, f, Sf);
+            D3 E, T;
+            decompose(P.diff.corrector, Sp, e, E, T);
+            g = dot(E, d_CF) / (dn * dn + EPSILON);
+            tf = dot(T, gradFace(m, phi, f));
+        }
+    }
+    // off-diagonal coefficients, the schemes' terms added in registration order
+    const int pon = P.face_pos[2 * f], pno = P.face_pos[2 * f + 1];
+    double a1 = P.accumulate ? P.A[pon] : 0.0;
+    double a2 = P.accumulate ? P.A[pno] : 0.0;
+    if (P.conv_first) {
+        if (P.has_conv) {
+            a1 = a1 + aNo;
+            a2 = a2 + aNn;
+        }
+        if (P.has_diff) {
+            a1 = a1 + -g;
+            a2 = a2 + -g;
+        }
+    } else {
+        if (P.has_diff) {
+            a1 = a1 + -g;
+            a2 = a2 + -g;
+        }
+        if (P.has_conv) {
+            a1 = a1 + aNo;
+            a2 = a2 + aNn;
+        }
+    }
+    P.A[pon] = a1;
+    P.A[pno] = a2;
+    putRec(P.rec, P.face_slot[2 * f], aCo, bo, g, tf);
+    putRec(P.rec, P.face_slot[2 * f + 1], aCn, bn, g, -tf);
+}
+
+__global__ void __launch_bounds__(256, 4) assemble_cells_kernel(const AssembleParams P) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const MeshView& m = P.m;
     if (c >= m.nc) return;
-    const ScalarView& phi = P.phi;
-    const D3 xc = cellCenter(m, c);
-    const double phic = phi.v[c];
-    D3 gradc{0, 0, 0};
-    if (P.need_grad) gradc = gradAt(phi, c);
 
+    // the rows' sums over the cell's faces, in insertion order
     double dcv = 0.0, ddf = 0.0, rcv = 0.0, rdf = 0.0;
+    const double4* R = reinterpret_cast<const double4*>(P.rec);
+    for (int q = P.ca_off[c]; q < P.ca_off[c + 1]; ++q) {
+        const double4 r = R[q];
+        dcv += r.x;
+        rcv += r.y;
+        ddf += r.z;
+        rdf += r.w;
+    }
+
     // symmetry handler sums, one per patch, applied in patch order after the sources
     double sym_a[6], sym_b[6];
     int nsym = 0, sym_patch = -1;
-
-    // zero this row's coefficients when the equation is clean
-    const int slice = c >> 5, lane = c & 31;
-    const int rb = m.sl_off[slice], width = (m.sl_off[slice + 1] - rb) >> 5;
-    if (!P.accumulate)
-        for (int j = 0; j < width; ++j) P.A[rb + 32 * j + lane] = 0.0;
-
-    for (int q = P.ca_off[c]; q < P.ca_off[c + 1]; ++q) {
-        const int f = P.ca_face[q];
-        if (f < m.nb) {
+    if (P.symmetry) {
+        const ScalarView& phi = P.phi;
+        const D3 xc = cellCenter(m, c);
+        for (int q = P.ca_off[c]; q < P.ca_off[c + 1]; ++q) {
+            const int f = P.ca_face[q];
+            if (f >= m.nb) continue;
             const int p = m.bpatch[f];
-            if (m.patch_empty[p]) continue;
-            const int k = phi.bc_kind[p];
+            if (m.patch_empty[p] || phi.bc_kind[p] != PRISM_BC_SYMMETRY) continue;
             const D3 Sf = areaVector(m, f);
-            if (P.has_conv) {
-                if (k == PRISM_BC_FIXED) {
-                    double phi_wall = phi.bc_val[p];
-                    double mdot = vectorFlux(m, P.conv.U, f);
-                    dcv += smax(mdot, 0.0);
-                    rcv += smax(-mdot, 0.0) * phi_wall;
-                } else if (k == PRISM_BC_OUTLET || k == PRISM_BC_ZERO_GRADIENT) {
-                    D3 Uf = vectorFace(m, P.conv.U, f);
-                    dcv += dot(Uf, Sf);
-                }
-            }
-            if (P.has_diff) {
-                if (k == PRISM_BC_FIXED || k == PRISM_BC_NOSLIP) {
-                    double phi_wall = scalarFace(m, phi, f);
-                    D3 d_Cf = faceCenter(m, f) - xc;
-                    double dn = norm(d_Cf);
-                    D3 Sp = kappaCell(P, c, Sf);
-                    if (!P.diff.corrected) {
-                        double g = dot(Sp, d_Cf) / (dn * dn + EPSILON);
-                        ddf += g;
-                        rdf += g * phi_wall;
-                    } else {
-                        D3 e = d_Cf / dn;
-                        D3 E, T;
-                        decompose(P.diff.corrector, Sp, e, E, T);
-                        double g = dot(E, d_Cf) / (dn * dn + EPSILON);
-                        ddf += g;
-                        rdf += (g * phi_wall) + dot(T, gradFace(m, phi, f));
-                    }
-                } else if (k == PRISM_BC_FIXED_GRADIENT) {
-                    D3 wg{phi.bc_vec[3 * p], phi.bc_vec[3 * p + 1], phi.bc_vec[3 * p + 2]};
-                    D3 Sp = kappaCell(P, c, Sf);
-                    rdf += -dot(wg, Sp);
-                }
-            }
-            if (P.symmetry && k == PRISM_BC_SYMMETRY) {
-                D3 n = faceNormal(m, f);
-                double d_normal = dot(faceCenter(m, f) - xc, n);
-                const VectorView& U = P.conv.U;
-                D3 Uc{U.c[0].v[c], U.c[1].v[c], U.c[2].v[c]};
-                double g = 2 * norm(kappaCell(P, c, Sf)) / d_normal;
-                double ac, bb;
-                if (P.phi_coord == 0) {
-                    ac = n.x * n.x;
-                    bb = ((Uc.y * n.y) + (Uc.z * n.z)) * n.x;
-                } else if (P.phi_coord == 1) {
-                    ac = n.y * n.y;
-                    bb = ((Uc.x * n.x) + (Uc.z * n.z)) * n.y;
-                } else {
-                    ac = n.z * n.z;
-                    bb = ((Uc.x * n.x) + (Uc.y * n.y)) * n.z;
-                }
-                if (p != sym_patch) {
-                    sym_patch = p;
-                    sym_a[nsym] = 0.0;
-                    sym_b[nsym] = 0.0;
-                    ++nsym;
-                }
-                sym_a[nsym - 1] += g * ac;
-                sym_b[nsym - 1] += -g * bb;
-            }
-        } else {
-            const int o = m.owner[f];
-            const int nb_ = m.nbr[f];
-            const bool own = (o == c);
-            const int n = own ? nb_ : o;
-            const D3 xn = cellCenter(m, n);
-            double off_cv = 0.0, off_df = 0.0;
-            if (P.has_conv) {
-                double mdot = vectorFlux(m, P.conv.U, f);
-                double aC, aN, b;
-                interpolate(P.conv.scheme, own ? mdot : -mdot, phic, phi.v[n], gradc, gradAt(phi, n), xc, xn, aC, aN,
-                            b);
-                dcv += aC;
-                off_cv = aN;
-                rcv += b;
-            }
-            if (P.has_diff) {
-                // owner-oriented quantities, so both cells compute the same g and T
-                const D3 xo = own ? xc : xn, xnb = own ? xn : xc;
-                const D3 d_CF = xnb - xo;
-                const double dn = norm(d_CF);
-                const D3 Sf = areaVector(m, f);
-                double g;
-                if (!P.diff.corrected) {
-                    D3 Sp = kappaFace(P, f, Sf);
-                    g = dot(Sp, d_CF) / (dn * dn + EPSILON);
-                } else {
-                    D3 e = d_CF / dn;
-                    D3 Sp = kappaFace(P, f, Sf);
-                    D3 E, T;
-                    decompose(P.diff.corrector, Sp, e, E, T);
-                    g = dot(E, d_CF) / (dn * dn + EPSILON);
-                    D3 gf = gradFace(m, phi, f);
-                    double t = dot(T, gf);
-                    rdf += own ? t : -t;
-                }
-                ddf += g;
-                off_df = -g;
-            }
-            const int pos = P.ca_pos[q];
-            double a = P.accumulate ? P.A[pos] : 0.0;
-            if (P.conv_first) {
-                if (P.has_conv) a = a + off_cv;
-                if (P.has_diff) a = a + off_df;
+            D3 n = faceNormal(m, f);
+            double d_normal = dot(faceCenter(m, f) - xc, n);
+            const VectorView& U = P.conv.U;
+            D3 Uc{U.c[0].v[c], U.c[1].v[c], U.c[2].v[c]};
+            double g = 2 * norm(kappaCell(P, c, Sf)) / d_normal;
+            double ac, bb;
+            if (P.phi_coord == 0) {
+                ac = n.x * n.x;
+                bb = ((Uc.y * n.y) + (Uc.z * n.z)) * n.x;
+            } else if (P.phi_coord == 1) {
+                ac = n.y * n.y;
+                bb = ((Uc.x * n.x) + (Uc.z * n.z)) * n.y;
             } else {
-                if (P.has_diff) a = a + off_df;
-                if (P.has_conv) a = a + off_cv;
+                ac = n.z * n.z;
+                bb = ((Uc.x * n.x) + (Uc.y * n.y)) * n.z;
             }
-            P.A[pos] = a;
+            if (p != sym_patch) {
+                sym_patch = p;
+                sym_a[nsym] = 0.0;
+                sym_b[nsym] = 0.0;
+                ++nsym;
+            }
+            sym_a[nsym - 1] += g * ac;
+            sym_b[nsym - 1] += -g * bb;
         }
     }
 
@@ -292,8 +351,13 @@ __global__ void __launch_bounds__(256) assemble_kernel(const AssembleParams P) {
 
 void launchAssemble(const AssembleParams& P, cudaStream_t s) {
     if (P.m.nc == 0) return;
-    assemble_kernel<<<ceil_div(P.m.nc, 256), 256, 0, s>>>(P); countLaunch();
-    PB_LAUNCH("assemble_kernel");
+    const int nfaces = P.m.nne + (P.m.nf - P.m.nb);
+    if (nfaces > 0) {
+        assemble_faces_kernel<<<ceil_div(nfaces, 256), 256, 0, s>>>(P); countLaunch();
+        PB_LAUNCH("assemble_faces_kernel");
+    }
+    assemble_cells_kernel<<<ceil_div(P.m.nc, 256), 256, 0, s>>>(P); countLaunch();
+    PB_LAUNCH("assemble_cells_kernel");
 }
 
 // Transport::relax (transport.cpp:54-64)

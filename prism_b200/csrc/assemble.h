@@ -46,6 +46,9 @@ struct AssembleParams {
     const int* ca_off;  // cell -> faces in insertion order
     const int* ca_face;
     const int* ca_pos;  // SELL position of (c, other), -1 on boundary
+    const int* face_slot;  // per face, owner / neighbour side: index of the face in that cell's list
+    const int* face_pos;   // per face, owner / neighbour side: SELL position of the off-diagonal
+    double* rec;        // 4 doubles per list entry: the face's terms of that row (zero on empty faces)
     double* A;          // SELL values
     double* b;
     double* bconv;      // accumulated scheme right-hand sides

@@ -187,7 +187,11 @@ __global__ void __launch_bounds__(BS, 5) spmv_kernel(int nslices, int n, const i
     double v[2] = {d0, d1}, out[2];
     if (reduceLast<2, false>(v, partials, counter, out) && threadIdx.x == 0) {
         if (STAGE == 1) {
-            S->alpha = S->rho / out[0];
+            // r0.v = 0 (or a non-finite alpha) breaks the recurrence down: the host restarts
+            // from the current x (every later kernel of this iteration returns at once)
+            const double alpha = S->rho / out[0];
+            if (out[0] == 0.0 || !isfinite(alpha)) S->done = isfinite(out[0]) ? 3 : 5;
+            else S->alpha = alpha;
         } else {
             S->ts = out[0];
             S->tt = out[1];
@@ -851,8 +855,14 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
             done = reliable(1);
             continue;
         }
+        if (done == 5) {  // the FP32 recurrence overflowed: drop its correction, restart from X
+            if (++restarts > 20) break;
+            fill_zero_f<<<gn, BS, 0, s>>>(n, w.x32.p); countLaunch();
+            done = reliable(1);
+            continue;
+        }
     }
-    if (done == 2 || done == 3 || done == 5) {
+    if (done == 2 || done == 3) {
         flush_kernel<<<gn, BS, 0, s>>>(n, X, w.x32.p); countLaunch();
     }
     out.iterations = w.host_state->iter;

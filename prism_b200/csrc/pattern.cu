@@ -124,6 +124,19 @@ __global__ void fill_kernel(int nc, int nslices, const int* cf_off, const int* c
     }
 }
 
+// face -> (cell, face) entries of the assembly-order lists, both sides
+__global__ void face_slots_kernel(int nc, const int* cf_off, const int* ca_face, const int* ca_pos, const int* owner,
+                                  int* face_slot, int* face_pos) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    for (int q = cf_off[c]; q < cf_off[c + 1]; ++q) {
+        const int f = ca_face[q];
+        const int side = owner[f] == c ? 0 : 1;
+        face_slot[2 * f + side] = q;
+        face_pos[2 * f + side] = ca_pos[q];
+    }
+}
+
 }  // namespace
 
 void buildPattern(const PatternInput& in, PatternOutput& out, cudaStream_t s) {
@@ -163,6 +176,13 @@ void buildPattern(const PatternInput& in, PatternOutput& out, cudaStream_t s) {
         nc, nslices, in.cf_off, in.cf_face, in.owner, in.nbr, in.nb, in.npatch, in.bpatch, in.ppos, out.rowptr.p,
         out.sl_off.p, out.col.p, out.sl_col.p, out.diag_pos.p, out.ca_face.p, out.ca_pos.p); countLaunch();
     PB_LAUNCH("pattern fill_kernel");
+    out.face_slot.alloc(2 * (size_t)std::max(in.nf, 1));
+    out.face_pos.alloc(2 * (size_t)std::max(in.nf, 1));
+    PB_CUDA(cudaMemsetAsync(out.face_slot.p, 0xff, 2 * (size_t)std::max(in.nf, 1) * sizeof(int), s));
+    PB_CUDA(cudaMemsetAsync(out.face_pos.p, 0xff, 2 * (size_t)std::max(in.nf, 1) * sizeof(int), s));
+    face_slots_kernel<<<ceil_div(nc, 256), 256, 0, s>>>(nc, in.cf_off, out.ca_face.p, out.ca_pos.p, in.owner,
+                                                        out.face_slot.p, out.face_pos.p); countLaunch();
+    PB_LAUNCH("pattern face_slots_kernel");
     PB_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -14,6 +14,7 @@ struct PatternInput {
     const int* nbr;        // device, nf (-1 on boundary)
     const int* bpatch;     // device, nb
     const int* ppos;       // device, nb: position of the face in its patch's face list
+    int nf;                // faces
 };
 
 struct PatternOutput {
@@ -23,6 +24,10 @@ struct PatternOutput {
     DevBuf<int> sl_off, sl_col;    // SELL-32
     DevBuf<int> diag_pos;          // SELL position of (c, c)
     DevBuf<int> ca_face, ca_pos;   // cell faces in assembly order + SELL positions
+    // per face, owner side then neighbour side (-1 where a boundary face has none): the
+    // index of the face in that cell's assembly-order list, and the SELL position of the
+    // off-diagonal coefficient the face contributes to that cell's row
+    DevBuf<int> face_slot, face_pos;
 };
 
 void buildPattern(const PatternInput& in, PatternOutput& out, cudaStream_t s);

@@ -177,7 +177,7 @@ void setupDevice(Mesh& m) {
     upload(m.cf_face, h.cf_face, s);
 
     PatternInput pin{m.nc, m.nb, m.npatch, (int64_t)h.cf_face.size(), m.cf_off.p, m.cf_face.p,
-                     m.owner.p, m.nbr.p, m.bpatch.p, m.ppos.p};
+                     m.owner.p, m.nbr.p, m.bpatch.p, m.ppos.p, m.nf};
     buildPattern(pin, m.pat, s);
 
     // Green-Gauss schedule: level[c] = 1 + max(level of lower-numbered neighbours)
@@ -201,6 +201,7 @@ void setupDevice(Mesh& m) {
     std::vector<int> lc(m.nc), fill(m.level_off.begin(), m.level_off.end() - 1);
     for (int c = 0; c < m.nc; ++c) lc[fill[level[c]]++] = c;
     upload(m.level_cells, lc, s);
+    upload(m.level_off_dev, m.level_off, s);
     m.scratch.alloc(std::max(3 * m.nf, 1));
     m.ls_ready = false;
     m.points_ready = false;
@@ -329,7 +330,7 @@ void computeGradient(Scalar& s) {
         m.ensureLeastSquares();
         launchLeastSquares(m.view(), s.view(), m.ls_pinv.p, m.ls_w.p, (int64_t)m.h->cf_face.size(), m.stream);
     } else {
-        launchGreenGauss(m.view(), s.view(), m.level_cells.p, m.level_off, m.stream);
+        launchGreenGauss(m.view(), s.view(), m.level_cells.p, m.level_off, m.level_off_dev.p, m.stream);
     }
     s.grad->computed = s.event;
 }
@@ -477,6 +478,14 @@ void updateCoeffs(Transport& eq) {
     P.ca_off = m.cf_off.p;
     P.ca_face = m.pat.ca_face.p;
     P.ca_pos = m.pat.ca_pos.p;
+    P.face_slot = m.pat.face_slot.p;
+    P.face_pos = m.pat.face_pos.p;
+    if (!m.asm_rec.p) {
+        // records of empty-patch faces are never written and stay zero
+        m.asm_rec.alloc(4 * std::max<size_t>(m.h->cf_face.size(), 1));
+        m.asm_rec.zero(m.stream);
+    }
+    P.rec = m.asm_rec.p;
     P.A = eq.A.p;
     P.b = eq.b.p;
     P.bconv = eq.bconv.p;

@@ -33,13 +33,14 @@ struct Mesh {
     DevBuf<double> area, nx, ny, nz, fx, fy, fz, cx, cy, cz, vol, gcw;
     PatternOutput pat;
     // Green-Gauss sweep schedule: cells grouped by dependency level
-    DevBuf<int> level_cells;
+    DevBuf<int> level_cells, level_off_dev;
     std::vector<int> level_off;
     // least-squares operators (built on first use, shared by every field)
     DevBuf<double> ls_pinv, ls_w;
     bool ls_ready = false;
     KrylovWork kw;
     DevBuf<int> cf_twin, tpos;  // adjoint: twin cell-face entries, transpose positions (built on first use)
+    DevBuf<double> asm_rec;      // assembly: 4 doubles per cell-face entry (allocated zeroed on first use)
     std::shared_ptr<Amg> p_amg;  // AMG hierarchy of the pressure-correction equation (SIMPLE/PRIME/PISO)
     // pressure-correction objects of SIMPLE/PRIME/PISO, reset on every step instead of
     // re-created (their device buffers stay allocated between steps)

@@ -1,12 +1,11 @@
 """The fused coarse-level launch of the AMG V-cycle at every size.
 
-The coarse levels run in one launch: a thread-block cluster for the levels of at
-most PRISM_AMG_TAIL_ROWS rows, or a cooperative launch over every SM for the
-levels of at most PRISM_AMG_GRID_ROWS rows (which takes precedence). Both are
-read once per process, hence the subprocesses. With the whole hierarchy below the
-finest level in either launch, with none of it, and with the defaults, the
-solutions must agree with the oracle within the solver tolerance of the other
-AMG tests, in FP64 and in mixed precision."""
+By default only levels of at most 4,096 rows run in the single
+thread-block-cluster launch; PRISM_AMG_TAIL_ROWS moves that threshold (it is
+read once per process, hence the subprocesses). With the whole hierarchy below
+the finest level in the cluster launch, with none of it, and with the default,
+the solutions must agree with the oracle within the solver tolerance of the
+other AMG tests, in FP64 and in mixed precision."""
 import json
 import os
 import subprocess
@@ -38,14 +37,13 @@ print(json.dumps(out))
 """
 
 
-def _run(tmp_path, rows, grid_rows=None):
-    path = str(tmp_path / f"tail{rows}_{grid_rows}")
+def _run(tmp_path, rows):
+    path = str(tmp_path / f"tail{rows}")
     env = dict(os.environ)
-    for key, v in (("PRISM_AMG_TAIL_ROWS", rows), ("PRISM_AMG_GRID_ROWS", grid_rows)):
-        if v is None:
-            env.pop(key, None)
-        else:
-            env[key] = str(v)
+    if rows is None:
+        env.pop("PRISM_AMG_TAIL_ROWS", None)
+    else:
+        env["PRISM_AMG_TAIL_ROWS"] = str(rows)
     r = subprocess.run([sys.executable, "-c", SCRIPT.format(root=ROOT, path=path)], env=env, cwd=ROOT,
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
@@ -58,9 +56,8 @@ def test_tail_threshold_does_not_change_the_solution(tmp_path, orc):
     from prism_b200 import api
     api.BiCGSTAB().solve(eqn, 1, 0.0)
     ref = T.values()
-    for rows, grid_rows in ((None, None), (0, 0), (10 ** 9, 0), (0, 10 ** 9), (None, 2000)):
-        for prec, ((status, its), sol) in _run(tmp_path, rows, grid_rows).items():
+    for rows in (None, 0, 10 ** 9):
+        for prec, ((status, its), sol) in _run(tmp_path, rows).items():
             err = cases.rel_l2(sol, ref)
-            print(f"tail rows {rows} grid rows {grid_rows} precision {prec}: {its} iterations, "
-                  f"rel L2 vs oracle {err:.2e}")
+            print(f"tail rows {rows} precision {prec}: {its} iterations, rel L2 vs oracle {err:.2e}")
             assert status == 0 and err < SOL_TOL
