@@ -11,13 +11,7 @@
 // The sweep is run level by level over the lower-neighbour dependency DAG
 // (level[c] = 1 + max level of its lower-numbered neighbours): cells of one level
 // never neighbour each other, so each cell reads exactly the values the
-// sequential sweep would read. Few levels: one launch per level; many (the
-// hyperplanes of a structured 3-D mesh: 382 at 128^3): one cooperative launch
-// with a grid barrier between levels.
-#include <cooperative_groups.h>
-
-#include <cstdlib>
-
+// sequential sweep would read. One launch per level, several lanes per cell.
 #include "devmath.cuh"
 #include "gradient.h"
 
@@ -49,63 +43,73 @@ __global__ void __launch_bounds__(256) ls_grad_kernel(const MeshView m, ScalarVi
     }
 }
 
-// gradient at a cell, read through L2 (values written by other blocks of the same launch)
-__device__ __forceinline__ D3 gradAtL2(const ScalarView& s, int c) {
-    return D3{__ldcg(s.g + c), __ldcg(s.g + s.gstride + c), __ldcg(s.g + 2 * s.gstride + c)};
-}
-
-// GreenGauss::computeGradAtCell (green_gauss.cpp:47-76) for cell c; L2: read the gradients
-// through L2 (the sweep kernel, where other blocks wrote them in this launch)
-template <bool L2>
-__device__ __forceinline__ void ggCell(const MeshView& m, const ScalarView& s, int c) {
-    const D3 xc = cellCenter(m, c);
-    const double phic = s.v[c];
-    const D3 gc = L2 ? gradAtL2(s, c) : gradAt(s, c);
-    D3 grad{0, 0, 0};
-    for (int q = m.cf_off[c]; q < m.cf_off[c + 1]; ++q) {
-        int f = m.cf_face[q];
-        if (f < m.nb) {
-            if (m.patch_empty[m.bpatch[f]]) continue;
-            double phi_b = scalarFace(m, s, f);
-            grad = grad + phi_b * areaVector(m, f);
-            continue;
-        }
-        int o = m.owner[f];
-        bool own = (o == c);
-        int n = own ? m.nbr[f] : o;
-        D3 Sf = areaVector(m, f);
-        if (!own) Sf = D3{-Sf.x, -Sf.y, -Sf.z};
-        double face_phi = 0.5 * (phic + s.v[n]);
-        D3 grad_sum = gc + (L2 ? gradAtL2(s, n) : gradAt(s, n));
-        D3 vec = faceCenter(m, f) - (0.5 * (xc + cellCenter(m, n)));
-        face_phi += 0.5 * dot(grad_sum, vec);
-        grad = grad + Sf * face_phi;
-    }
-    grad = grad / m.vol[c];
-    s.g[c] = grad.x;
-    s.g[s.gstride + c] = grad.y;
-    s.g[2 * s.gstride + c] = grad.z;
-}
-
+// GreenGauss::computeGradAtCell (green_gauss.cpp:47-76) for the cells of one dependency
+// level, GG_LPC lanes per cell: each lane evaluates one face's term (phi_b S_f on a
+// boundary face of a non-empty patch, S_f^out phi_f with the skewness correction on an
+// interior face; nothing on an empty patch) independently of the others, and the cell's
+// first lane adds the terms in the cell's face order, so the sum is the sequential
+// sweep's, term for term. The face terms' loads are in flight together instead of one
+// face after another.
+constexpr int GG_LPC = 8;
 __global__ void __launch_bounds__(256) gg_level_kernel(const MeshView m, ScalarView s, const int* __restrict__ cells,
                                                        int count) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    ggCell<false>(m, s, cells[t]);
-}
-
-// The whole sweep in one cooperative launch: the levels in order, separated by grid
-// barriers (every block is co-resident and takes every barrier), so level l reads the
-// gradients level l - 1 wrote exactly as the one-launch-per-level sweep does.
-__global__ void __launch_bounds__(256) gg_sweep_kernel(const MeshView m, ScalarView s, const int* __restrict__ cells,
-                                                       const int* __restrict__ level_off, int nlevels) {
-    namespace cg = cooperative_groups;
-    const int nthreads = (int)(gridDim.x * blockDim.x);
-    const int t0 = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    for (int l = 0; l < nlevels; ++l) {
-        const int end = level_off[l + 1];
-        for (int t = level_off[l] + t0; t < end; t += nthreads) ggCell<true>(m, s, cells[t]);
-        if (l + 1 < nlevels) cg::this_grid().sync();
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const int idx = gt / GG_LPC, sub = gt % GG_LPC;
+    const int lane = threadIdx.x & 31, lead = lane & ~(GG_LPC - 1);
+    const bool valid = idx < count;
+    const int c = valid ? cells[idx] : 0;
+    const int q0 = valid ? m.cf_off[c] : 0;
+    const int nq = valid ? m.cf_off[c + 1] - q0 : 0;
+    const int nq_max = __reduce_max_sync(0xffffffffu, (unsigned)nq);
+    D3 xc{0, 0, 0}, gc{0, 0, 0};
+    double phic = 0.0;
+    if (valid) {
+        xc = cellCenter(m, c);
+        phic = s.v[c];
+        gc = gradAt(s, c);
+    }
+    D3 grad{0, 0, 0};
+    for (int base = 0; base < nq_max; base += GG_LPC) {
+        const int q = base + sub;
+        D3 term{0, 0, 0};
+        int has = 0;
+        if (q < nq) {
+            const int f = m.cf_face[q0 + q];
+            if (f < m.nb) {
+                if (!m.patch_empty[m.bpatch[f]]) {
+                    double phi_b = scalarFace(m, s, f);
+                    term = phi_b * areaVector(m, f);
+                    has = 1;
+                }
+            } else {
+                const int o = m.owner[f];
+                const bool own = (o == c);
+                const int n = own ? m.nbr[f] : o;
+                D3 Sf = areaVector(m, f);
+                if (!own) Sf = D3{-Sf.x, -Sf.y, -Sf.z};
+                double face_phi = 0.5 * (phic + s.v[n]);
+                D3 grad_sum = gc + gradAt(s, n);
+                D3 vec = faceCenter(m, f) - (0.5 * (xc + cellCenter(m, n)));
+                face_phi += 0.5 * dot(grad_sum, vec);
+                term = Sf * face_phi;
+                has = 1;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < GG_LPC; ++k) {
+            const int src = lead + k;
+            const double tx = __shfl_sync(0xffffffffu, term.x, src);
+            const double ty = __shfl_sync(0xffffffffu, term.y, src);
+            const double tz = __shfl_sync(0xffffffffu, term.z, src);
+            const int h = __shfl_sync(0xffffffffu, has, src);
+            if (h) grad = grad + D3{tx, ty, tz};
+        }
+    }
+    if (valid && sub == 0) {
+        grad = grad / m.vol[c];
+        s.g[c] = grad.x;
+        s.g[s.gstride + c] = grad.y;
+        s.g[2 * s.gstride + c] = grad.z;
     }
 }
 
@@ -116,48 +120,13 @@ void launchLeastSquares(const MeshView& m, const ScalarView& s, const double* pi
     PB_LAUNCH("ls_grad_kernel");
 }
 
-// sweeps of more levels than this run as one cooperative launch (PRISM_GG_COOP_LEVELS; 0, the
-// default: never -- on the 128^3 mesh the grid barriers cost more than the launches they replace)
-int ggCoopLevels() {
-    static const int v = [] {
-        const char* e = std::getenv("PRISM_GG_COOP_LEVELS");
-        return e && e[0] ? std::max(0, std::atoi(e)) : 0;
-    }();
-    return v;
-}
-
 void launchGreenGauss(const MeshView& m, const ScalarView& s, const int* level_cells,
-                      const std::vector<int>& level_off, const int* level_off_dev, cudaStream_t st) {
-    const int nlevels = (int)level_off.size() - 1;
-    if (nlevels <= 0) return;
-    if (ggCoopLevels() > 0 && nlevels > ggCoopLevels() && level_off_dev) {
-        static const int blocks = [] {
-            int dev = 0, sms = 148, per = 1;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, gg_sweep_kernel, 256, 0) != cudaSuccess || per < 1)
-                per = 1;
-            cudaGetLastError();
-            return per * sms;
-        }();
-        cudaLaunchConfig_t cfg{};
-        cfg.gridDim = dim3((unsigned)blocks);
-        cfg.blockDim = dim3(256);
-        cfg.stream = st;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeCooperative;
-        at[0].val.cooperative = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        PB_CUDA(cudaLaunchKernelEx(&cfg, gg_sweep_kernel, m, s, level_cells, level_off_dev, nlevels));
-        countLaunch();
-        PB_LAUNCH("gg_sweep_kernel");
-        return;
-    }
-    for (int l = 0; l < nlevels; ++l) {
-        int count = level_off[l + 1] - level_off[l];
+                      const std::vector<int>& level_off, cudaStream_t st) {
+    for (size_t l = 0; l + 1 < level_off.size(); ++l) {
+        const int count = level_off[l + 1] - level_off[l];
         if (count == 0) continue;
-        gg_level_kernel<<<ceil_div(count, 256), 256, 0, st>>>(m, s, level_cells + level_off[l], count); countLaunch();
+        gg_level_kernel<<<ceil_div((int64_t)count * GG_LPC, 256), 256, 0, st>>>(m, s, level_cells + level_off[l],
+                                                                                count); countLaunch();
     }
     PB_LAUNCH("gg_level_kernel");
 }

@@ -11,7 +11,7 @@ namespace pb {
 void launchLeastSquares(const MeshView& m, const ScalarView& s, const double* pinv, const double* w, int64_t nk,
                         cudaStream_t st);
 void launchGreenGauss(const MeshView& m, const ScalarView& s, const int* level_cells,
-                      const std::vector<int>& level_off, const int* level_off_dev, cudaStream_t st);
+                      const std::vector<int>& level_off, cudaStream_t st);
 void launchScalarFaces(const MeshView& m, const ScalarView& s, double* out, cudaStream_t st);
 void launchVectorFlux(const MeshView& m, const VectorView& U, double* out, cudaStream_t st);
 

@@ -201,7 +201,6 @@ void setupDevice(Mesh& m) {
     std::vector<int> lc(m.nc), fill(m.level_off.begin(), m.level_off.end() - 1);
     for (int c = 0; c < m.nc; ++c) lc[fill[level[c]]++] = c;
     upload(m.level_cells, lc, s);
-    upload(m.level_off_dev, m.level_off, s);
     m.scratch.alloc(std::max(3 * m.nf, 1));
     m.ls_ready = false;
     m.points_ready = false;
@@ -330,7 +329,7 @@ void computeGradient(Scalar& s) {
         m.ensureLeastSquares();
         launchLeastSquares(m.view(), s.view(), m.ls_pinv.p, m.ls_w.p, (int64_t)m.h->cf_face.size(), m.stream);
     } else {
-        launchGreenGauss(m.view(), s.view(), m.level_cells.p, m.level_off, m.level_off_dev.p, m.stream);
+        launchGreenGauss(m.view(), s.view(), m.level_cells.p, m.level_off, m.stream);
     }
     s.grad->computed = s.event;
 }

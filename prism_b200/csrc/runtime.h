@@ -33,7 +33,7 @@ struct Mesh {
     DevBuf<double> area, nx, ny, nz, fx, fy, fz, cx, cy, cz, vol, gcw;
     PatternOutput pat;
     // Green-Gauss sweep schedule: cells grouped by dependency level
-    DevBuf<int> level_cells, level_off_dev;
+    DevBuf<int> level_cells;
     std::vector<int> level_off;
     // least-squares operators (built on first use, shared by every field)
     DevBuf<double> ls_pinv, ls_w;
