@@ -151,10 +151,16 @@ public:
     DevArena() = default;
     DevArena(const DevArena&) = delete;
     DevArena& operator=(const DevArena&) = delete;
+    // drains and frees on the device the chunks were taken on, whichever device is
+    // current at destruction (several meshes may live on several GPUs of one process)
     ~DevArena() {
         if (chunks_.empty()) return;
+        int cur = device_;
+        cudaGetDevice(&cur);
+        if (cur != device_) cudaSetDevice(device_);
         cudaDeviceSynchronize();
         for (auto& c : chunks_) cudaFree(c.p);
+        if (cur != device_) cudaSetDevice(cur);
     }
     template <typename T>
     T* take(size_t count, cudaStream_t s) {
@@ -167,6 +173,7 @@ public:
                 return reinterpret_cast<T*>(p);
             }
         size_t size = std::max(std::max(bytes, MIN_CHUNK), total_);
+        if (chunks_.empty()) PB_CUDA(cudaGetDevice(&device_));
         char* p = nullptr;
         PB_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), size, scratchPool(), s));
         chunks_.push_back({p, size});
@@ -191,6 +198,7 @@ private:
     static constexpr size_t MIN_CHUNK = size_t(2) << 20;
     std::vector<Chunk> chunks_;
     size_t cur_ = 0, off_ = 0, total_ = 0;
+    int device_ = 0;  // device current when the first chunk was taken
 };
 
 // A buffer inside a DevArena: the arena owns the memory, so release() only
@@ -233,6 +241,14 @@ inline bool verbose() {
     static const bool v = [] {
         const char* e = std::getenv("PRISM_VERBOSE");
         return e && e[0] && e[0] != '0';
+    }();
+    return v;
+}
+// PRISM_VERBOSE=2: also every reliable update and restart of the mixed-precision solver
+inline int verboseLevel() {
+    static const int v = [] {
+        const char* e = std::getenv("PRISM_VERBOSE");
+        return e && e[0] ? std::atoi(e) : 0;
     }();
     return v;
 }

@@ -208,15 +208,12 @@ void setupDevice(Mesh& m) {
 }
 }  // namespace
 
-std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d) {
-    auto mesh = std::make_unique<Mesh>();
-    mesh->h = buildHostMesh(d);
-    const HostMesh& h = *mesh->h;
+// The CSR and SELL-32 patterns number their entries with 32-bit ints: bound both for the
+// current cell numbering (a row holds the cell and at most one entry per interior face of
+// the cell; SELL pads every 32-row slice to its longest row, so the count depends on the
+// numbering and is checked again after a renumbering).
+void checkPatternBounds(const HostMesh& h) {
     constexpr int64_t LIMIT = int64_t(1) << 31;
-    if (h.nc >= LIMIT || h.nf >= LIMIT || (int64_t)h.cf_face.size() >= LIMIT)
-        fail(PRISM_INVALID_MESH, "mesh too large for 32-bit indices");
-    // the CSR and SELL-32 patterns number their entries with 32-bit ints: bound both
-    // (a row holds the cell and at most one entry per interior face of the cell)
     int64_t nnz = 0, sell = 0;
     for (int64_t s0 = 0; s0 < h.nc; s0 += 32) {
         int64_t width = 0;
@@ -229,6 +226,16 @@ std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d) {
         sell += 32 * width;
     }
     if (nnz >= LIMIT || sell >= LIMIT) fail(PRISM_INVALID_MESH, "matrix pattern too large for 32-bit indices");
+}
+
+std::unique_ptr<Mesh> createMesh(const PrismUnvMesh* d) {
+    auto mesh = std::make_unique<Mesh>();
+    mesh->h = buildHostMesh(d);
+    const HostMesh& h = *mesh->h;
+    constexpr int64_t LIMIT = int64_t(1) << 31;
+    if (h.nc >= LIMIT || h.nf >= LIMIT || (int64_t)h.cf_face.size() >= LIMIT)
+        fail(PRISM_INVALID_MESH, "mesh too large for 32-bit indices");
+    checkPatternBounds(h);
     PB_CUDA(cudaStreamCreateWithFlags(&mesh->stream, cudaStreamNonBlocking));
     setupDevice(*mesh);
     return mesh;
@@ -242,6 +249,7 @@ void reorderMesh(Mesh& m, bool reverse) {
     std::vector<int64_t> perm = cuthillMckee(*m.h);
     if (reverse) std::reverse(perm.begin(), perm.end());
     permuteCells(*m.h, perm);
+    checkPatternBounds(*m.h);
     setupDevice(m);
 }
 

@@ -6,7 +6,8 @@
 //   * every buffer is 256-byte aligned and lies inside one chunk;
 //   * no two live buffers overlap;
 //   * chunks grow geometrically (few pool calls per build);
-//   * the destructor returns every chunk.
+//   * the destructor returns every chunk, on the device the arena took them on,
+//     and leaves the caller's current device current.
 #include "../../prism_b200/csrc/common.h"
 
 #include <cstdio>
@@ -15,8 +16,10 @@
 
 namespace {
 std::map<char*, size_t> g_chunks;
+std::map<char*, int> g_chunk_device;
 long g_pool_calls = 0;
 int g_failures = 0;
+int g_device = 0;  // the fake current device
 
 void check(bool ok, const char* what) {
     if (!ok && g_failures++ < 10) std::fprintf(stderr, "FAILED: %s\n", what);
@@ -27,17 +30,24 @@ extern "C" {
 cudaError_t cudaMallocFromPoolAsync(void** p, size_t size, cudaMemPool_t, cudaStream_t) {
     *p = std::aligned_alloc(256, (size + 255) / 256 * 256);
     g_chunks[static_cast<char*>(*p)] = size;
+    g_chunk_device[static_cast<char*>(*p)] = g_device;
     ++g_pool_calls;
     return cudaSuccess;
 }
 cudaError_t cudaFree(void* p) {
     check(g_chunks.erase(static_cast<char*>(p)) == 1, "free of an unknown chunk");
+    check(g_chunk_device[static_cast<char*>(p)] == g_device, "chunk freed with its own device current");
+    g_chunk_device.erase(static_cast<char*>(p));
     std::free(p);
     return cudaSuccess;
 }
 cudaError_t cudaDeviceSynchronize() { return cudaSuccess; }
 cudaError_t cudaGetDevice(int* d) {
-    *d = 0;
+    *d = g_device;
+    return cudaSuccess;
+}
+cudaError_t cudaSetDevice(int d) {
+    g_device = d;
     return cudaSuccess;
 }
 cudaError_t cudaMemPoolCreate(cudaMemPool_t* p, const cudaMemPoolProps*) {
@@ -55,6 +65,8 @@ int main() {
     std::mt19937_64 rng(7);
     long builds = 0;
     for (int trial = 0; trial < 200; ++trial) {
+        // every third arena lives on device 1 and is destroyed while device 0 is current
+        g_device = (trial % 3 == 0) ? 1 : 0;
         {
             pb::DevArena arena;
             struct Live {
@@ -95,8 +107,10 @@ int main() {
                     n = n / 4 + 1;
                 }
             }
+            g_device = 0;
         }
         check(g_chunks.empty(), "destructor returns every chunk");
+        check(g_device == 0, "destructor restores the current device");
     }
     const double per_build = double(g_pool_calls) / double(builds);
     check(per_build < 4.0, "few pool calls per build");
