@@ -10,7 +10,8 @@ launch (PrismSolveOpts.graph: the solver loops are device-side conditional nodes
 and the kernels are those of the ordinary path, so the fields are identical).
 Inputs live in HBM; the working set (~1 GB) is larger than L2, so no flush is
 needed. The same steps on the ordinary path (every kernel launched from the host)
-are reported as "simple_eager", with the live bandwidth samples.
+are reported as "simple_eager", with the live bandwidth samples, and the same solver
+timed again after --late-steps more iterations as "simple_later" (the developed flow).
 
 Also reported: time to 1e-8 relative error of the 128^3 jittered-hex transport
 solve (MUSCL + Corrected + Green-Gauss, one step() of the system assembled at
@@ -417,6 +418,26 @@ def run_ours(args, world, rank, local):
     t_dev = max_over_ranks(world, g0.elapsed_time(g1) / 1000.0)
     value = world * args.steps / t_dev
 
+    # later in the run: the same solver continued for late_steps untimed steps (the pressure
+    # solves cost differently once the flow has developed), then steps timed again
+    late = None
+    if args.late_steps > 0:
+        for _ in range(args.late_steps):
+            gsimple.step(eqs, U, mdot, p)
+        torch.cuda.synchronize()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record()
+        late_reports = []
+        for _ in range(args.steps):
+            late_reports = gsimple.step(eqs, U, mdot, p)
+        l1.record()
+        torch.cuda.synchronize()
+        t_late = max_over_ranks(world, l0.elapsed_time(l1) / 1000.0)
+        late = {"value": world * args.steps / t_late, "unit": UNIT, "ms_per_step": 1000.0 * t_late / args.steps,
+                "timed_after_iterations": args.warmup + args.steps + args.late_steps,
+                "last_step_reports": [(r.field_name, r.n_iterations, r.initial_residual, r.final_residual)
+                                      for r in late_reports]}
+
     # end to end through the public API with pinned host buffers, same initial state
     U, p, nu, mdot, eqs = fresh()
     for _ in range(args.warmup):
@@ -567,7 +588,7 @@ def run_ours(args, world, rank, local):
                                      "kernels, counted there over the same number of steps",
                 "graph_launches": int(gprof.graph_launches), "cpu_baseline": cpu,
                 "last_step_reports": [(r.field_name, r.n_iterations) for r in reports],
-                "simple_eager": eager_line}
+                "simple_eager": eager_line, "simple_later": late}
         line.update(extra)
         print(json.dumps(line), flush=True)
 
@@ -584,6 +605,8 @@ def main():
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--ref-n", type=int, default=N_CAVITY, help="cavity size of the reference arm (tests only)")
+    ap.add_argument("--late-steps", type=int, default=175,
+                    help="untimed steps before the second timing of the SIMPLE run (0: skip it)")
     args = ap.parse_args()
     world, rank, local = dist_init(args)
     try:

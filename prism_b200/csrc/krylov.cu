@@ -141,10 +141,9 @@ int waveGrid(K kernel, int needed) {
 // STAGE 0: plain; 1: alpha = rho / (u.y); 2: w = (u.y)/(y.y)
 // The columns and values of up to 8 slots are loaded before their gathers, so
 // a row's loads are all in flight at once; the sum runs over the slots in order.
-template <typename T>
+template <typename T, int W = 8>
 __device__ __forceinline__ T sliceRow(const int* __restrict__ col, const T* __restrict__ val,
                                       const T* __restrict__ x, int b, int width, int lane) {
-    constexpr int W = 8;
     T sum = 0;
     for (int j0 = 0; j0 < width; j0 += W) {
         int c[W];
@@ -162,8 +161,8 @@ __device__ __forceinline__ T sliceRow(const int* __restrict__ col, const T* __re
     return sum;
 }
 
-template <typename T, int STAGE>
-__global__ void __launch_bounds__(BS, 5) spmv_kernel(int nslices, int n, const int* __restrict__ sl_off,
+template <typename T, int STAGE, int W = 8, int MINB = 5>
+__global__ void __launch_bounds__(BS, MINB) spmv_kernel(int nslices, int n, const int* __restrict__ sl_off,
                                                   const int* __restrict__ col, const T* __restrict__ val,
                                                   const T* __restrict__ x, T* __restrict__ y,
                                                   const T* __restrict__ u, double* partials,
@@ -175,7 +174,7 @@ __global__ void __launch_bounds__(BS, 5) spmv_kernel(int nslices, int n, const i
     for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
         const int b = sl_off[sl];
         const int width = (sl_off[sl + 1] - b) >> 5;
-        const T sum = sliceRow<T>(col, val, x, b, width, lane);
+        const T sum = sliceRow<T, W>(col, val, x, b, width, lane);
         const int r = sl * 32 + lane;
         y[r] = sum;
         if (STAGE != 0 && r < n) {
@@ -598,13 +597,40 @@ inline void precApply(Amg* amg, const float* r, float* z, const KState* S, cudaS
 
 // `count` BiCGSTAB iterations on the operator M (SELL values), launched one
 // kernel at a time. With amg: right-preconditioned, y = M^-1 p and z = M^-1 s.
+// launch shape of the reducing SpMV stages: W slots loaded ahead per lane, at least MINB
+// blocks per SM. Measured on the 128^3 transport matrix (ncu, FP64): 4x6 (40 registers,
+// 71% warps active) 45 / 43 us for the two stages against 47 / 53 us for 8x5 (48
+// registers, 60%) and 52 / 50 us for 4x8 (32 registers, 97%). PRISM_SPMV_SHAPE = "WxMINB"
+// (4x6, 8x5, 4x8) overrides it.
+int spmvShape() {
+    static const int v = [] {
+        const char* e = std::getenv("PRISM_SPMV_SHAPE");
+        if (!e || !e[0]) return 3;
+        const std::string t(e);
+        return t == "4x8" ? 1 : t == "8x5" ? 0 : 3;
+    }();
+    return v;
+}
+template <typename T, int STAGE, typename F>
+void withSpmvShape(F&& f) {
+    switch (spmvShape()) {
+        case 0: f(spmv_kernel<T, STAGE, 8, 5>); break;
+        case 1: f(spmv_kernel<T, STAGE, 4, 8>); break;
+        default: f(spmv_kernel<T, STAGE, 4, 6>); break;
+    }
+}
+
 template <typename T>
 void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, long long count, bool sample,
                   KrylovWork& w, cudaStream_t s) {
     KState* S = w.state.p;
     const int n = A.n, vg = vecGrid(n);
-    const int sg1 = waveGrid(spmv_kernel<T, 1>, ceil_div(A.nslices, WARPS));
-    const int sg2 = waveGrid(spmv_kernel<T, 2>, ceil_div(A.nslices, WARPS));
+    decltype(&spmv_kernel<T, 1>) k1 = nullptr;
+    decltype(&spmv_kernel<T, 2>) k2 = nullptr;
+    withSpmvShape<T, 1>([&](auto k) { k1 = k; });
+    withSpmvShape<T, 2>([&](auto k) { k2 = k; });
+    const int sg1 = waveGrid(k1, ceil_div(A.nslices, WARPS));
+    const int sg2 = waveGrid(k2, ceil_div(A.nslices, WARPS));
     for (long long it = 0; it < count; ++it) {
         launchPdl(p_kernel<T>, vg, BS, s, n, V.p, V.r, V.v, S);
         const T* dp = V.p;
@@ -613,7 +639,7 @@ void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T*
             dp = y;
         }
         const int slot = sample ? profBegin(PROF_SPMV, sizeof(T) == 4, spmvBytes<T>(A), s) : -1;
-        launchPdl(spmv_kernel<T, 1>, sg1, BS, s, A.nslices, n, A.sl_off, A.col, M, dp, V.v, V.r0, w.partials.p,
+        launchPdl(k1, sg1, BS, s, A.nslices, n, A.sl_off, A.col, M, dp, V.v, V.r0, w.partials.p,
                   w.counter.p, S);
         profEnd(slot, s);
         launchPdl(s_kernel<T>, vg, BS, s, n, V.s, V.r, V.v, S);
@@ -622,7 +648,7 @@ void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T*
             precApply(amg, V.s, z, S, s, sample);
             ds = z;
         }
-        launchPdl(spmv_kernel<T, 2>, sg2, BS, s, A.nslices, n, A.sl_off, A.col, M, ds, V.t, V.s, w.partials.p,
+        launchPdl(k2, sg2, BS, s, A.nslices, n, A.sl_off, A.col, M, ds, V.t, V.s, w.partials.p,
                   w.counter.p, S);
         launchPdl(xr_kernel<T>, vg, BS, s, n, V.x, V.r, dp, ds, V.s, V.t, V.r0, w.partials.p, w.counter.p, S);
     }
@@ -744,6 +770,21 @@ KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, 
 
 }  // namespace
 
+// Mixed precision: the FP32 recurrence restarts from the FP64 solution at every reliable
+// update (r0 = the true residual, fresh directions), which measured fewer iterations than
+// continuing it (128^2 Poisson with Jacobi: 364 against 662; 128^3 transport with AMG: 124
+// against 132) -- continuing it also stalled for 14,000 iterations on the Poisson problem.
+// PRISM_MIXED_RESTART=0 continues it instead. Either way a segment longer than kStallFactor
+// x the longest earlier one (and than kStallMin iterations) is restarted.
+constexpr long long kStallMin = 64, kStallFactor = 8;
+bool restartOnUpdate() {
+    static const bool v = [] {
+        const char* e = std::getenv("PRISM_MIXED_RESTART");
+        return !(e && e[0] == '0');
+    }();
+    return v;
+}
+
 KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, int precision,
                    double inner_tol, KrylovWork& w, cudaStream_t s, Amg* amg, const int* rowptr, const int* col) {
     const bool mixed = precision == PRISM_PREC_MIXED;
@@ -825,12 +866,22 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
         PB_LAUNCH("reliable update");
         PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
         PB_CUDA(cudaStreamSynchronize(s));
+        if (verboseLevel() >= 2)
+            std::fprintf(stderr, "[prism] mixed %s at iteration %lld: true rel residual %.3e, done %d\n",
+                         first ? "restart" : "reliable update", w.host_state->iter,
+                         w.host_state->bb > 0 ? std::sqrt(w.host_state->rr / w.host_state->bb) : 0.0,
+                         w.host_state->done);
         return w.host_state->done;
     };
     fill_zero_f<<<gn, BS, 0, s>>>(n, w.x32.p); countLaunch();
     int done = reliable(1);
-    int restarts = 0, n_reliable = 0;
+    int restarts = 0, n_reliable = 0, stalls = 0;
     long long batch = 8;
+    // iterations of the current segment (since the last reliable update or restart) and the
+    // longest segment so far: a segment far longer than every earlier one has stalled (the
+    // FP32 recurrence stops reducing its residual), and restarting it from the current
+    // FP64 solution recovers the convergence rate
+    long long seg_start = 0, longest = 0;
     Vecs<float> V32{w.x32.p, w.r32.p, w.r032.p, w.p32.p, w.v32.p, w.s32.p, w.t32.p};
     bool first = true;
     while (done == 0) {
@@ -840,13 +891,29 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
         PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
         PB_CUDA(cudaStreamSynchronize(s));
         done = w.host_state->done;
+        const long long seg = w.host_state->iter - seg_start;
         if (done == 0) {
+            if (seg > std::max(kStallMin, kStallFactor * longest) && stalls < 20) {
+                ++stalls;
+                longest = std::max(longest, seg);
+                seg_start = w.host_state->iter;
+                flush_kernel<<<gn, BS, 0, s>>>(n, X, w.x32.p); countLaunch();
+                done = reliable(1);
+                continue;
+            }
             batch = std::min<long long>(batch * 2, 64);
             continue;
         }
+        longest = std::max(longest, seg);
+        seg_start = w.host_state->iter;
         if (done == 6) {
             ++n_reliable;
-            done = reliable(0);
+            if (restartOnUpdate()) {
+                flush_kernel<<<gn, BS, 0, s>>>(n, X, w.x32.p); countLaunch();
+                done = reliable(1);
+            } else {
+                done = reliable(0);
+            }
             continue;
         }
         if (done == 3) {  // breakdown of the recurrence: flush and restart from the current x
@@ -875,8 +942,8 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
     finish();
     if (verbose())
         std::fprintf(stderr, "[prism] bicgstab fp32+fp64 n=%d: %lld iterations, %d reliable updates, %d restarts, "
-                     "rel residual %.3e, status %d\n", n, out.iterations, n_reliable, restarts, out.rel_residual,
-                     out.status);
+                     "%d stalled segments restarted, rel residual %.3e, status %d\n", n, out.iterations, n_reliable,
+                     restarts, stalls, out.rel_residual, out.status);
     return out;
 }
 
