@@ -18,7 +18,11 @@
 //   * cycle: V(1,1), damped Jacobi (omega = 0.9) smoothing, coarse correction
 //     scaled by 1.8, or 2.0 for the pressure correction (unsmoothed aggregation
 //     under-corrects), dense inverse
-//     (single-block Gauss-Jordan with partial pivoting) on the coarsest level.
+//     (single-block Gauss-Jordan with partial pivoting) on the coarsest level;
+//   * K-cycle (applyK, for the flexible-CG solve of the pressure correction):
+//     on the levels Amg::kLevel names, the coarse correction is two
+//     flexible-CG steps preconditioned by cycles from that level instead of
+//     one over-corrected cycle (see k_first_kernel).
 // The hierarchy's structure is built once per matrix pattern and reused; every
 // solve refreshes the values from the current matrix.
 #include <cooperative_groups.h>
@@ -31,6 +35,7 @@
 #include <type_traits>
 
 #include "amg.h"
+#include "reduce.cuh"
 
 namespace pb {
 
@@ -432,6 +437,124 @@ __global__ void __launch_bounds__(BS) post_kernel(int n, const int* __restrict__
     }
 }
 
+// ---- K-cycle (FP64): two flexible-CG steps on a coarse level
+// (Notay and Vassilevski 2008, the K-cycle of AGMG). With rc the restricted
+// residual and B one cycle from the coarse level:
+//   z1 = B rc ; q1 = A z1 ; a1 = (z1.rc)/(z1.q1) ; r1 = rc - a1 q1
+//   z2 = B r1 ; gamma = z2.q1 ; beta = z2.(A z2) ; rho2 = z2.r1
+//   a2 = rho2 / (beta - gamma^2/(z1.q1)) ; e = (a1 - a2 gamma/(z1.q1)) z1 + a2 z2
+// (the second direction is z2 made A-orthogonal to z1); the fine level then
+// adds the prolongated e without the V-cycle's over-correction factor. The
+// scalars of a level sit in 8 doubles of Amg::kscal.
+enum { KS_RHO1 = 0, KS_ALPHA1 = 1, KS_A1 = 2, KS_C1 = 3, KS_C2 = 4, KS_N = 8 };
+constexpr int K_MAX_GRID = NUM_SMS * 8;  // reducing K-cycle kernels: grid-stride over at most this many blocks
+
+inline int kGrid(int64_t rows, int lpr) { return std::max(1, std::min<int>(ceil_div(rows * lpr, BS), K_MAX_GRID)); }
+
+// q1 = A z1 ; z1.rc, z1.q1 -> a1
+template <int LPR>
+__global__ void __launch_bounds__(BS) k_first_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
+                                                     const double* __restrict__ val, const double* __restrict__ z1,
+                                                     const double* __restrict__ rc, double* __restrict__ q1,
+                                                     double* partials, unsigned int* counter, double* ks,
+                                                     const KState* S) {
+    pdlEnter();
+    if (S && S->done) return;
+    const int64_t total = (int64_t)n * LPR;
+    double d0 = 0.0, d1 = 0.0;
+    for (int64_t base = (int64_t)blockIdx.x * BS; base < total; base += (int64_t)gridDim.x * BS) {
+        const int64_t gt = base + threadIdx.x;
+        const bool valid = gt < total;
+        const int row = (int)(gt / LPR), sub = (int)(gt % LPR);
+        const double sum = rowSum<double, LPR>(sl_off, col, val, row, valid, sub, [&](int c) { return z1[c]; });
+        if (valid && sub == 0) {
+            q1[row] = sum;
+            d0 += z1[row] * rc[row];
+            d1 += z1[row] * sum;
+        }
+    }
+    double v[2] = {d0, d1}, out[2];
+    if (reduceLast<2, false>(v, partials, counter, out) && threadIdx.x == 0) {
+        ks[KS_RHO1] = out[0];
+        ks[KS_ALPHA1] = out[1];
+        ks[KS_A1] = (out[1] > 0.0 && isfinite(out[0])) ? out[0] / out[1] : 0.0;
+    }
+}
+
+// r1 = rc - a1 q1
+__global__ void k_residual_kernel(int n, const double* __restrict__ rc, const double* __restrict__ q1,
+                                  const double* __restrict__ ks, double* __restrict__ r1, const KState* S) {
+    pdlEnter();
+    if (S && S->done) return;
+    const double a1 = ks[KS_A1];
+    const int i = blockIdx.x * BS + threadIdx.x;
+    if (i < n) r1[i] = rc[i] - a1 * q1[i];
+}
+
+// z2.q1, z2.(A z2), z2.r1 -> the combination coefficients c1, c2 of z1, z2
+// (a non-positive denominator keeps the first step alone: c1 = a1, c2 = 0)
+template <int LPR>
+__global__ void __launch_bounds__(BS) k_second_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
+                                                      const double* __restrict__ val, const double* __restrict__ z2,
+                                                      const double* __restrict__ q1, const double* __restrict__ r1,
+                                                      double* partials, unsigned int* counter, double* ks,
+                                                      const KState* S) {
+    pdlEnter();
+    if (S && S->done) return;
+    const int64_t total = (int64_t)n * LPR;
+    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+    for (int64_t base = (int64_t)blockIdx.x * BS; base < total; base += (int64_t)gridDim.x * BS) {
+        const int64_t gt = base + threadIdx.x;
+        const bool valid = gt < total;
+        const int row = (int)(gt / LPR), sub = (int)(gt % LPR);
+        const double sum = rowSum<double, LPR>(sl_off, col, val, row, valid, sub, [&](int c) { return z2[c]; });
+        if (valid && sub == 0) {
+            const double zi = z2[row];
+            d0 += zi * q1[row];
+            d1 += zi * sum;
+            d2 += zi * r1[row];
+        }
+    }
+    double v[3] = {d0, d1, d2}, out[3];
+    if (reduceLast<3, false>(v, partials, counter, out) && threadIdx.x == 0) {
+        const double a1 = ks[KS_A1], al1 = ks[KS_ALPHA1];
+        double c1 = a1, c2 = 0.0;
+        if (al1 > 0.0) {
+            const double den = out[1] - out[0] * out[0] / al1;
+            const double a2 = out[2] / den;
+            if (den > 0.0 && isfinite(a2)) {
+                c2 = a2;
+                c1 = a1 - a2 * out[0] / al1;
+            }
+        }
+        ks[KS_C1] = c1;
+        ks[KS_C2] = c2;
+    }
+}
+
+// prolongation of a K-cycle correction and post-smoothing:
+// out = xp + omega D^-1 (b - A xp), xp = x + (c1 z1 + c2 z2)[agg]
+template <int LPR>
+__global__ void __launch_bounds__(BS) post_k_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
+                                                    const double* __restrict__ val, const double* __restrict__ b,
+                                                    const double* __restrict__ x, const double* __restrict__ z1,
+                                                    const double* __restrict__ z2, const int* __restrict__ agg,
+                                                    const double* __restrict__ ks, const double* __restrict__ dinv,
+                                                    double omega, double* __restrict__ out, const KState* S) {
+    pdlEnter();
+    if (S && S->done) return;
+    const double c1 = ks[KS_C1], c2 = ks[KS_C2];
+    const int gt = blockIdx.x * BS + threadIdx.x;
+    const int row = gt / LPR, sub = gt % LPR;
+    const bool valid = row < n;
+    auto xp = [&](int c) {
+        const int a = agg[c];
+        return x[c] + (c1 * z1[a] + c2 * z2[a]);
+    };
+    const double sum = rowSum<double, LPR>(sl_off, col, val, row, valid, sub, xp);
+    if (valid && sub == 0) out[row] = xp(row) + omega * dinv[row] * (b[row] - sum);
+}
+
 // damped Jacobi sweep (coarsest level without a dense inverse): out = x + omega D^-1 (b - A x)
 template <typename T>
 __global__ void smooth0_kernel(int n, T* x, const T* b, const T* dinv, T omega, const KState* S) {
@@ -795,7 +918,7 @@ void members(DevArena& ar, AmgLevel& L, int nc, cudaStream_t s) {
 }
 
 // returns true if a buffer was allocated
-bool allocCycle(DevArena& ar, AmgLevel& L, bool mixed, cudaStream_t s) {
+bool allocCycle(DevArena& ar, AmgLevel& L, bool mixed, bool klevel, cudaStream_t s) {
     bool fresh = false;
     int np = L.nslices * 32;
     for (auto* b : {&L.b, &L.x, &L.x2, &L.res, &L.dinv})
@@ -804,6 +927,13 @@ bool allocCycle(DevArena& ar, AmgLevel& L, bool mixed, cudaStream_t s) {
             b->zero(s);
             fresh = true;
         }
+    if (klevel)
+        for (auto* b : {&L.kz2, &L.kq1, &L.kr1})
+            if (!b->p) {
+                b->alloc(ar, np, s);
+                b->zero(s);
+                fresh = true;
+            }
     if (mixed) {
         for (auto* b : {&L.b32, &L.x32, &L.x232, &L.res32, &L.dinv32})
             if (!b->p) {
@@ -831,6 +961,17 @@ uint64_t nextGeneration() {
 }
 }  // namespace
 
+void Amg::forPressure() {
+    scale = 2.0;
+    flex_scale = 2.2;
+    const char* e = std::getenv("PRISM_AMG_KCYCLE");
+    k_levels = e && e[0] ? std::max(0, std::atoi(e)) : 0;
+}
+
+bool Amg::kLevel(size_t l) const {
+    return k_levels > 0 && l >= 1 && l <= (size_t)k_levels && l + 1 < levels.size() && (tail < 0 || (int)l < tail);
+}
+
 void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mixed, cudaStream_t s) {
     if (!built || levels.empty() || levels[0]->n != A.n || levels[0]->sl_off != A.sl_off) {
         levels.clear();
@@ -838,6 +979,9 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
         coarse_inv.release();
         coarse_inv32.release();
         coarse_bad.release();
+        kscal.release();
+        kpart.release();
+        kcount.release();
         arena.reset();  // stream order keeps earlier work on the old hierarchy ahead of its reuse
         auto L0 = std::make_unique<AmgLevel>();
         L0->n = A.n;
@@ -924,14 +1068,23 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
         // smoother weight and coarse-correction factor (PRISM_AMG_OMEGA / PRISM_AMG_SCALE override them)
         if (const char* e = std::getenv("PRISM_AMG_OMEGA")) omega = std::atof(e);
         if (const char* e = std::getenv("PRISM_AMG_SCALE")) scale = std::atof(e);
+        if (const char* e = std::getenv("PRISM_AMG_FLEX_SCALE")) flex_scale = std::atof(e);
         built = true;
         generation = nextGeneration();
     } else if (levels[0]->vals != A.vals) {
         levels[0]->vals = A.vals;
         generation = nextGeneration();
     }
-    for (auto& L : levels)
-        if (allocCycle(arena, *L, mixed, s)) generation = nextGeneration();
+    for (size_t l = 0; l < levels.size(); ++l)
+        if (allocCycle(arena, *levels[l], mixed, kLevel(l), s)) generation = nextGeneration();
+    if (k_levels > 0 && !kscal.p) {
+        kscal.alloc(arena, (size_t)KS_N * MAX_LEVELS, s);
+        kscal.zero(s);
+        kpart.alloc(arena, (size_t)K_MAX_GRID * 4, s);
+        kcount.alloc(arena, 1, s);
+        kcount.zero(s);
+        generation = nextGeneration();
+    }
     if (mixed && coarse_inv.p && !coarse_inv32.p) {
         coarse_inv32.alloc(arena, coarse_inv.n, s);
         generation = nextGeneration();
@@ -983,7 +1136,32 @@ Bufs<double> bufs64(AmgLevel& L) { return {L.b.p, L.x.p, L.x2.p, L.res.p, L.dinv
 Bufs<float> bufs32(AmgLevel& L) { return {L.b32.p, L.x32.p, L.x232.p, L.res32.p, L.dinv32.p}; }
 
 template <typename T>
-void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s, bool sample) {
+void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s, bool sample, bool kc);
+
+// K-cycle on level k (FP64): z1 = N.x2 and z2 = N.kz2 from two cycles, the
+// combination coefficients in the level's scalars (see k_first_kernel)
+void kStep(Amg& A, size_t k, const KState* S, cudaStream_t s) {
+    AmgLevel& N = *A.levels[k];
+    double* ks = A.kscal.p + (size_t)KS_N * k;
+    vcycle<double>(A, k, N.b.p, N.x2.p, S, s, false, true);
+    withLpr(N.lpr, [&](auto c) {
+        constexpr int P = decltype(c)::value;
+        launchPdl(k_first_kernel<P>, kGrid(N.n, P), BS, s, N.n, N.sl_off, N.sl_col, N.vals,
+                  (const double*)N.x2.p, (const double*)N.b.p, N.kq1.p, A.kpart.p, A.kcount.p, ks, S);
+    });
+    launchPdl(k_residual_kernel, grid(N.n), BS, s, N.n, (const double*)N.b.p, (const double*)N.kq1.p,
+              (const double*)ks, N.kr1.p, S);
+    vcycle<double>(A, k, N.kr1.p, N.kz2.p, S, s, false, true);
+    withLpr(N.lpr, [&](auto c) {
+        constexpr int P = decltype(c)::value;
+        launchPdl(k_second_kernel<P>, kGrid(N.n, P), BS, s, N.n, N.sl_off, N.sl_col, N.vals,
+                  (const double*)N.kz2.p, (const double*)N.kq1.p, (const double*)N.kr1.p, A.kpart.p, A.kcount.p,
+                  ks, S);
+    });
+}
+
+template <typename T>
+void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s, bool sample, bool kc) {
     AmgLevel& L = *A.levels[l];
     auto B = [&](AmgLevel& X) {
         if constexpr (sizeof(T) == 8) return bufs64(X);
@@ -998,7 +1176,7 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
             else P.inv = A.coarse_inv32.p;
         }
         P.omega = (T)A.omega;
-        P.scale = (T)A.scale;
+        P.scale = (T)(kc ? A.flex_scale : A.scale);
         P.S = S;
         for (int k = 0; k < P.nlev; ++k) {
             AmgLevel& X = *A.levels[l + k];
@@ -1061,14 +1239,28 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
     profEnd(slot, s);
     launchPdl(restrict_kernel<T>, grid(N.n), BS, s, N.n, (const int*)L.m_off.p, (const int*)L.m_idx.p,
               (const T*)lb.res, nb.b, S);
-    vcycle<T>(A, l + 1, nb.b, nb.x2, S, s, false);
+    if constexpr (sizeof(T) == 8) {
+        if (kc && A.kLevel(l + 1)) {
+            kStep(A, l + 1, S, s);
+            slot = fine ? profBegin(PROF_AMG_POST, false, mat_bytes + 36.0 * L.n + 16.0 * N.n, s) : -1;
+            withLpr(L.lpr, [&](auto c) {
+                constexpr int P = decltype(c)::value;
+                launchPdl(post_k_kernel<P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b,
+                          (const double*)lb.x, (const double*)nb.x2, (const double*)N.kz2.p, (const int*)L.agg.p,
+                          (const double*)(A.kscal.p + (size_t)KS_N * (l + 1)), lb.dinv, omega, out, S);
+            });
+            profEnd(slot, s);
+            return;
+        }
+    }
+    vcycle<T>(A, l + 1, nb.b, nb.x2, S, s, false, kc);
     slot = fine ? profBegin(PROF_AMG_POST, sizeof(T) == 4,
                             mat_bytes + (4.0 * sizeof(T) + 4.0) * L.n + (double)sizeof(T) * N.n, s)
                 : -1;
     withLpr(L.lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
         launchPdl(post_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, lb.x, nb.x2,
-                  L.agg.p, (T)A.scale, lb.dinv, omega, out, S);
+                  L.agg.p, (T)(kc ? A.flex_scale : A.scale), lb.dinv, omega, out, S);
     });
     profEnd(slot, s);
 }
@@ -1076,10 +1268,14 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
 }  // namespace
 
 void Amg::apply(const double* r, double* z, const KState* S, cudaStream_t s, bool sample) {
-    vcycle<double>(*this, 0, r, z, S, s, sample);
+    vcycle<double>(*this, 0, r, z, S, s, sample, false);
 }
-void Amg::apply32(const float* r, float* z, const KState* S, cudaStream_t s) {
-    vcycle<float>(*this, 0, r, z, S, s, false);
+void Amg::apply32(const float* r, float* z, const KState* S, cudaStream_t s, bool flexible) {
+    vcycle<float>(*this, 0, r, z, S, s, false, flexible);
+}
+void Amg::applyK(const double* r, double* z, const KState* S, cudaStream_t s, bool sample) {
+    if (k_levels > 0 && !kscal.p) fail(PRISM_INTERNAL, "K-cycle without its buffers (setup first)");
+    vcycle<double>(*this, 0, r, z, S, s, sample, true);
 }
 
 }  // namespace pb

@@ -1,4 +1,4 @@
-// amg.h -- aggregation algebraic multigrid preconditioner for BiCGSTAB.
+// amg.h -- aggregation algebraic multigrid preconditioner for BiCGSTAB and flexible CG.
 #pragma once
 
 #include <memory>
@@ -39,6 +39,8 @@ struct AmgLevel {
     // cycle vectors (FP64 and FP32)
     ArenaBuf<double> b, x, x2, res;
     ArenaBuf<float> b32, x32, x232, res32;
+    // K-cycle level (Amg::kLevel): second cycle's result, A z1 and the residual r1
+    ArenaBuf<double> kz2, kq1, kr1;
 };
 
 struct Amg {
@@ -54,9 +56,23 @@ struct Amg {
     int tail = -1;            // first level of the fused coarse tail (-1: every level launches its own kernels)
     // V-cycle smoother weight and coarse-correction factor; the pressure-correction
     // equation of SIMPLE/PRIME/PISO gains from a larger over-correction
-    // (forPressure). PRISM_AMG_OMEGA / PRISM_AMG_SCALE override both.
-    double omega = 0.9, scale = 1.8;
-    void forPressure() { scale = 2.0; }
+    // (forPressure). PRISM_AMG_OMEGA / PRISM_AMG_SCALE override both. flex_scale:
+    // the factor of the cycles that precondition flexible CG (the pressure
+    // correction: 2.2, measured best of 1.8-3.2 on the 2.1M-cell cavity;
+    // PRISM_AMG_FLEX_SCALE overrides it)
+    double omega = 0.9, scale = 1.8, flex_scale = 1.8;
+    // levels 1..k_levels are K-cycle levels in applyK() (two flexible-CG steps
+    // each, instead of one coarse cycle), when they lie above the fused tail and
+    // are not the coarsest
+    int k_levels = 0;
+    ArenaBuf<double> kscal, kpart;  // K-cycle scalars (8 per level), block partials of its reductions
+    ArenaBuf<unsigned int> kcount;
+    // the pressure-correction equation: over-correction 2.0 in V-cycles and
+    // PRISM_AMG_KCYCLE K-cycle levels for the flexible CG solve (default 0: on the
+    // 2.1M-cell cavity one or two K levels cut the iterations by 1.7x / 2.5x but the
+    // extra coarse-level launches cost more than that saved)
+    void forPressure();
+    bool kLevel(size_t l) const;
 
     // Build the hierarchy (first call) or refresh its values (later calls) for
     // the matrix A, whose CSR pattern (device rowptr/col) lists each row's
@@ -67,7 +83,11 @@ struct Amg {
     // z = M^-1 r (one V(1,1) cycle); S (optional): skip the work once the solve has stopped
     // sample: time the finest-level kernels when a profiling window is open
     void apply(const double* r, double* z, const KState* S, cudaStream_t s, bool sample = false);
-    void apply32(const float* r, float* z, const KState* S, cudaStream_t s);
+    // flexible: the cycle preconditions flexible CG (flex_scale)
+    void apply32(const float* r, float* z, const KState* S, cudaStream_t s, bool flexible = false);
+    // z = B r by one cycle with the K-cycle levels and flex_scale (a variable
+    // preconditioner: flexible CG only), FP64
+    void applyK(const double* r, double* z, const KState* S, cudaStream_t s, bool sample = false);
 };
 
 }  // namespace pb

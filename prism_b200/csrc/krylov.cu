@@ -34,6 +34,7 @@
 
 #include "krylov.h"
 #include "amg.h"
+#include "reduce.cuh"
 
 namespace pb {
 
@@ -42,63 +43,6 @@ namespace {
 constexpr int BS = 256;
 constexpr int WARPS = BS / 32;
 constexpr int MAX_GRID = NUM_SMS * 8;
-
-__device__ __forceinline__ double warpSum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ double warpMax(double v) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    return v;
-}
-
-// Block-reduce NV sums (or maxima), publish the block partial, and let the last
-// block to arrive reduce all partials in block order. Returns true in the last block.
-template <int NV, bool MAX>
-__device__ bool reduceLast(double (&v)[NV], double* partials, unsigned int* counter, double (&out)[NV]) {
-    __shared__ double sh[NV][WARPS];
-    __shared__ int is_last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = 0; k < NV; ++k) {
-        double x = MAX ? warpMax(v[k]) : warpSum(v[k]);
-        if (lane == 0) sh[k][warp] = x;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < NV; ++k) {
-            double s = sh[k][0];
-            for (int w = 1; w < WARPS; ++w) s = MAX ? fmax(s, sh[k][w]) : s + sh[k][w];
-            partials[blockIdx.x * NV + k] = s;
-        }
-        __threadfence();
-        unsigned int t = atomicAdd(counter, 1u);
-        is_last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!is_last) return false;
-    __threadfence();
-    double acc[NV];
-    for (int k = 0; k < NV; ++k) {
-        acc[k] = MAX ? 0.0 : 0.0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
-            double x = __ldcg(&partials[b * NV + k]);
-            acc[k] = MAX ? fmax(acc[k], x) : acc[k] + x;
-        }
-    }
-    __syncthreads();
-    for (int k = 0; k < NV; ++k) {
-        double x = MAX ? warpMax(acc[k]) : warpSum(acc[k]);
-        if (lane == 0) sh[k][warp] = x;
-    }
-    __syncthreads();
-    for (int k = 0; k < NV; ++k) {
-        double s = sh[k][0];
-        for (int w = 1; w < WARPS; ++w) s = MAX ? fmax(s, sh[k][w]) : s + sh[k][w];
-        out[k] = s;
-    }
-    if (threadIdx.x == 0) *counter = 0u;
-    return true;
-}
 
 inline int vecGrid(int n) { return std::max(1, std::min(ceil_div(n, BS), MAX_GRID)); }
 inline int spmvGrid(int nslices) { return std::max(1, std::min(ceil_div(nslices, WARPS), NUM_SMS * 16)); }
@@ -141,9 +85,9 @@ int waveGrid(K kernel, int needed) {
 // STAGE 0: plain; 1: alpha = rho / (u.y); 2: w = (u.y)/(y.y)
 // The columns and values of up to 8 slots are loaded before their gathers, so
 // a row's loads are all in flight at once; the sum runs over the slots in order.
-template <typename T, int W = 8>
+template <typename T, int W = 8, typename TX = T>
 __device__ __forceinline__ T sliceRow(const int* __restrict__ col, const T* __restrict__ val,
-                                      const T* __restrict__ x, int b, int width, int lane) {
+                                      const TX* __restrict__ x, int b, int width, int lane) {
     T sum = 0;
     for (int j0 = 0; j0 < width; j0 += W) {
         int c[W];
@@ -156,7 +100,7 @@ __device__ __forceinline__ T sliceRow(const int* __restrict__ col, const T* __re
             }
 #pragma unroll
         for (int k = 0; k < W; ++k)
-            if (j0 + k < width) sum += v[k] * __ldg(x + c[k]);
+            if (j0 + k < width) sum += v[k] * (T)__ldg(x + c[k]);
     }
     return sum;
 }
@@ -286,6 +230,125 @@ __global__ void __launch_bounds__(BS) init_kernel(int n, T* __restrict__ r, cons
         else if (out[1] == 0.0) S->done = 4;
         else if (out[0] <= S->tol2) S->done = 1;
         else S->done = 0;
+    }
+}
+
+// ---- flexible CG (FP64, AMG K-cycle preconditioner B): per iteration
+//   z = B r                                          AMG (applyK)
+//   u = A z ; z.q, z.u, z.r                          SpMV + fused dots
+//   beta = (z.q)/dq ; dq' = z.u - beta (z.q) ; dr' = z.r - beta dr ; alpha = dr'/dq'
+//   d = z - beta d ; q = u - beta q ; x += alpha d ; r -= alpha q ; r.r, d.q, d.r
+// (q = A d is carried, not recomputed: A d = A z - beta A d_prev). dq and dr
+// are the previous direction's d.q and d.r, taken exactly in the update pass;
+// dq' expands d.q for symmetric A.
+
+// r = b - r (r holds A x); d = q = 0; state as init_kernel
+__global__ void __launch_bounds__(BS) fcg_init_kernel(int n, double* __restrict__ r, const double* __restrict__ b,
+                                                      double* __restrict__ d, double* __restrict__ q,
+                                                      float* __restrict__ r32, double tol, double* partials,
+                                                      unsigned int* counter, KState* S) {
+    double d0 = 0.0, d1 = 0.0;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS) {
+        const double bi = b[i], ri = bi - r[i];
+        r[i] = ri;
+        if (r32) r32[i] = (float)ri;
+        d[i] = 0.0;
+        q[i] = 0.0;
+        d0 += ri * ri;
+        d1 += bi * bi;
+    }
+    double vv[2] = {d0, d1}, out[2];
+    if (reduceLast<2, false>(vv, partials, counter, out) && threadIdx.x == 0) {
+        S->rr = out[0];
+        S->bb = out[1];
+        S->r0sq = out[0];
+        S->tol2 = tol * tol * out[1];
+        S->dq = 1.0;
+        S->dr = 0.0;
+        S->alpha = 0.0;
+        S->beta = 0.0;
+        if (!isfinite(out[0]) || !isfinite(out[1])) S->done = 5;
+        else if (out[1] == 0.0) S->done = 4;
+        else if (out[0] <= S->tol2) S->done = 1;
+        else S->done = 0;
+    }
+}
+
+// u = A z with the dots z.q, z.u, z.r -> beta, alpha (non-positive d.q: restart);
+// z in FP64 or FP32 (the preconditioner's precision)
+template <int W, int MINB, typename TZ>
+__global__ void __launch_bounds__(BS, MINB) fcg_spmv_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                      const int* __restrict__ col, const double* __restrict__ val,
+                                                      const TZ* __restrict__ z, double* __restrict__ u,
+                                                      const double* __restrict__ q, const double* __restrict__ r,
+                                                      double* partials, unsigned int* counter, KState* S) {
+    pdlEnter();
+    if (S->done) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int b = sl_off[sl];
+        const int width = (sl_off[sl + 1] - b) >> 5;
+        const double sum = sliceRow<double, W, TZ>(col, val, z, b, width, lane);
+        const int i = sl * 32 + lane;
+        u[i] = sum;
+        if (i < n) {
+            const double zi = (double)z[i];
+            d0 += zi * q[i];
+            d1 += zi * sum;
+            d2 += zi * r[i];
+        }
+    }
+    double v[3] = {d0, d1, d2}, out[3];
+    if (reduceLast<3, false>(v, partials, counter, out) && threadIdx.x == 0) {
+        const double beta = out[0] / S->dq;
+        const double dq = out[1] - beta * out[0];
+        const double dr = out[2] - beta * S->dr;
+        const double alpha = dr / dq;
+        if (!isfinite(out[0]) || !isfinite(out[1]) || !isfinite(out[2])) S->done = 5;
+        else if (!(dq > 0.0) || !isfinite(alpha)) S->done = 3;
+        else {
+            S->beta = beta;
+            S->alpha = alpha;
+        }
+    }
+}
+
+// d = z - beta d ; q = u - beta q ; x += alpha d ; r -= alpha q ; r.r, d.q, d.r -> convergence
+// (r32: the FP32 copy of r that an FP32 preconditioner reads)
+template <typename TZ>
+__global__ void __launch_bounds__(BS) fcg_update_kernel(int n, double* __restrict__ x, double* __restrict__ r,
+                                                        double* __restrict__ d, double* __restrict__ q,
+                                                        const TZ* __restrict__ z, const double* __restrict__ u,
+                                                        float* __restrict__ r32, double* partials,
+                                                        unsigned int* counter, KState* S) {
+    pdlEnter();
+    if (S->done) return;
+    const double alpha = S->alpha, beta = S->beta;
+    double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+    for (int i = blockIdx.x * BS + threadIdx.x; i < n; i += gridDim.x * BS) {
+        const double di = (double)z[i] - beta * d[i];
+        const double qi = u[i] - beta * q[i];
+        const double ri = r[i] - alpha * qi;
+        x[i] += alpha * di;
+        d[i] = di;
+        q[i] = qi;
+        r[i] = ri;
+        if (r32) r32[i] = (float)ri;
+        d0 += ri * ri;
+        d1 += di * qi;
+        d2 += di * ri;
+    }
+    double v[3] = {d0, d1, d2}, out[3];
+    if (reduceLast<3, false>(v, partials, counter, out) && threadIdx.x == 0) {
+        S->rr = out[0];
+        S->dq = out[1];
+        S->dr = out[2];
+        S->iter += 1;
+        if (!isfinite(out[0]) || !isfinite(out[1])) S->done = 5;
+        else if (out[0] <= S->tol2) S->done = 1;
+        else if (S->iter >= S->maxit) S->done = 2;
+        else if (!(out[1] > 0.0)) S->done = 3;
     }
 }
 
@@ -455,6 +518,29 @@ __global__ void __launch_bounds__(BS) resid_kernel(int nslices, int n, const int
         out3[1] = out[1];
         out3[2] = out[2];
     }
+}
+
+// max over rows of sum_{j != i} |a_ij| / |a_ii| (infinite for a zero or non-finite diagonal)
+__global__ void __launch_bounds__(BS) offdiag_ratio_kernel(int nslices, int n, const int* __restrict__ sl_off,
+                                                           const int* __restrict__ col, const double* __restrict__ val,
+                                                           double* partials, unsigned int* counter, double* out1) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double m = 0.0;
+    for (int sl = blockIdx.x * WARPS + warp; sl < nslices; sl += gridDim.x * WARPS) {
+        const int bo = sl_off[sl], width = (sl_off[sl + 1] - bo) >> 5;
+        const int r = sl * 32 + lane;
+        if (r >= n) continue;
+        double off = 0.0, diag = 0.0;
+        for (int j = 0; j < width; ++j) {
+            const double a = fabs(val[bo + 32 * j + lane]);
+            if (col[bo + 32 * j + lane] == r) diag += a;
+            else off += a;
+        }
+        const double t = off / diag;
+        m = (diag > 0.0 && isfinite(t)) ? fmax(m, t) : INFINITY;
+    }
+    double v[1] = {m}, out[1];
+    if (reduceLast<1, true>(v, partials, counter, out) && threadIdx.x == 0) out1[0] = out[0];
 }
 
 }  // namespace
@@ -654,6 +740,42 @@ void iterateEager(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T*
     }
 }
 
+// Krylov method of a solve: BiCGSTAB, or flexible CG preconditioned by an FP64
+// cycle (with the K-cycle levels) or by an FP32 V-cycle
+enum { KM_BICGSTAB = 0, KM_FCG = 1, KM_FCG_PRE32 = 2 };
+
+// `count` flexible-CG iterations (FP64 recurrences), launched one kernel at a time.
+// Vectors: x = V.x, r = V.r, d = V.p, q = V.v, u = V.t; z = y (KM_FCG) or, for
+// KM_FCG_PRE32, the FP32 pair r32 = w.y32 -> z32 = w.z32.
+void iterateFcgEager(const SellMatrix& A, const double* M, Vecs<double> V, Amg* amg, double* y, int mode,
+                     long long count, bool sample, KrylovWork& w, cudaStream_t s) {
+    KState* S = w.state.p;
+    const int n = A.n, vg = vecGrid(n);
+    const bool p32 = mode == KM_FCG_PRE32;
+    auto k64 = fcg_spmv_kernel<4, 6, double>;
+    auto k32 = fcg_spmv_kernel<4, 6, float>;
+    const int sg = p32 ? waveGrid(k32, ceil_div(A.nslices, WARPS)) : waveGrid(k64, ceil_div(A.nslices, WARPS));
+    for (long long it = 0; it < count; ++it) {
+        if (p32) {
+            amg->apply32(w.y32.p, w.z32.p, S, s, true);
+            const int slot = sample ? profBegin(PROF_SPMV, false, spmvBytes<double>(A), s) : -1;
+            launchPdl(k32, sg, BS, s, A.nslices, n, A.sl_off, A.col, M, (const float*)w.z32.p, V.t,
+                      (const double*)V.v, (const double*)V.r, w.partials.p, w.counter.p, S);
+            profEnd(slot, s);
+            launchPdl(fcg_update_kernel<float>, vg, BS, s, n, V.x, V.r, V.p, V.v, (const float*)w.z32.p,
+                      (const double*)V.t, w.y32.p, w.partials.p, w.counter.p, S);
+        } else {
+            amg->applyK(V.r, y, S, s, sample);
+            const int slot = sample ? profBegin(PROF_SPMV, false, spmvBytes<double>(A), s) : -1;
+            launchPdl(k64, sg, BS, s, A.nslices, n, A.sl_off, A.col, M, (const double*)y, V.t, (const double*)V.v,
+                      (const double*)V.r, w.partials.p, w.counter.p, S);
+            profEnd(slot, s);
+            launchPdl(fcg_update_kernel<double>, vg, BS, s, n, V.x, V.r, V.p, V.v, (const double*)y,
+                      (const double*)V.t, (float*)nullptr, w.partials.p, w.counter.p, S);
+        }
+    }
+}
+
 // PRISM_NO_GRAPHS=1: launch every iteration kernel by kernel (diagnostics)
 bool graphsEnabled() {
     static const bool on = [] {
@@ -669,17 +791,30 @@ bool graphsEnabled() {
 // only when an operand changes. Kernels after convergence return at once, so
 // replays past the end of a batch change nothing.
 template <typename T>
+void iterateAny(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, long long count, bool sample,
+                int mode, KrylovWork& w, cudaStream_t s) {
+    if constexpr (sizeof(T) == 8) {
+        if (mode != KM_BICGSTAB) {
+            iterateFcgEager(A, M, V, amg, y, mode, count, sample, w, s);
+            return;
+        }
+    }
+    iterateEager<T>(A, M, V, amg, y, z, count, sample, w, s);
+}
+
+template <typename T>
 void iterate(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, long long batch, bool first,
-             KrylovWork& w, cudaStream_t s) {
+             KrylovWork& w, cudaStream_t s, int mode = KM_BICGSTAB) {
     if (first || !graphsEnabled()) {
-        iterateEager<T>(A, M, V, amg, y, z, batch, true, w, s);
+        iterateAny<T>(A, M, V, amg, y, z, batch, true, mode, w, s);
         return;
     }
-    std::vector<uintptr_t> key = {(uintptr_t)sizeof(T), (uintptr_t)A.sl_off, (uintptr_t)A.col, (uintptr_t)A.nslices,
+    std::vector<uintptr_t> key = {(uintptr_t)mode, (uintptr_t)sizeof(T), (uintptr_t)A.sl_off, (uintptr_t)A.col, (uintptr_t)A.nslices,
                                   (uintptr_t)A.n, (uintptr_t)M, (uintptr_t)V.x, (uintptr_t)V.r, (uintptr_t)V.r0,
                                   (uintptr_t)V.p, (uintptr_t)V.v, (uintptr_t)V.s, (uintptr_t)V.t, (uintptr_t)amg,
                                   (uintptr_t)(amg ? amg->generation : 0), (uintptr_t)y, (uintptr_t)z,
-                                  (uintptr_t)w.state.p, (uintptr_t)w.partials.p, (uintptr_t)w.counter.p};
+                                  (uintptr_t)w.state.p, (uintptr_t)w.partials.p, (uintptr_t)w.counter.p,
+                                  (uintptr_t)w.y32.p, (uintptr_t)w.z32.p};
     constexpr size_t MAX_GRAPHS = 8;
     auto hit = std::find_if(w.graphs.begin(), w.graphs.end(), [&](const KrylovWork::IterGraph& g) { return g.key == key; });
     if (hit != w.graphs.end()) {
@@ -695,7 +830,7 @@ void iterate(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, l
         PB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
         cudaGraph_t graph = nullptr;
         try {
-            iterateEager<T>(A, M, V, amg, y, z, 1, false, w, s);
+            iterateAny<T>(A, M, V, amg, y, z, 1, false, mode, w, s);
         } catch (...) {
             cudaStreamEndCapture(s, &graph);
             if (graph) cudaGraphDestroy(graph);
@@ -724,7 +859,9 @@ void iterate(const SellMatrix& A, const T* M, Vecs<T> V, Amg* amg, T* y, T* z, l
 // BiCGSTAB iterations on (M, rhs) from the current x; returns iterations done.
 template <typename T>
 KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, bool from_zero, double tol,
-                      long long maxit, KrylovWork& w, cudaStream_t s, Amg* amg, T* y, T* z) {
+                      long long maxit, KrylovWork& w, cudaStream_t s, Amg* amg, T* y, T* z,
+                      int mode = KM_BICGSTAB) {
+    const bool flex = mode != KM_BICGSTAB;
     KrylovOut out;
     KState* S = w.state.p;
     KState init{};
@@ -738,13 +875,23 @@ KrylovOut runBicgstab(const SellMatrix& A, const T* M, const T* rhs, Vecs<T> V, 
         if (!zero)
             spmv_kernel<T, 0><<<sg, BS, 0, s>>>(A.nslices, n, A.sl_off, A.col, M, V.x, V.r, nullptr, nullptr, nullptr,
                                                 nullptr); countLaunch();
-        init_kernel<T><<<vg, BS, 0, s>>>(n, V.r, rhs, V.r0, V.p, V.v, zero ? 1 : 0, tol, w.partials.p, w.counter.p, S); countLaunch();
+        if constexpr (sizeof(T) == 8) {
+            if (flex) {
+                if (zero) fail(PRISM_INTERNAL, "flexible CG starts from A x");
+                fcg_init_kernel<<<vg, BS, 0, s>>>(n, V.r, rhs, V.p, V.v, mode == KM_FCG_PRE32 ? w.y32.p : nullptr, tol,
+                                                  w.partials.p, w.counter.p, S); countLaunch();
+            }
+        }
+        if (!flex) {
+            init_kernel<T><<<vg, BS, 0, s>>>(n, V.r, rhs, V.r0, V.p, V.v, zero ? 1 : 0, tol, w.partials.p, w.counter.p,
+                                             S); countLaunch();
+        }
         PB_LAUNCH("bicgstab init");
         zero = false;
         int done = 0;
         bool first = true;
         while (true) {
-            iterate<T>(A, M, V, amg, y, z, batch, first, w, s);
+            iterate<T>(A, M, V, amg, y, z, batch, first, w, s, mode);
             first = false;
             PB_LAUNCH("bicgstab iteration");
             PB_CUDA(cudaMemcpyAsync(w.host_state, S, sizeof(KState), cudaMemcpyDeviceToHost, s));
@@ -785,9 +932,28 @@ bool restartOnUpdate() {
     return v;
 }
 
+namespace {
+// flexible CG's preconditioner: an FP32 V-cycle (half the bytes of the FP64 one; the
+// recurrences stay FP64) unless the hierarchy has K-cycle levels (FP64 only) or
+// PRISM_FCG_PREC=fp64
+int fcgMode(const Amg* amg) { return fcgPre32(amg) ? KM_FCG_PRE32 : KM_FCG; }
+}  // namespace
+
+bool fcgPre32(const Amg* amg) {
+    static const bool p64 = [] {
+        const char* e = std::getenv("PRISM_FCG_PREC");
+        return e && std::strcmp(e, "fp64") == 0;
+    }();
+    return !p64 && amg->k_levels == 0;
+}
+
 KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, int precision,
-                   double inner_tol, KrylovWork& w, cudaStream_t s, Amg* amg, const int* rowptr, const int* col) {
+                   double inner_tol, KrylovWork& w, cudaStream_t s, Amg* amg, const int* rowptr, const int* col,
+                   bool flexible) {
     const bool mixed = precision == PRISM_PREC_MIXED;
+    if (flexible && (mixed || !amg)) fail(PRISM_INTERNAL, "flexible CG runs FP64 with AMG only");
+    const int mode = flexible ? fcgMode(amg) : KM_BICGSTAB;
+    const bool pre32 = mixed || mode == KM_FCG_PRE32;  // FP32 copy of the hierarchy
     w.ensure(A.nslices * 32, A.nnz_padded, mixed);
     const int n = A.n;
     const int gn = ceil_div(n, BS);
@@ -810,12 +976,12 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
         M32 = w.As32.p;
     } else {
         if (!rowptr || !col) fail(PRISM_INTERNAL, "AMG preconditioner without a CSR pattern");
-        w.ensurePrec(mixed);
+        w.ensurePrec(pre32);
         VerboseTimer vt("amg setup", s);
-        amg->setup(A, rowptr, col, mixed, s);
+        amg->setup(A, rowptr, col, pre32, s);
         M32 = amg->vals32();
     }
-    VerboseTimer vt_solve(mixed ? "bicgstab fp32+fp64" : "bicgstab fp64", s);
+    VerboseTimer vt_solve(mixed ? "bicgstab fp32+fp64" : flexible ? "fcg fp64" : "bicgstab fp64", s);
     auto finish = [&] {
         if (scaled) {
             unscale_kernel<<<gn, BS, 0, s>>>(n, w.dinv.p, w.xs.p, x); countLaunch();
@@ -827,7 +993,7 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
         Vecs<double> V{X, w.r.p, w.r0.p, w.p.p, w.v.p, w.s.p, w.t.p};
         // accurate-residual restarts: the recursive residual drifts from b - A x
         for (int pass = 0; pass < 4; ++pass) {
-            KrylovOut o = runBicgstab<double>(A, A64.vals, b, V, false, tol, maxit, w, s, amg, w.y.p, w.z.p);
+            KrylovOut o = runBicgstab<double>(A, A64.vals, b, V, false, tol, maxit, w, s, amg, w.y.p, w.z.p, mode);
             if (w.host_state->done == 4) PB_CUDA(cudaMemsetAsync(X, 0, n * sizeof(double), s));  // b = 0: x = 0
             out.iterations += o.iterations;
             out.status = o.status;
@@ -843,8 +1009,8 @@ KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, 
             if (o.status != PRISM_OK || out.rel_residual <= 10 * tol || maxit <= 0 || rb[1] == 0) break;
         }
         if (verbose())
-            std::fprintf(stderr, "[prism] bicgstab fp64 n=%d: %lld iterations, rel residual %.3e, status %d\n", n,
-                         out.iterations, out.rel_residual, out.status);
+            std::fprintf(stderr, "[prism] %s fp64 n=%d: %lld iterations, rel residual %.3e, status %d\n",
+                         flexible ? "fcg" : "bicgstab", n, out.iterations, out.rel_residual, out.status);
         return out;
     }
     // mixed precision: FP32 BiCGSTAB with FP64 reliable updates of X and r
@@ -1028,6 +1194,17 @@ double scaledResidual(const SellMatrix& A, const double* b, const double* x, Kry
     PB_CUDA(cudaStreamSynchronize(s));
     if (h[2] != 0.0) return NAN;
     return h[0] / (h[1] + EPSILON);
+}
+
+double offDiagonalRatio(const SellMatrix& A, KrylovWork& w, cudaStream_t s) {
+    w.ensure(A.nslices * 32, A.nnz_padded, false);
+    offdiag_ratio_kernel<<<waveGrid(offdiag_ratio_kernel, ceil_div(A.nslices, WARPS)), BS, 0, s>>>(
+        A.nslices, A.n, A.sl_off, A.col, A.vals, w.partials.p, w.counter.p, w.scal.p); countLaunch();
+    PB_LAUNCH("offdiag_ratio_kernel");
+    double h = 0.0;
+    PB_CUDA(cudaMemcpyAsync(&h, w.scal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    return h;
 }
 
 // ---------------------------------------------------------------- solves inside a CUDA graph
@@ -1229,7 +1406,9 @@ void emitOuterStep(SolveCtl* ctl, KrylovWork& w, cudaGraphConditionalHandle oute
 // The kernels and their order are those of the eager path, so the results are the same.
 void emitBicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, KrylovWork& w,
                   cudaStream_t s, Amg* amg, const int* rowptr, const int* col, SolveCtl* ctl, CaptureStreams& cs,
-                  int depth) {
+                  int depth, bool flexible) {
+    if (flexible && !amg) fail(PRISM_INTERNAL, "flexible CG runs with AMG only");
+    const int mode = flexible ? fcgMode(amg) : KM_BICGSTAB;
     w.ensure(A.nslices * 32, A.nnz_padded, false);
     const int n = A.n, gn = ceil_div(n, BS);
     const bool scaled = amg == nullptr;
@@ -1243,8 +1422,8 @@ void emitBicgstab(const SellMatrix& A, const double* b, double* x, double tol, l
         X = w.xs.p;
     } else {
         if (!rowptr || !col) fail(PRISM_INTERNAL, "AMG preconditioner without a CSR pattern");
-        w.ensurePrec(false);
-        amg->setup(A, rowptr, col, false, s);
+        w.ensurePrec(mode == KM_FCG_PRE32);
+        amg->setup(A, rowptr, col, mode == KM_FCG_PRE32, s);
     }
     KState* S = w.state.p;
     Vecs<double> V{X, w.r.p, w.r0.p, w.p.p, w.v.p, w.s.p, w.t.p};
@@ -1260,10 +1439,15 @@ void emitBicgstab(const SellMatrix& A, const double* b, double* x, double tol, l
     beginConditional(body, cudaGraphCondTypeIf, hi, sub);
     spmv_kernel<double, 0><<<sg, BS, 0, sub>>>(A.nslices, n, A.sl_off, A.col, A64.vals, V.x, V.r, nullptr, nullptr,
                                                nullptr, nullptr); countLaunch();
-    init_kernel<double><<<vg, BS, 0, sub>>>(n, V.r, b, V.r0, V.p, V.v, 0, tol, w.partials.p, w.counter.p, S); countLaunch();
+    if (flexible) {
+        fcg_init_kernel<<<vg, BS, 0, sub>>>(n, V.r, b, V.p, V.v, mode == KM_FCG_PRE32 ? w.y32.p : nullptr, tol,
+                                            w.partials.p, w.counter.p, S); countLaunch();
+    } else {
+        init_kernel<double><<<vg, BS, 0, sub>>>(n, V.r, b, V.r0, V.p, V.v, 0, tol, w.partials.p, w.counter.p, S); countLaunch();
+    }
     endConditional(sub);
     beginConditional(body, cudaGraphCondTypeIf, ht, sub);
-    iterateEager<double>(A, A64.vals, V, amg, w.y.p, w.z.p, GRAPH_UNROLL, false, w, sub);
+    iterateAny<double>(A, A64.vals, V, amg, w.y.p, w.z.p, GRAPH_UNROLL, false, mode, w, sub);
     endConditional(sub);
     beginConditional(body, cudaGraphCondTypeIf, hc, sub);
     zero_if_rhs_zero_kernel<<<vg, BS, 0, sub>>>(n, X, S); countLaunch();

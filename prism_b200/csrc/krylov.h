@@ -38,6 +38,7 @@ struct KState {
     double rr, bb, tol2, r0sq;
     double ts, tt;
     double rr_update, delta2;  // mixed precision: |r|^2 at the last reliable update, trigger factor^2
+    double dq, dr;             // flexible CG: d.(A d) and d.r of the last direction
     long long iter, maxit;
     int done;  // 0 running, 1 converged, 2 max iterations, 3 restart needed, 4 zero rhs, 5 non-finite,
                // 6 reliable update due (mixed precision)
@@ -82,13 +83,22 @@ struct KrylovOut {
 // (column scaling) when amg is null, else one V-cycle of amg, whose hierarchy is
 // built on first use from the device CSR pattern (rowptr, col) of A and refreshed
 // with A's values on every call.
+// flexible: FP64 with amg only -- flexible conjugate gradients (Notay 2000, one
+// previous direction kept) preconditioned by amg->applyK(), for symmetric
+// positive (semi-)definite A (the pressure-correction equation), in place of
+// BiCGSTAB; same stopping rule, passes and statuses.
 KrylovOut bicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, int precision,
                    double inner_tol, KrylovWork& w, cudaStream_t s, Amg* amg = nullptr, const int* rowptr = nullptr,
-                   const int* col = nullptr);
+                   const int* col = nullptr, bool flexible = false);
+// flexible CG with amg preconditions with an FP32 V-cycle (else with the FP64 cycle)
+bool fcgPre32(const Amg* amg);
 // x <- x + D^-1 (b - A x)   (numerics/jacobi.cpp:5-9)
 void jacobiStep(const SellMatrix& A, const double* b, double* x, KrylovWork& w, cudaStream_t s);
 // max|A x - b| / (max|diag(A) x| + eps)   (numerics/solver.cpp:8-24); returns NaN if non-finite values met
 double scaledResidual(const SellMatrix& A, const double* b, const double* x, KrylovWork& w, cudaStream_t s);
+// max over rows of sum_{j != i} |a_ij| / |a_ii| (inf for a zero diagonal): below 1, Jacobi
+// converges at least that fast, whatever the coupling
+double offDiagonalRatio(const SellMatrix& A, KrylovWork& w, cudaStream_t s);
 // y <- A x (FP64)
 void spmv(const SellMatrix& A, const double* x, double* y, cudaStream_t s);
 // H-operator of the explicit momentum step: x_new = (b - (A x - diag x)) / diag  (PRIME.cpp:39-56)
@@ -142,6 +152,6 @@ void emitOuterStep(SolveCtl* ctl, KrylovWork& w, cudaGraphConditionalHandle oute
 // the FP64 bicgstab() of one step, as device-controlled nodes (streams: helpers for the bodies)
 void emitBicgstab(const SellMatrix& A, const double* b, double* x, double tol, long long maxit, KrylovWork& w,
                   cudaStream_t s, Amg* amg, const int* rowptr, const int* col, SolveCtl* ctl, CaptureStreams& cs,
-                  int depth);
+                  int depth, bool flexible = false);
 
 }  // namespace pb

@@ -536,6 +536,46 @@ int choosePreconditioner(int pc, int64_t n) {
     return pc;
 }
 
+// PRISM_PC_AUTO at AMG sizes: an equation whose off-diagonal row sums stay below this
+// fraction of the diagonal (an under-relaxed momentum predictor: about the relaxation
+// factor) is solved with Jacobi, whose iteration then converges fast and costs a third
+// of an AMG one; PRISM_PC_AUTO_JACOBI overrides it (0: always AMG). The spd pressure
+// correction keeps AMG.
+static double autoJacobiRatio() {
+    static const double v = [] {
+        const char* e = std::getenv("PRISM_PC_AUTO_JACOBI");
+        return e && e[0] ? std::atof(e) : 0.8;
+    }();
+    return v;
+}
+
+// preconditioner of a solve of eq (A: its assembled matrix); measures and records the
+// automatic choice on the first solve (a host round trip, never inside a capture)
+static int pcFor(Transport& eq, const PrismSolveOpts& o, const SellMatrix& A) {
+    const int c = choosePreconditioner(o.preconditioner, A.n);
+    if (o.preconditioner != PRISM_PC_AUTO || c != PRISM_PC_AMG || eq.spd || autoJacobiRatio() <= 0.0) return c;
+    if (eq.auto_pc == 0) {
+        Mesh& m = *eq.phi->m;
+        if (capturing(m.stream)) fail(PRISM_INTERNAL, "automatic preconditioner not chosen before capture");
+        const double t = offDiagonalRatio(A, m.kw, m.stream);
+        eq.auto_pc = t <= autoJacobiRatio() ? PRISM_PC_JACOBI : PRISM_PC_AMG;
+        if (verbose())
+            std::fprintf(stderr, "[prism] automatic preconditioner of %s: %s (off-diagonal ratio %.3f)\n",
+                         eq.phi->name.c_str(), eq.auto_pc == PRISM_PC_AMG ? "AMG" : "Jacobi", t);
+    }
+    return eq.auto_pc;
+}
+
+// FP64 AMG solves of an spd equation run flexible CG; PRISM_PRESSURE_SOLVER=bicgstab
+// keeps BiCGSTAB with the V-cycle for them
+static bool flexibleFor(const Transport& eq, const PrismSolveOpts& o, const Amg* amg) {
+    static const bool on = [] {
+        const char* e = std::getenv("PRISM_PRESSURE_SOLVER");
+        return !(e && std::strcmp(e, "bicgstab") == 0);
+    }();
+    return on && eq.spd && amg && o.method == PRISM_SOLVER_BICGSTAB && o.precision == PRISM_PREC_FP64;
+}
+
 namespace {
 // set while a solve or step is being captured into a graph (graph_capture below)
 struct GraphCapture {
@@ -565,7 +605,7 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
     const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
     const double itol = o.inner_tol > 0 ? o.inner_tol : 0.1;
     Amg* amg = nullptr;
-    if (o.method != PRISM_SOLVER_JACOBI && choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
+    if (o.method != PRISM_SOLVER_JACOBI && pcFor(eq, o, A) == PRISM_PC_AMG) {
         if (!eq.amg) eq.amg = std::make_shared<Amg>();
         amg = eq.amg.get();
     }
@@ -584,7 +624,7 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
             jacobiStep(A, eq.b.p, phi.v.p, m.kw, m.stream);
         } else {
             KrylovOut k = bicgstab(A, eq.b.p, phi.v.p, ktol, kmax, o.precision, itol, m.kw, m.stream, amg,
-                                   m.pat.rowptr.p, m.pat.col.p);
+                                   m.pat.rowptr.p, m.pat.col.p, flexibleFor(eq, o, amg));
             r.krylov_iterations += k.iterations;
             r.krylov_rel_residual = k.rel_residual;
             if (k.status != PRISM_OK && r.status == PRISM_OK) r.status = k.status;
@@ -791,6 +831,7 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
         m.p_amg->forPressure();
     }
     pEqn.amg = m.p_amg;
+    pEqn.spd = true;
     for (int64_t i = 0; i <= c.non_ortho_correctors; ++i) {
         PhaseTimer pt("pressure corrector " + std::to_string(i), m.stream);
         auto r = solve(pEqn, inner(so, c.pressure_max_iter, c.pressure_residual, c.p_ref_cell, c.p_ref_value, true));
@@ -1161,7 +1202,7 @@ PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o) {
     const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
     const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
     Amg* amg = nullptr;
-    if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
+    if (pcFor(eq, o, A) == PRISM_PC_AMG) {
         if (!eq.amg) eq.amg = std::make_shared<Amg>();
         amg = eq.amg.get();
     }
@@ -1175,7 +1216,8 @@ PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o) {
         cudaStream_t body = m.cs.at(0);
         beginConditional(s, cudaGraphCondTypeWhile, outer, body);
         phi.event += 2;
-        emitBicgstab(A, eq.b.p, phi.v.p, ktol, kmax, m.kw, body, amg, m.pat.rowptr.p, m.pat.col.p, ctl, m.cs, 1);
+        emitBicgstab(A, eq.b.p, phi.v.p, ktol, kmax, m.kw, body, amg, m.pat.rowptr.p, m.pat.col.p, ctl, m.cs, 1,
+                     flexibleFor(eq, o, amg));
         ++phi.event;
         emitResidual(A, eq.b.p, phi.v.p, m.kw, body);
         emitOuterStep(ctl, m.kw, outer, body);
@@ -1257,10 +1299,21 @@ bool graphReady(const Transport& eq, const PrismSolveOpts& o) {
     const Mesh& m = *eq.phi->m;
     if (o.method != PRISM_SOLVER_BICGSTAB || o.precision != PRISM_PREC_FP64) return false;
     if (!eq.A || !eq.b || m.kw.n != m.n_pad) return false;
-    if (choosePreconditioner(o.preconditioner, m.nc) == PRISM_PC_AMG) {
+    int pc = choosePreconditioner(o.preconditioner, m.nc);
+    if (o.preconditioner == PRISM_PC_AUTO && pc == PRISM_PC_AMG && !eq.spd && autoJacobiRatio() > 0.0) {
+        if (eq.auto_pc == 0) return false;  // chosen on an ordinary solve first
+        pc = eq.auto_pc;
+    }
+    if (pc == PRISM_PC_AMG) {
         if (!eq.amg || !eq.amg->built || !m.kw.y) return false;
         for (auto& L : eq.amg->levels)
             if (!L->b || !L->dinv) return false;
+        if (eq.amg->k_levels > 0 && !eq.amg->kscal) return false;
+        if (flexibleFor(eq, o, eq.amg.get()) && fcgPre32(eq.amg.get())) {
+            if (!m.kw.y32 || (!eq.amg->coarse_inv32 && eq.amg->coarse_inv)) return false;
+            for (auto& L : eq.amg->levels)
+                if (!L->b32 || !L->vals32) return false;
+        }
     }
     return true;
 }

@@ -137,6 +137,12 @@ struct Transport {
     DevBuf<double> store;  // A, b, bconv and bdiff in one allocation
     DevSlice<double> A, b, bconv, bdiff;
     std::shared_ptr<Amg> amg;  // AMG hierarchy (PRISM_PC_AMG), built on the first solve
+    // symmetric positive (semi-)definite matrix (the pressure correction): with AMG,
+    // FP64 solves run flexible CG with the K-cycle instead of BiCGSTAB
+    bool spd = false;
+    // PRISM_PC_AUTO at AMG sizes, decided on the equation's first solve: Jacobi when
+    // its matrix is diagonally dominant enough (offDiagonalRatio), else AMG (0: not yet)
+    int auto_pc = 0;
     // adjoint: A^T values and the AMG hierarchy of A^T
     DevBuf<double> AT;
     std::shared_ptr<Amg> amg_adj;

@@ -1,4 +1,4 @@
-"""AMG-preconditioned BiCGSTAB on the GPU vs the oracle.
+"""AMG-preconditioned BiCGSTAB (and flexible CG for the pressure correction) on the GPU vs the oracle.
 
 The preconditioner changes only the path to the solution: every solved field
 must agree with the oracle (ILUT-BiCGSTAB to machine precision) within 1e-8
@@ -79,6 +79,33 @@ def test_cavity_simple_amg(gpu, orc, precision):
     for i, k in enumerate(("U", "p", "mdot")):
         err = cases.rel_l2(out["gpu"][i], out["orc"][i])
         print(f"cavity 24x24 AMG precision={precision} {k}: rel L2 vs oracle {err:.3e}")
+        assert err < SOL_TOL
+
+
+_CAVITY160 = {}
+
+
+def _cavity160(lib, solver, steps=3):
+    mesh, U, p, nu, mdot, eqs = cases.cavity(160, lib)
+    simple = api.IncompressibleSIMPLE(api.SIMPLEControls(), solver=solver)
+    for _ in range(steps):
+        simple.step(eqs, U, mdot, p)
+    return U.values(), p.values(), mdot.face_flux()
+
+
+@pytest.mark.parametrize("kcycle", [None, "1"])
+def test_cavity_simple_flexible_cg(gpu, orc, kcycle, monkeypatch):
+    """The FP64 pressure correction at AMG sizes runs flexible CG: preconditioned by an
+    FP32 V-cycle by default, by the FP64 K-cycle with PRISM_AMG_KCYCLE=1 (160 x 160:
+    level 1 has 5,000+ rows and lies above the fused tail, so it is a K level)."""
+    if kcycle:
+        monkeypatch.setenv("PRISM_AMG_KCYCLE", kcycle)
+    got = _cavity160(gpu, api.BiCGSTAB(preconditioner="amg"))
+    if "orc" not in _CAVITY160:
+        _CAVITY160["orc"] = _cavity160(orc, api.BiCGSTAB())
+    for i, k in enumerate(("U", "p", "mdot")):
+        err = cases.rel_l2(got[i], _CAVITY160["orc"][i])
+        print(f"cavity 160x160, 3 SIMPLE iterations, K-cycle levels {kcycle or 0} {k}: rel L2 vs oracle {err:.3e}")
         assert err < SOL_TOL
 
 
