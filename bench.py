@@ -495,33 +495,41 @@ def run_ours(args, world, rank, local):
         return avg_b / (avg_ms * 1e-3) / 1e9, avg_ms, avg_b
 
     spmv_gbs, spmv_ms, spmv_bytes = live(prof.fp64_launches, prof.fp64_ms, prof.fp64_bytes)
-    post_gbs, post_ms, post_bytes = live(prof.amg_post_launches, prof.amg_post_ms, prof.amg_post_bytes)
-    pre_gbs, pre_ms, pre_bytes = live(prof.amg_pre_launches, prof.amg_pre_ms, prof.amg_pre_bytes)
+    fcg_gbs, fcg_ms, fcg_bytes = live(prof.fcg_launches, prof.fcg_ms, prof.fcg_bytes)
+    # the pressure correction's cycle runs in FP32 (flexible CG), other AMG solves in FP64
+    a32 = prof.amg32_post_launches > 0
+    prec = "float" if a32 else "double"
+    post_gbs, post_ms, post_bytes = live(*((prof.amg32_post_launches, prof.amg32_post_ms, prof.amg32_post_bytes) if a32
+                                          else (prof.amg_post_launches, prof.amg_post_ms, prof.amg_post_bytes)))
+    down_gbs, down_ms, down_bytes = live(*((prof.amg32_down_launches, prof.amg32_down_ms, prof.amg32_down_bytes) if a32
+                                          else (prof.amg_down_launches, prof.amg_down_ms, prof.amg_down_bytes)))
 
     def traffic_for(name, nbytes):
-        # DRAM bytes of one launch measured by ncu on a case larger than L2, scaled to this
-        # launch by its algorithmic bytes (traffic grows in proportion to them: no re-reads)
+        # DRAM bytes of one launch measured by ncu, scaled to this launch by its algorithmic
+        # bytes (same workload: the ratio is the measured traffic per algorithmic byte)
         f = os.path.join(ROOT, "profiles", name)
         if nbytes is None or not os.path.exists(f):
             return None
         with open(f) as fh:
             return json.load(fh)["traffic_per_algorithmic_byte"] * nbytes
 
-    spmv = {"kernel": "spmv_kernel<double,1> (SELL-32 SpMV + fused dot, BiCGSTAB v = A y)", "bound": "hbm",
-            "achieved": spmv_gbs, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-            "frac": spmv_gbs / hbm if spmv_gbs else None,
-            "traffic": traffic_for("spmv_fp64_traffic.json", spmv_bytes),
-            "algorithmic_bytes_per_launch": spmv_bytes, "avg_launch_ms": spmv_ms,
-            "sampled_launches": prof.fp64_launches}
+    def kernel_line(kernel, gbs, ms, nbytes, launches, traffic_file):
+        return {"kernel": kernel, "bound": "hbm", "achieved": gbs, "peak": hbm, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": gbs / hbm if gbs else None, "traffic": traffic_for(traffic_file, nbytes),
+                "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": ms, "sampled_launches": launches}
+
+    spmv = kernel_line("spmv_kernel<double,1> (SELL-32 SpMV + fused dot, BiCGSTAB v = A y: the momentum predictors)",
+                spmv_gbs, spmv_ms, spmv_bytes, prof.fp64_launches, "spmv_fp64_traffic.json")
+    fcg = kernel_line("fcg_spmv_kernel<4,6,float> (flexible CG u = A z + three fused dots: the pressure correction)",
+               fcg_gbs, fcg_ms, fcg_bytes, prof.fcg_launches, "fcg_spmv_traffic.json")
     if post_gbs:
-        roof = {"kernel": "post_kernel<double,1> (AMG finest level: prolongation + post-smoothing SpMV)",
-                "bound": "hbm", "achieved": post_gbs, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": post_gbs / hbm, "traffic": traffic_for("amg_post_fp64_traffic.json", post_bytes),
-                "algorithmic_bytes_per_launch": post_bytes, "avg_launch_ms": post_ms,
-                "sampled_launches": prof.amg_post_launches,
-                "pre_kernel": {"achieved": pre_gbs, "frac": pre_gbs / hbm if pre_gbs else None,
-                               "avg_launch_ms": pre_ms, "algorithmic_bytes_per_launch": pre_bytes,
-                               "sampled_launches": prof.amg_pre_launches}}
+        roof = kernel_line(f"post_kernel<{prec},1> (AMG finest level: prolongation + post-smoothing SpMV)",
+                    post_gbs, post_ms, post_bytes, prof.amg32_post_launches if a32 else prof.amg_post_launches,
+                    f"amg{'32' if a32 else ''}_post_traffic.json")
+        roof["down_kernel"] = kernel_line(f"down_kernel<{prec},1> (AMG finest level: smoothed restriction SpMV)",
+                                   down_gbs, down_ms, down_bytes,
+                                   prof.amg32_down_launches if a32 else prof.amg_down_launches,
+                                   f"amg{'32' if a32 else ''}_down_traffic.json")
     else:
         roof = spmv
     extra = {}
@@ -575,12 +583,13 @@ def run_ours(args, world, rank, local):
                 "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": f"cavity SIMPLE {N_CAVITY}x{N_CAVITY}x1 ({n} cells), Re=100, Upwind + "
-                                       "Corrected, urf 0.7/0.3, BiCGSTAB (AMG-preconditioned, PRISM_PC_AUTO) to 1e-12, "
+                                       "Corrected, urf 0.7/0.3, solves to 1e-12 (PRISM_PC_AUTO: momentum BiCGSTAB "
+                                       "with Jacobi, pressure correction flexible CG with an FP32 AMG V-cycle), "
                                        "each outer iteration one CUDA graph launch (PrismSolveOpts.graph)",
                            "cells": n, "l2": "inputs larger than L2 (no flush)",
                            "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                            "mesh_build_s": t_build},
-                "spmv_gbs": spmv_gbs, "roofline": roof, "spmv": spmv, "clocks": clk,
+                "spmv_gbs": spmv_gbs, "roofline": roof, "spmv": spmv, "fcg_spmv": fcg, "clocks": clk,
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(hU.nbytes + hp.nbytes),
                         "d2h_bytes_per_step": int(hU.nbytes + hp.nbytes)},
                 "gpu_launches": int(prof.kernel_launches),

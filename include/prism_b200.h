@@ -406,16 +406,22 @@ int prism_piso_step(const PrismPISOControls* controls, PrismTransport* const* mo
 int prism_needs_pressure_reference(PrismScalar* p, int32_t* out);
 
 /* ---- measurement --------------------------------------------------------- */
-/* Live timing of the SpMV kernel inside BiCGSTAB (v = A p launches), sampled
- * with CUDA events on the launching stream while a profiling window is open.
- * bytes are the algorithmic bytes of the sampled launches:
- * nnz*(value + 4) + 4*(n+1) + 2*n*value (CSR values, columns, row pointers,
- * x read once, y written once). The amg_* fields sample the two FP64 kernels
- * of the AMG V-cycle on the finest level (pre-smoothing + residual, and
- * prolongation + post-smoothing) with their algorithmic bytes:
- *   pre:  nnz*12 + 4*(n+1) + 32*n        (matrix; b, D^-1 read; x, r written)
- *   post: nnz*12 + 4*(n+1) + 36*n + 8*nc (matrix; b, x, D^-1, aggregate map read,
- *                                          output written; coarse correction read)
+/* Live timing of the hot solver kernels, sampled with CUDA events on the
+ * launching stream while a profiling window is open, with the algorithmic
+ * bytes of the sampled launches (nnz: the structural entries of the matrix):
+ *   fp64 / fp32: the SpMV inside BiCGSTAB (v = A p), FP64 / FP32 values:
+ *       nnz*(value + 4) + 4*(n+1) + 2*n*value (values, columns, row pointers,
+ *       x read once, y written once);
+ *   fcg: the SpMV of flexible CG (u = A z with the dots z.q, z.u, z.r), FP64
+ *       matrix: nnz*12 + 4*(n+1) + (zbytes + 24)*n (z read in the
+ *       preconditioner's precision; u written; q, r read);
+ *   amg_down / amg_post (FP64 cycle), amg32_down / amg32_post (FP32 cycle):
+ *       the two kernels of the AMG cycle on the finest level,
+ *       down: nc rows of the smoothed restriction Rt = P^T (I - omega A D^-1),
+ *             rt_nnz*(value + 4) + 4*(nc+1) + value*(n + nc) (Rt; b read, next
+ *             level's b written);
+ *       post: nnz*(value + 4) + 4*(n+1) + (3*value + 4)*n + value*nc (matrix;
+ *             b, D^-1, aggregate map read, output written; coarse correction read).
  * Iterations replayed from a CUDA graph are not sampled. No counterpart in the
  * reference. */
 typedef struct {
@@ -426,13 +432,22 @@ typedef struct {
     double fp32_ms;
     double fp32_bytes;
     int64_t kernel_launches; /* every kernel this library launched in the window */
-    int64_t amg_pre_launches;
-    double amg_pre_ms;
-    double amg_pre_bytes;
+    int64_t amg_down_launches;
+    double amg_down_ms;
+    double amg_down_bytes;
     int64_t amg_post_launches;
     double amg_post_ms;
     double amg_post_bytes;
     int64_t graph_launches; /* solves and steps run as one CUDA graph launch (PrismSolveOpts.graph) */
+    int64_t amg32_down_launches;
+    double amg32_down_ms;
+    double amg32_down_bytes;
+    int64_t amg32_post_launches;
+    double amg32_post_ms;
+    double amg32_post_bytes;
+    int64_t fcg_launches;
+    double fcg_ms;
+    double fcg_bytes;
 } PrismProfile;
 int prism_profile_start(int32_t max_samples);
 int prism_profile_stop(PrismProfile* out);

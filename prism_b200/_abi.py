@@ -115,9 +115,12 @@ class Profile(C.Structure):
     _fields_ = [("fp64_launches", i64), ("fp64_ms", f64), ("fp64_bytes", f64),
                 ("fp32_launches", i64), ("fp32_ms", f64), ("fp32_bytes", f64),
                 ("kernel_launches", i64),
-                ("amg_pre_launches", i64), ("amg_pre_ms", f64), ("amg_pre_bytes", f64),
+                ("amg_down_launches", i64), ("amg_down_ms", f64), ("amg_down_bytes", f64),
                 ("amg_post_launches", i64), ("amg_post_ms", f64), ("amg_post_bytes", f64),
-                ("graph_launches", i64)]
+                ("graph_launches", i64),
+                ("amg32_down_launches", i64), ("amg32_down_ms", f64), ("amg32_down_bytes", f64),
+                ("amg32_post_launches", i64), ("amg32_post_ms", f64), ("amg32_post_bytes", f64),
+                ("fcg_launches", i64), ("fcg_ms", f64), ("fcg_bytes", f64)]
 
 
 PP = C.POINTER(P)

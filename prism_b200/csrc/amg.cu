@@ -17,8 +17,14 @@
 //     segmented sum per coarse entry in a fixed order;
 //   * cycle: V(1,1), damped Jacobi (omega = 0.9) smoothing, coarse correction
 //     scaled by 1.8, or 2.0 for the pressure correction (unsmoothed aggregation
-//     under-corrects), dense inverse
-//     (single-block Gauss-Jordan with partial pivoting) on the coarsest level;
+//     under-corrects; 2.2 when it preconditions flexible CG), dense inverse
+//     (single-block Gauss-Jordan with partial pivoting) on the coarsest level.
+//     Each level's down-sweep is one SpMV with the smoothed restriction
+//     Rt = P^T (I - omega A D^-1): pre-smoothing from zero, residual and
+//     restriction at once (Rt has fewer entries than A: an aggregate's rows share
+//     columns), and the up-sweep forms the pre-smoothed x = omega D^-1 b where it
+//     reads it, so a level costs two launches; Rt's values are refreshed with the
+//     Galerkin operators;
 //   * K-cycle (applyK, for the flexible-CG solve of the pressure correction):
 //     on the levels Amg::kLevel names, the coarse correction is two
 //     flexible-CG steps preconditioned by cycles from that level instead of
@@ -162,6 +168,18 @@ __global__ void keys_kernel(int n, const int* rowptr, const int* col, const int*
     }
 }
 
+// smoothed-restriction keys: agg(i) * ncols + j for every entry (i, j)
+__global__ void rt_keys_kernel(int n, const int* rowptr, const int* col, const int* agg, long long ncols,
+                               long long* keys, int* idx) {
+    int i = blockIdx.x * BS + threadIdx.x;
+    if (i >= n) return;
+    long long ai = agg[i];
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+        keys[k] = ai * ncols + col[k];
+        idx[k] = k;
+    }
+}
+
 __global__ void heads_kernel(int64_t m, const long long* keys, int* head) {
     int64_t q = blockIdx.x * (int64_t)BS + threadIdx.x;
     if (q < m) head[q] = (q == 0 || keys[q] != keys[q - 1]) ? 1 : 0;
@@ -245,6 +263,25 @@ __global__ void galerkin_values_kernel(int nnz_c, const int* seg, const int* src
     double sum = 0.0;
     for (int q = seg[m]; q < seg[m + 1]; ++q) sum += fine_vals[src[q]];
     coarse_vals[coarse_csr_pos[m]] = sum;
+}
+
+// smoothed-restriction values, one coarse row per thread:
+// Rt[c, j] = [agg(j) = c] - omega dinv[j] sum_{i in c} a_ij
+__global__ void rt_values_kernel(int nc, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                 const int* __restrict__ seg, const int* __restrict__ src,
+                                 const int* __restrict__ csr_pos, const int* __restrict__ agg,
+                                 const double* __restrict__ fine_vals, const double* __restrict__ dinv, double omega,
+                                 double* __restrict__ out, float* __restrict__ out32) {
+    const int c = blockIdx.x * BS + threadIdx.x;
+    if (c >= nc) return;
+    for (int e = rowptr[c]; e < rowptr[c + 1]; ++e) {
+        double sum = 0.0;
+        for (int q = seg[e]; q < seg[e + 1]; ++q) sum += fine_vals[src[q]];
+        const int j = col[e];
+        const double v = (agg[j] == c ? 1.0 : 0.0) - omega * dinv[j] * sum;
+        out[csr_pos[e]] = v;
+        if (out32) out32[csr_pos[e]] = (float)v;
+    }
 }
 
 __global__ void dinv_kernel(int n, const int* diag_pos, const double* vals, double* dinv, float* dinv32) {
@@ -367,6 +404,7 @@ __global__ void __launch_bounds__(1024) gauss_jordan_kernel(int n, const double*
 // few, long rows: more lanes per row keep enough loads in flight.
 
 // sum_j A[row, c_j] * xf(c_j); the result is valid in every lane of the row's group
+// (a look-ahead of 4 slots per lane measured slower for the post-smoothing kernel)
 template <typename T, int LPR, typename F>
 __device__ __forceinline__ T rowSum(const int* __restrict__ sl_off, const int* __restrict__ col,
                                     const T* __restrict__ val, int row, bool valid, int sub, F xf) {
@@ -387,54 +425,37 @@ __device__ __forceinline__ T rowSum(const int* __restrict__ sl_off, const int* _
     return sum;
 }
 
-// pre-smoothing from zero and residual: x = omega D^-1 b ; res = b - A x
-// (x at the neighbours formed on the fly, so no separate smoothing pass)
+// down-sweep of a level: the next level's right-hand side bc = Rt b (smoothed
+// restriction: pre-smoothing from zero, residual and restriction in one pass)
 template <typename T, int LPR>
-__global__ void __launch_bounds__(BS) pre_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
-                                                 const T* __restrict__ val, const T* __restrict__ b,
-                                                 const T* __restrict__ dinv, T omega, T* __restrict__ x,
-                                                 T* __restrict__ res, const KState* S) {
+__global__ void __launch_bounds__(BS) down_kernel(int nc, const int* __restrict__ sl_off, const int* __restrict__ col,
+                                                  const T* __restrict__ val, const T* __restrict__ b,
+                                                  T* __restrict__ bc, const KState* S) {
     pdlEnter();
     if (S && S->done) return;
     const int gt = blockIdx.x * BS + threadIdx.x;
     const int row = gt / LPR, sub = gt % LPR;
-    const bool valid = row < n;
-    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, [&](int c) { return omega * dinv[c] * b[c]; });
-    if (valid && sub == 0) {
-        x[row] = omega * dinv[row] * b[row];
-        res[row] = b[row] - sum;
-    }
-}
-
-template <typename T>
-__global__ void restrict_kernel(int nc, const int* m_off, const int* m_idx, const T* res, T* bc, const KState* S) {
-    pdlEnter();
-    if (S && S->done) return;
-    int c = blockIdx.x * BS + threadIdx.x;
-    if (c >= nc) return;
-    T sum = 0;
-    for (int q = m_off[c]; q < m_off[c + 1]; ++q) sum += res[m_idx[q]];
-    bc[c] = sum;
+    const bool valid = row < nc;
+    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, [&](int j) { return b[j]; });
+    if (valid && sub == 0) bc[row] = sum;
 }
 
 // prolongation and post-smoothing: out = xp + omega D^-1 (b - A xp), xp = x + scale * xc[agg]
+// with x = omega D^-1 b the pre-smoothed solution (formed where it is read)
 template <typename T, int LPR>
 __global__ void __launch_bounds__(BS) post_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
                                                   const T* __restrict__ val, const T* __restrict__ b,
-                                                  const T* __restrict__ x, const T* __restrict__ xc,
-                                                  const int* __restrict__ agg, T scale, const T* __restrict__ dinv,
-                                                  T omega, T* __restrict__ out, const KState* S) {
+                                                  const T* __restrict__ xc, const int* __restrict__ agg, T scale,
+                                                  const T* __restrict__ dinv, T omega, T* __restrict__ out,
+                                                  const KState* S) {
     pdlEnter();
     if (S && S->done) return;
     const int gt = blockIdx.x * BS + threadIdx.x;
     const int row = gt / LPR, sub = gt % LPR;
     const bool valid = row < n;
-    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub,
-                                 [&](int c) { return x[c] + scale * xc[agg[c]]; });
-    if (valid && sub == 0) {
-        const T xp = x[row] + scale * xc[agg[row]];
-        out[row] = xp + omega * dinv[row] * (b[row] - sum);
-    }
+    auto xp = [&](int c) { return omega * dinv[c] * b[c] + scale * xc[agg[c]]; };
+    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, xp);
+    if (valid && sub == 0) out[row] = xp(row) + omega * dinv[row] * (b[row] - sum);
 }
 
 // ---- K-cycle (FP64): two flexible-CG steps on a coarse level
@@ -533,14 +554,14 @@ __global__ void __launch_bounds__(BS) k_second_kernel(int n, const int* __restri
 }
 
 // prolongation of a K-cycle correction and post-smoothing:
-// out = xp + omega D^-1 (b - A xp), xp = x + (c1 z1 + c2 z2)[agg]
+// out = xp + omega D^-1 (b - A xp), xp = omega D^-1 b + (c1 z1 + c2 z2)[agg]
 template <int LPR>
 __global__ void __launch_bounds__(BS) post_k_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
                                                     const double* __restrict__ val, const double* __restrict__ b,
-                                                    const double* __restrict__ x, const double* __restrict__ z1,
-                                                    const double* __restrict__ z2, const int* __restrict__ agg,
-                                                    const double* __restrict__ ks, const double* __restrict__ dinv,
-                                                    double omega, double* __restrict__ out, const KState* S) {
+                                                    const double* __restrict__ z1, const double* __restrict__ z2,
+                                                    const int* __restrict__ agg, const double* __restrict__ ks,
+                                                    const double* __restrict__ dinv, double omega,
+                                                    double* __restrict__ out, const KState* S) {
     pdlEnter();
     if (S && S->done) return;
     const double c1 = ks[KS_C1], c2 = ks[KS_C2];
@@ -549,7 +570,7 @@ __global__ void __launch_bounds__(BS) post_k_kernel(int n, const int* __restrict
     const bool valid = row < n;
     auto xp = [&](int c) {
         const int a = agg[c];
-        return x[c] + (c1 * z1[a] + c2 * z2[a]);
+        return omega * dinv[c] * b[c] + (c1 * z1[a] + c2 * z2[a]);
     };
     const double sum = rowSum<double, LPR>(sl_off, col, val, row, valid, sub, xp);
     if (valid && sub == 0) out[row] = xp(row) + omega * dinv[row] * (b[row] - sum);
@@ -592,6 +613,7 @@ void withLpr(int lpr, F&& f) {
 }
 
 // lanes per row: enough threads to fill the GPU once, at most the mean row length
+// (2, 4 or 8 times as many threads measured slower on the 2.1M-cell cavity)
 int lanesPerRow(int n, int64_t nnz) {
     const int64_t target = (int64_t)NUM_SMS * 2048;
     const double mean = n > 0 ? (double)nnz / n : 1.0;
@@ -917,6 +939,64 @@ void members(DevArena& ar, AmgLevel& L, int nc, cudaStream_t s) {
     PB_LAUNCH("amg members");
 }
 
+// Smoothed restriction Rt of level L (aggregates L.agg, nc of them): the fine
+// entries (i, j) sorted by (agg(i), j); each distinct key is one Rt entry.
+void restrictionStructure(DevArena& ar, AmgLevel& L, int nc, cudaStream_t s) {
+    const int n = L.n;
+    const int64_t m = L.nnz;
+    TmpBuf<long long> keys(m, s), keys_s(m, s);
+    TmpBuf<int> idx(m, s), idx_s(m, s), head(m + 1, s), mid(m + 1, s);
+    rt_keys_kernel<<<grid(n), BS, 0, s>>>(n, L.rowptr, L.col, L.agg.p, (long long)n, keys.p, idx.p); countLaunch();
+    int end_bit = 1;
+    while (end_bit < 63 && ((long long)1 << end_bit) < (long long)nc * n) ++end_bit;
+    size_t tb = 0;
+    PB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.p, keys_s.p, idx.p, idx_s.p, m, 0, end_bit, s));
+    TmpBuf<unsigned char> tmp(std::max<size_t>(tb, 1), s);
+    PB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, keys.p, keys_s.p, idx.p, idx_s.p, m, 0, end_bit, s));
+    heads_kernel<<<grid(m), BS, 0, s>>>(m, keys_s.p, head.p); countLaunch();
+    PB_CUDA(cudaMemsetAsync(head.p + m, 0, sizeof(int), s));
+    size_t tb2 = 0;
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb2, head.p, mid.p, m + 1, s));
+    TmpBuf<unsigned char> tmp2(std::max<size_t>(tb2, 1), s);
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(tmp2.p, tb2, head.p, mid.p, m + 1, s));
+    int nnz = 0;
+    PB_CUDA(cudaMemcpyAsync(&nnz, mid.p + m, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    L.rt_nnz = nnz;
+    L.rt_seg.alloc(ar, nnz + 1, s);
+    L.rt_src.alloc(ar, m, s);
+    L.rt_rowptr.alloc(ar, nc + 1, s);
+    L.rt_col.alloc(ar, std::max(nnz, 1), s);
+    coarse_csr_kernel<<<grid(m), BS, 0, s>>>(m, keys_s.p, head.p, mid.p, idx_s.p, L.csr_pos, (long long)n,
+                                             L.rt_seg.p, L.rt_col.p, L.rt_rowptr.p, L.rt_src.p); countLaunch();
+    int hm = (int)m;
+    PB_CUDA(cudaMemcpyAsync(L.rt_seg.p + nnz, &hm, sizeof(int), cudaMemcpyHostToDevice, s));
+    PB_CUDA(cudaMemcpyAsync(L.rt_rowptr.p + nc, &nnz, sizeof(int), cudaMemcpyHostToDevice, s));
+    // SELL layout (rows: aggregates; padded slots point at column 0 with value 0)
+    L.rt_nslices = ceil_div(nc, 32);
+    TmpBuf<int> se(L.rt_nslices + 1, s);
+    PB_CUDA(cudaMemsetAsync(se.p + L.rt_nslices, 0, sizeof(int), s));
+    rowlen_slice_kernel<<<grid(L.rt_nslices), BS, 0, s>>>(nc, L.rt_nslices, L.rt_rowptr.p, se.p); countLaunch();
+    L.rt_sl_off.alloc(ar, L.rt_nslices + 1, s);
+    size_t tb3 = 0;
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb3, se.p, L.rt_sl_off.p, L.rt_nslices + 1, s));
+    TmpBuf<unsigned char> tmp3(std::max<size_t>(tb3, 1), s);
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(tmp3.p, tb3, se.p, L.rt_sl_off.p, L.rt_nslices + 1, s));
+    int sell = 0;
+    PB_CUDA(cudaMemcpyAsync(&sell, L.rt_sl_off.p + L.rt_nslices, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PB_CUDA(cudaStreamSynchronize(s));
+    L.rt_sl_col.alloc(ar, std::max(sell, 1), s);
+    L.rt_csr_pos.alloc(ar, std::max(nnz, 1), s);
+    TmpBuf<int> dummy_diag(nc, s);
+    sell_fill_kernel<<<grid((int64_t)L.rt_nslices * 32), BS, 0, s>>>(nc, L.rt_nslices, L.rt_rowptr.p, L.rt_col.p,
+                                                                      L.rt_sl_off.p, L.rt_sl_col.p, L.rt_csr_pos.p,
+                                                                      dummy_diag.p); countLaunch();
+    L.rt_vals.alloc(ar, std::max(sell, 1), s);
+    L.rt_vals.zero(s);
+    L.rt_lpr = lanesPerRow(nc, nnz);
+    PB_LAUNCH("amg restriction structure");
+}
+
 // returns true if a buffer was allocated
 bool allocCycle(DevArena& ar, AmgLevel& L, bool mixed, bool klevel, cudaStream_t s) {
     bool fresh = false;
@@ -946,6 +1026,11 @@ bool allocCycle(DevArena& ar, AmgLevel& L, bool mixed, bool klevel, cudaStream_t
             L.vals32.zero(s);
             fresh = true;
         }
+        if (L.rt_vals.p && !L.rt_vals32.p) {
+            L.rt_vals32.alloc(ar, L.rt_vals.n, s);
+            L.rt_vals32.zero(s);
+            fresh = true;
+        }
     }
     return fresh;
 }
@@ -966,10 +1051,25 @@ void Amg::forPressure() {
     flex_scale = 2.2;
     const char* e = std::getenv("PRISM_AMG_KCYCLE");
     k_levels = e && e[0] ? std::max(0, std::atoi(e)) : 0;
+    k_mask = 0;
+    for (int l = 1; l <= k_levels && l < 31; ++l) k_mask |= 1u << l;
+    // PRISM_AMG_KLEVELS: the K levels as a list ("2" or "2,3")
+    if (const char* m = std::getenv("PRISM_AMG_KLEVELS")) {
+        k_mask = 0;
+        for (const char* q = m; *q;) {
+            const int l = std::atoi(q);
+            if (l >= 1 && l < 31) k_mask |= 1u << l;
+            while (*q && *q != ',') ++q;
+            if (*q == ',') ++q;
+        }
+        k_levels = 0;
+        for (int l = 1; l < 31; ++l)
+            if (k_mask >> l & 1u) k_levels = l;
+    }
 }
 
 bool Amg::kLevel(size_t l) const {
-    return k_levels > 0 && l >= 1 && l <= (size_t)k_levels && l + 1 < levels.size() && (tail < 0 || (int)l < tail);
+    return l >= 1 && l < 31 && (k_mask >> l & 1u) && l + 1 < levels.size() && (tail < 0 || (int)l < tail);
 }
 
 void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mixed, cudaStream_t s) {
@@ -1039,6 +1139,7 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
             });
             timed(t_mem, [&] {
                 members(arena, L, n2, s);
+                restrictionStructure(arena, L, n2, s);
                 return 0;
             });
             levels.push_back(std::move(C));
@@ -1099,6 +1200,13 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
                                                                                                L->vals32.p); countLaunch();
         }
     }
+    for (size_t l = 0; l + 1 < levels.size(); ++l) {
+        AmgLevel& L = *levels[l];
+        const int nc = levels[l + 1]->n;
+        rt_values_kernel<<<grid(nc), BS, 0, s>>>(nc, L.rt_rowptr.p, L.rt_col.p, L.rt_seg.p, L.rt_src.p,
+                                                 L.rt_csr_pos.p, L.agg.p, L.vals, L.dinv.p, omega, L.rt_vals.p,
+                                                 mixed ? L.rt_vals32.p : nullptr); countLaunch();
+    }
     if (coarse_inv.p) {
         const AmgLevel& C = *levels.back();
         const int n = coarse_n;
@@ -1121,11 +1229,16 @@ namespace {
 template <typename T>
 struct CycleData {
     static const T* vals(const AmgLevel& L);
+    static const T* rt(const AmgLevel& L);
 };
 template <>
 const double* CycleData<double>::vals(const AmgLevel& L) { return L.vals; }
 template <>
 const float* CycleData<float>::vals(const AmgLevel& L) { return L.vals32.p; }
+template <>
+const double* CycleData<double>::rt(const AmgLevel& L) { return L.rt_vals.p; }
+template <>
+const float* CycleData<float>::rt(const AmgLevel& L) { return L.rt_vals32.p; }
 
 template <typename T>
 struct Bufs {
@@ -1230,23 +1343,24 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
     Bufs<T> nb = B(N);
     const bool fine = sample && l == 0;
     const double mat_bytes = (double)L.nnz * (sizeof(T) + 4) + 4.0 * (L.n + 1);
-    int slot = fine ? profBegin(PROF_AMG_PRE, sizeof(T) == 4, mat_bytes + 4.0 * sizeof(T) * L.n, s) : -1;
-    withLpr(L.lpr, [&](auto c) {
+    // down: bc = Rt b (algorithmic bytes: Rt's entries and columns, its row offsets, b, bc)
+    const double rt_bytes = (double)L.rt_nnz * (sizeof(T) + 4) + 4.0 * (N.n + 1) + (double)sizeof(T) * (L.n + N.n);
+    int slot = fine ? profBegin(PROF_AMG_DOWN, sizeof(T) == 4, rt_bytes, s) : -1;
+    withLpr(L.rt_lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
-        launchPdl(pre_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, lb.dinv, omega,
-                  lb.x, lb.res, S);
+        launchPdl(down_kernel<T, P>, grid((int64_t)N.n * P), BS, s, N.n, (const int*)L.rt_sl_off.p,
+                  (const int*)L.rt_sl_col.p, CycleData<T>::rt(L), b, nb.b, S);
     });
     profEnd(slot, s);
-    launchPdl(restrict_kernel<T>, grid(N.n), BS, s, N.n, (const int*)L.m_off.p, (const int*)L.m_idx.p,
-              (const T*)lb.res, nb.b, S);
+    // up: the matrix, b, dinv, agg and out per row, the coarse correction(s) per coarse row
     if constexpr (sizeof(T) == 8) {
         if (kc && A.kLevel(l + 1)) {
             kStep(A, l + 1, S, s);
-            slot = fine ? profBegin(PROF_AMG_POST, false, mat_bytes + 36.0 * L.n + 16.0 * N.n, s) : -1;
+            slot = fine ? profBegin(PROF_AMG_POST, false, mat_bytes + 28.0 * L.n + 16.0 * N.n, s) : -1;
             withLpr(L.lpr, [&](auto c) {
                 constexpr int P = decltype(c)::value;
                 launchPdl(post_k_kernel<P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b,
-                          (const double*)lb.x, (const double*)nb.x2, (const double*)N.kz2.p, (const int*)L.agg.p,
+                          (const double*)nb.x2, (const double*)N.kz2.p, (const int*)L.agg.p,
                           (const double*)(A.kscal.p + (size_t)KS_N * (l + 1)), lb.dinv, omega, out, S);
             });
             profEnd(slot, s);
@@ -1255,12 +1369,12 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
     }
     vcycle<T>(A, l + 1, nb.b, nb.x2, S, s, false, kc);
     slot = fine ? profBegin(PROF_AMG_POST, sizeof(T) == 4,
-                            mat_bytes + (4.0 * sizeof(T) + 4.0) * L.n + (double)sizeof(T) * N.n, s)
+                            mat_bytes + (3.0 * sizeof(T) + 4.0) * L.n + (double)sizeof(T) * N.n, s)
                 : -1;
     withLpr(L.lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
-        launchPdl(post_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, lb.x, nb.x2,
-                  L.agg.p, (T)(kc ? A.flex_scale : A.scale), lb.dinv, omega, out, S);
+        launchPdl(post_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b,
+                  (const T*)nb.x2, (const int*)L.agg.p, (T)(kc ? A.flex_scale : A.scale), lb.dinv, omega, out, S);
     });
     profEnd(slot, s);
 }
@@ -1270,8 +1384,8 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
 void Amg::apply(const double* r, double* z, const KState* S, cudaStream_t s, bool sample) {
     vcycle<double>(*this, 0, r, z, S, s, sample, false);
 }
-void Amg::apply32(const float* r, float* z, const KState* S, cudaStream_t s, bool flexible) {
-    vcycle<float>(*this, 0, r, z, S, s, false, flexible);
+void Amg::apply32(const float* r, float* z, const KState* S, cudaStream_t s, bool flexible, bool sample) {
+    vcycle<float>(*this, 0, r, z, S, s, sample, flexible);
 }
 void Amg::applyK(const double* r, double* z, const KState* S, cudaStream_t s, bool sample) {
     if (k_levels > 0 && !kscal.p) fail(PRISM_INTERNAL, "K-cycle without its buffers (setup first)");

@@ -41,6 +41,15 @@ struct AmgLevel {
     ArenaBuf<float> b32, x32, x232, res32;
     // K-cycle level (Amg::kLevel): second cycle's result, A z1 and the residual r1
     ArenaBuf<double> kz2, kq1, kr1;
+    // smoothed restriction of the down-sweep: b_next = Rt b, Rt = P^T (I - omega A D^-1)
+    // (the residual of one damped-Jacobi step from zero, restricted), next-level rows x
+    // this level's columns: CSR pattern with the sorted A entries each Rt entry sums
+    // (rt_seg/rt_src), SELL layout, FP64 / FP32 values
+    int rt_lpr = 1, rt_nslices = 0;
+    int64_t rt_nnz = 0;
+    ArenaBuf<int> rt_rowptr, rt_col, rt_csr_pos, rt_sl_off, rt_sl_col, rt_seg, rt_src;
+    ArenaBuf<double> rt_vals;
+    ArenaBuf<float> rt_vals32;
 };
 
 struct Amg {
@@ -64,7 +73,8 @@ struct Amg {
     // levels 1..k_levels are K-cycle levels in applyK() (two flexible-CG steps
     // each, instead of one coarse cycle), when they lie above the fused tail and
     // are not the coarsest
-    int k_levels = 0;
+    int k_levels = 0;       // the deepest K level (0: none)
+    unsigned k_mask = 0;    // bit l: level l is a K level
     ArenaBuf<double> kscal, kpart;  // K-cycle scalars (8 per level), block partials of its reductions
     ArenaBuf<unsigned int> kcount;
     // the pressure-correction equation: over-correction 2.0 in V-cycles and
@@ -84,7 +94,8 @@ struct Amg {
     // sample: time the finest-level kernels when a profiling window is open
     void apply(const double* r, double* z, const KState* S, cudaStream_t s, bool sample = false);
     // flexible: the cycle preconditions flexible CG (flex_scale)
-    void apply32(const float* r, float* z, const KState* S, cudaStream_t s, bool flexible = false);
+    void apply32(const float* r, float* z, const KState* S, cudaStream_t s, bool flexible = false,
+                 bool sample = false);
     // z = B r by one cycle with the K-cycle levels and flex_scale (a variable
     // preconditioner: flexible CG only), FP64
     void applyK(const double* r, double* z, const KState* S, cudaStream_t s, bool sample = false);

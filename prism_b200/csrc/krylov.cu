@@ -30,6 +30,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <tuple>
 #include <unordered_map>
 
 #include "krylov.h"
@@ -644,6 +645,10 @@ template <typename T>
 double spmvBytes(const SellMatrix& A) {
     return (double)A.nnz_csr * (sizeof(T) + 4) + 4.0 * (A.n + 1) + 2.0 * A.n * sizeof(T);
 }
+// flexible CG's u = A z: FP64 matrix, z of zbytes, u written, q and r read for the dots
+double fcgSpmvBytes(const SellMatrix& A, int zbytes) {
+    return (double)A.nnz_csr * 12.0 + 4.0 * (A.n + 1) + (zbytes + 24.0) * A.n;
+}
 
 template <typename T>
 struct Vecs {
@@ -757,8 +762,8 @@ void iterateFcgEager(const SellMatrix& A, const double* M, Vecs<double> V, Amg* 
     const int sg = p32 ? waveGrid(k32, ceil_div(A.nslices, WARPS)) : waveGrid(k64, ceil_div(A.nslices, WARPS));
     for (long long it = 0; it < count; ++it) {
         if (p32) {
-            amg->apply32(w.y32.p, w.z32.p, S, s, true);
-            const int slot = sample ? profBegin(PROF_SPMV, false, spmvBytes<double>(A), s) : -1;
+            amg->apply32(w.y32.p, w.z32.p, S, s, true, sample);
+            const int slot = sample ? profBegin(PROF_FCG_SPMV, false, fcgSpmvBytes(A, 4), s) : -1;
             launchPdl(k32, sg, BS, s, A.nslices, n, A.sl_off, A.col, M, (const float*)w.z32.p, V.t,
                       (const double*)V.v, (const double*)V.r, w.partials.p, w.counter.p, S);
             profEnd(slot, s);
@@ -766,7 +771,7 @@ void iterateFcgEager(const SellMatrix& A, const double* M, Vecs<double> V, Amg* 
                       (const double*)V.t, w.y32.p, w.partials.p, w.counter.p, S);
         } else {
             amg->applyK(V.r, y, S, s, sample);
-            const int slot = sample ? profBegin(PROF_SPMV, false, spmvBytes<double>(A), s) : -1;
+            const int slot = sample ? profBegin(PROF_FCG_SPMV, false, fcgSpmvBytes(A, 8), s) : -1;
             launchPdl(k64, sg, BS, s, A.nslices, n, A.sl_off, A.col, M, (const double*)y, V.t, (const double*)V.v,
                       (const double*)V.r, w.partials.p, w.counter.p, S);
             profEnd(slot, s);
@@ -1148,16 +1153,22 @@ void profileStop(PrismProfile* out) {
         PB_CUDA(cudaEventSynchronize(smp.b));
         float ms = 0.f;
         PB_CUDA(cudaEventElapsedTime(&ms, smp.a, smp.b));
-        if (smp.kind == PROF_AMG_PRE) {
-            if (smp.fp32) continue;
-            out->amg_pre_launches++;
-            out->amg_pre_ms += ms;
-            out->amg_pre_bytes += smp.bytes;
+        if (smp.kind == PROF_AMG_DOWN) {
+            auto [l, t, b] = smp.fp32 ? std::tie(out->amg32_down_launches, out->amg32_down_ms, out->amg32_down_bytes)
+                                       : std::tie(out->amg_down_launches, out->amg_down_ms, out->amg_down_bytes);
+            l++;
+            t += ms;
+            b += smp.bytes;
         } else if (smp.kind == PROF_AMG_POST) {
-            if (smp.fp32) continue;
-            out->amg_post_launches++;
-            out->amg_post_ms += ms;
-            out->amg_post_bytes += smp.bytes;
+            auto [l, t, b] = smp.fp32 ? std::tie(out->amg32_post_launches, out->amg32_post_ms, out->amg32_post_bytes)
+                                       : std::tie(out->amg_post_launches, out->amg_post_ms, out->amg_post_bytes);
+            l++;
+            t += ms;
+            b += smp.bytes;
+        } else if (smp.kind == PROF_FCG_SPMV) {
+            out->fcg_launches++;
+            out->fcg_ms += ms;
+            out->fcg_bytes += smp.bytes;
         } else if (smp.fp32) {
             out->fp32_launches++;
             out->fp32_ms += ms;

@@ -20,11 +20,11 @@ struct SellMatrix {
 void jacobiStepNoAlloc(int64_t n, const int32_t* rowptr, const int32_t* col, const double* values, const double* b,
                        double* x, cudaStream_t stream);
 
-// Sampled CUDA-event timing of the BiCGSTAB SpMV launches (v = A p) and of
-// the finest-level AMG cycle kernels.
+// Sampled CUDA-event timing of the BiCGSTAB and flexible-CG SpMV launches and
+// of the finest-level AMG cycle kernels.
 void profileStart(int max_samples);
 void profileStop(PrismProfile* out);
-enum ProfKind { PROF_SPMV = 0, PROF_AMG_PRE = 1, PROF_AMG_POST = 2 };
+enum ProfKind { PROF_SPMV = 0, PROF_AMG_DOWN = 1, PROF_AMG_POST = 2, PROF_FCG_SPMV = 3 };
 // Opens a sample (records the start event on s) when a window is open and has
 // room: returns its slot, else -1. profEnd(slot) records the end event.
 int profBegin(int kind, bool fp32, double bytes, cudaStream_t s);
