@@ -265,23 +265,27 @@ __global__ void galerkin_values_kernel(int nnz_c, const int* seg, const int* src
     coarse_vals[coarse_csr_pos[m]] = sum;
 }
 
-// smoothed-restriction values, one coarse row per thread:
+// smoothed-restriction values, one entry per thread (erow: the entry's row):
 // Rt[c, j] = [agg(j) = c] - omega dinv[j] sum_{i in c} a_ij
-__global__ void rt_values_kernel(int nc, const int* __restrict__ rowptr, const int* __restrict__ col,
+__global__ void rt_values_kernel(int nnz, const int* __restrict__ erow, const int* __restrict__ col,
                                  const int* __restrict__ seg, const int* __restrict__ src,
                                  const int* __restrict__ csr_pos, const int* __restrict__ agg,
                                  const double* __restrict__ fine_vals, const double* __restrict__ dinv, double omega,
                                  double* __restrict__ out, float* __restrict__ out32) {
-    const int c = blockIdx.x * BS + threadIdx.x;
-    if (c >= nc) return;
-    for (int e = rowptr[c]; e < rowptr[c + 1]; ++e) {
-        double sum = 0.0;
-        for (int q = seg[e]; q < seg[e + 1]; ++q) sum += fine_vals[src[q]];
-        const int j = col[e];
-        const double v = (agg[j] == c ? 1.0 : 0.0) - omega * dinv[j] * sum;
-        out[csr_pos[e]] = v;
-        if (out32) out32[csr_pos[e]] = (float)v;
-    }
+    const int e = blockIdx.x * BS + threadIdx.x;
+    if (e >= nnz) return;
+    double sum = 0.0;
+    for (int q = seg[e]; q < seg[e + 1]; ++q) sum += fine_vals[src[q]];
+    const int j = col[e];
+    const double v = (agg[j] == erow[e] ? 1.0 : 0.0) - omega * dinv[j] * sum;
+    out[csr_pos[e]] = v;
+    if (out32) out32[csr_pos[e]] = (float)v;
+}
+
+__global__ void entry_rows_kernel(int n, const int* rowptr, int* erow) {
+    const int r = blockIdx.x * BS + threadIdx.x;
+    if (r >= n) return;
+    for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) erow[e] = r;
 }
 
 __global__ void dinv_kernel(int n, const int* diag_pos, const double* vals, double* dinv, float* dinv32) {
@@ -972,6 +976,8 @@ void restrictionStructure(DevArena& ar, AmgLevel& L, int nc, cudaStream_t s) {
     int hm = (int)m;
     PB_CUDA(cudaMemcpyAsync(L.rt_seg.p + nnz, &hm, sizeof(int), cudaMemcpyHostToDevice, s));
     PB_CUDA(cudaMemcpyAsync(L.rt_rowptr.p + nc, &nnz, sizeof(int), cudaMemcpyHostToDevice, s));
+    L.rt_erow.alloc(ar, std::max(nnz, 1), s);
+    entry_rows_kernel<<<grid(nc), BS, 0, s>>>(nc, L.rt_rowptr.p, L.rt_erow.p); countLaunch();
     // SELL layout (rows: aggregates; padded slots point at column 0 with value 0)
     L.rt_nslices = ceil_div(nc, 32);
     TmpBuf<int> se(L.rt_nslices + 1, s);
@@ -1073,6 +1079,9 @@ bool Amg::kLevel(size_t l) const {
 }
 
 void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mixed, cudaStream_t s) {
+    if (values_current && built && !levels.empty() && levels[0]->n == A.n && levels[0]->sl_off == A.sl_off &&
+        levels[0]->vals == A.vals && (!mixed || has32))
+        return;
     if (!built || levels.empty() || levels[0]->n != A.n || levels[0]->sl_off != A.sl_off) {
         levels.clear();
         coarse_a.release();
@@ -1202,10 +1211,9 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
     }
     for (size_t l = 0; l + 1 < levels.size(); ++l) {
         AmgLevel& L = *levels[l];
-        const int nc = levels[l + 1]->n;
-        rt_values_kernel<<<grid(nc), BS, 0, s>>>(nc, L.rt_rowptr.p, L.rt_col.p, L.rt_seg.p, L.rt_src.p,
-                                                 L.rt_csr_pos.p, L.agg.p, L.vals, L.dinv.p, omega, L.rt_vals.p,
-                                                 mixed ? L.rt_vals32.p : nullptr); countLaunch();
+        rt_values_kernel<<<grid(L.rt_nnz), BS, 0, s>>>((int)L.rt_nnz, L.rt_erow.p, L.rt_col.p, L.rt_seg.p,
+                                                       L.rt_src.p, L.rt_csr_pos.p, L.agg.p, L.vals, L.dinv.p, omega,
+                                                       L.rt_vals.p, mixed ? L.rt_vals32.p : nullptr); countLaunch();
     }
     if (coarse_inv.p) {
         const AmgLevel& C = *levels.back();

@@ -47,7 +47,7 @@ struct AmgLevel {
     // (rt_seg/rt_src), SELL layout, FP64 / FP32 values
     int rt_lpr = 1, rt_nslices = 0;
     int64_t rt_nnz = 0;
-    ArenaBuf<int> rt_rowptr, rt_col, rt_csr_pos, rt_sl_off, rt_sl_col, rt_seg, rt_src;
+    ArenaBuf<int> rt_rowptr, rt_erow, rt_col, rt_csr_pos, rt_sl_off, rt_sl_col, rt_seg, rt_src;
     ArenaBuf<double> rt_vals;
     ArenaBuf<float> rt_vals32;
 };
@@ -61,6 +61,10 @@ struct Amg {
     ArenaBuf<int> coarse_bad;
     bool built = false;
     bool has32 = false;
+    // set by the caller while the matrix values are those of the last setup (the
+    // pressure correction's later correctors, the later outer steps of one solve):
+    // setup() then keeps the hierarchy's values instead of recomputing the same ones
+    bool values_current = false;
     uint64_t generation = 0;  // new process-wide value whenever a buffer of the hierarchy is (re)allocated
     int tail = -1;            // first level of the fused coarse tail (-1: every level launches its own kernels)
     // V-cycle smoother weight and coarse-correction factor; the pressure-correction

@@ -536,6 +536,17 @@ int choosePreconditioner(int pc, int64_t n) {
     return pc;
 }
 
+// Amg::values_current for one solve (cleared however the solve ends)
+struct HoldAmgValues {
+    Amg* a;
+    HoldAmgValues(Amg* amg, bool on) : a(amg) {
+        if (a) a->values_current = on;
+    }
+    ~HoldAmgValues() {
+        if (a) a->values_current = false;
+    }
+};
+
 // PRISM_PC_AUTO at AMG sizes: an equation whose off-diagonal row sums stay below this
 // fraction of the diagonal (an under-relaxed momentum predictor: about the relaxation
 // factor) is solved with Jacobi, whose iteration then converges fast and costs a third
@@ -623,6 +634,7 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
         if (o.method == PRISM_SOLVER_JACOBI) {
             jacobiStep(A, eq.b.p, phi.v.p, m.kw, m.stream);
         } else {
+            const HoldAmgValues hold(amg, eq.matrix_unchanged || iter > 0);  // A is fixed within one solve
             KrylovOut k = bicgstab(A, eq.b.p, phi.v.p, ktol, kmax, o.precision, itol, m.kw, m.stream, amg,
                                    m.pat.rowptr.p, m.pat.col.p, flexibleFor(eq, o, amg));
             r.krylov_iterations += k.iterations;
@@ -834,6 +846,13 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
     pEqn.spd = true;
     for (int64_t i = 0; i <= c.non_ortho_correctors; ++i) {
         PhaseTimer pt("pressure corrector " + std::to_string(i), m.stream);
+        // the correctors re-assemble the same matrix (D and the mesh are fixed; only the
+        // explicit non-orthogonal part of b changes)
+        struct Unchanged {
+            Transport& e;
+            Unchanged(Transport& t, bool on) : e(t) { e.matrix_unchanged = on; }
+            ~Unchanged() { e.matrix_unchanged = false; }
+        } unchanged(pEqn, i > 0);
         auto r = solve(pEqn, inner(so, c.pressure_max_iter, c.pressure_residual, c.p_ref_cell, c.p_ref_value, true));
         rep.push_back({pp->name + "_corr_" + std::to_string(i), r.iterations, r.initial_residual, r.final_residual,
                        r.converged != 0});
@@ -1216,6 +1235,7 @@ PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o) {
         cudaStream_t body = m.cs.at(0);
         beginConditional(s, cudaGraphCondTypeWhile, outer, body);
         phi.event += 2;
+        const HoldAmgValues hold(amg, eq.matrix_unchanged);
         emitBicgstab(A, eq.b.p, phi.v.p, ktol, kmax, m.kw, body, amg, m.pat.rowptr.p, m.pat.col.p, ctl, m.cs, 1,
                      flexibleFor(eq, o, amg));
         ++phi.event;

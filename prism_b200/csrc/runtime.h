@@ -143,6 +143,9 @@ struct Transport {
     // PRISM_PC_AUTO at AMG sizes, decided on the equation's first solve: Jacobi when
     // its matrix is diagonally dominant enough (offDiagonalRatio), else AMG (0: not yet)
     int auto_pc = 0;
+    // the next solves assemble the same matrix as the last one (only b changes):
+    // its AMG hierarchy keeps its values
+    bool matrix_unchanged = false;
     // adjoint: A^T values and the AMG hierarchy of A^T
     DevBuf<double> AT;
     std::shared_ptr<Amg> amg_adj;

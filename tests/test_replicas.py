@@ -85,4 +85,6 @@ def test_reference_arm_under_torchrun():
     d = lines[0]
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["e2e"]["h2d_bytes_per_step"] == 0
-    assert d["config"]["cells"] == 16 * 16
+    assert d["config"]["cells"] == 1448 * 1448 and d["config"]["sample_cells"] == 16 * 16
+    # the sample's measured time per step, its it/s scaled to the stated cavity by the cell ratio
+    assert d["value"] == pytest.approx(1000.0 / d["ms_per_step"] * (16 * 16) / (1448 * 1448))
