@@ -416,12 +416,16 @@ int prism_needs_pressure_reference(PrismScalar* p, int32_t* out);
  *       matrix: nnz*12 + 4*(n+1) + (zbytes + 24)*n (z read in the
  *       preconditioner's precision; u written; q, r read);
  *   amg_down / amg_post (FP64 cycle), amg32_down / amg32_post (FP32 cycle):
- *       the two kernels of the AMG cycle on the finest level,
- *       down: nc rows of the smoothed restriction Rt = P^T (I - omega A D^-1),
+ *       the AMG cycle's down-sweep and up-sweep kernels on the finest level,
+ *       down, by the smoothed restriction Rt = P^T (I - omega A D^-1) (nc rows):
  *             rt_nnz*(value + 4) + 4*(nc+1) + value*(n + nc) (Rt; b read, next
  *             level's b written);
+ *       down, by pre-smoothing with the residual (the member sums not sampled):
+ *             nnz*(value + 4) + 4*(n+1) + 4*value*n (matrix; b, D^-1 read; x, r
+ *             written);
  *       post: nnz*(value + 4) + 4*(n+1) + (3*value + 4)*n + value*nc (matrix;
- *             b, D^-1, aggregate map read, output written; coarse correction read).
+ *             b, D^-1, aggregate map read, output written; coarse correction
+ *             read), one value per row more when x was stored by the down-sweep.
  * Iterations replayed from a CUDA graph are not sampled. No counterpart in the
  * reference. */
 typedef struct {

@@ -429,6 +429,37 @@ __device__ __forceinline__ T rowSum(const int* __restrict__ sl_off, const int* _
     return sum;
 }
 
+// pre-smoothing from zero and residual (the down-sweep of a level without the
+// smoothed restriction): x = omega D^-1 b ; res = b - A x, x at the neighbours
+// formed on the fly; restrict_kernel then sums the residuals of each aggregate
+template <typename T, int LPR>
+__global__ void __launch_bounds__(BS) pre_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
+                                                 const T* __restrict__ val, const T* __restrict__ b,
+                                                 const T* __restrict__ dinv, T omega, T* __restrict__ x,
+                                                 T* __restrict__ res, const KState* S) {
+    pdlEnter();
+    if (S && S->done) return;
+    const int gt = blockIdx.x * BS + threadIdx.x;
+    const int row = gt / LPR, sub = gt % LPR;
+    const bool valid = row < n;
+    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, [&](int c) { return omega * dinv[c] * b[c]; });
+    if (valid && sub == 0) {
+        x[row] = omega * dinv[row] * b[row];
+        res[row] = b[row] - sum;
+    }
+}
+
+template <typename T>
+__global__ void restrict_kernel(int nc, const int* m_off, const int* m_idx, const T* res, T* bc, const KState* S) {
+    pdlEnter();
+    if (S && S->done) return;
+    int c = blockIdx.x * BS + threadIdx.x;
+    if (c >= nc) return;
+    T sum = 0;
+    for (int q = m_off[c]; q < m_off[c + 1]; ++q) sum += res[m_idx[q]];
+    bc[c] = sum;
+}
+
 // down-sweep of a level: the next level's right-hand side bc = Rt b (smoothed
 // restriction: pre-smoothing from zero, residual and restriction in one pass)
 template <typename T, int LPR>
@@ -445,19 +476,23 @@ __global__ void __launch_bounds__(BS) down_kernel(int nc, const int* __restrict_
 }
 
 // prolongation and post-smoothing: out = xp + omega D^-1 (b - A xp), xp = x + scale * xc[agg]
-// with x = omega D^-1 b the pre-smoothed solution (formed where it is read)
-template <typename T, int LPR>
+// with x = omega D^-1 b the pre-smoothed solution: stored by pre_kernel (SX), or formed
+// where it is read (after the smoothed restriction)
+template <typename T, int LPR, bool SX>
 __global__ void __launch_bounds__(BS) post_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
                                                   const T* __restrict__ val, const T* __restrict__ b,
-                                                  const T* __restrict__ xc, const int* __restrict__ agg, T scale,
-                                                  const T* __restrict__ dinv, T omega, T* __restrict__ out,
-                                                  const KState* S) {
+                                                  const T* __restrict__ x, const T* __restrict__ xc,
+                                                  const int* __restrict__ agg, T scale, const T* __restrict__ dinv,
+                                                  T omega, T* __restrict__ out, const KState* S) {
     pdlEnter();
     if (S && S->done) return;
     const int gt = blockIdx.x * BS + threadIdx.x;
     const int row = gt / LPR, sub = gt % LPR;
     const bool valid = row < n;
-    auto xp = [&](int c) { return omega * dinv[c] * b[c] + scale * xc[agg[c]]; };
+    auto xp = [&](int c) {
+        if constexpr (SX) return x[c] + scale * xc[agg[c]];
+        else return omega * dinv[c] * b[c] + scale * xc[agg[c]];
+    };
     const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, xp);
     if (valid && sub == 0) out[row] = xp(row) + omega * dinv[row] * (b[row] - sum);
 }
@@ -558,14 +593,14 @@ __global__ void __launch_bounds__(BS) k_second_kernel(int n, const int* __restri
 }
 
 // prolongation of a K-cycle correction and post-smoothing:
-// out = xp + omega D^-1 (b - A xp), xp = omega D^-1 b + (c1 z1 + c2 z2)[agg]
-template <int LPR>
+// out = xp + omega D^-1 (b - A xp), xp = x + (c1 z1 + c2 z2)[agg], x as in post_kernel
+template <int LPR, bool SX>
 __global__ void __launch_bounds__(BS) post_k_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
                                                     const double* __restrict__ val, const double* __restrict__ b,
-                                                    const double* __restrict__ z1, const double* __restrict__ z2,
-                                                    const int* __restrict__ agg, const double* __restrict__ ks,
-                                                    const double* __restrict__ dinv, double omega,
-                                                    double* __restrict__ out, const KState* S) {
+                                                    const double* __restrict__ x, const double* __restrict__ z1,
+                                                    const double* __restrict__ z2, const int* __restrict__ agg,
+                                                    const double* __restrict__ ks, const double* __restrict__ dinv,
+                                                    double omega, double* __restrict__ out, const KState* S) {
     pdlEnter();
     if (S && S->done) return;
     const double c1 = ks[KS_C1], c2 = ks[KS_C2];
@@ -574,7 +609,8 @@ __global__ void __launch_bounds__(BS) post_k_kernel(int n, const int* __restrict
     const bool valid = row < n;
     auto xp = [&](int c) {
         const int a = agg[c];
-        return omega * dinv[c] * b[c] + (c1 * z1[a] + c2 * z2[a]);
+        if constexpr (SX) return x[c] + (c1 * z1[a] + c2 * z2[a]);
+        else return omega * dinv[c] * b[c] + (c1 * z1[a] + c2 * z2[a]);
     };
     const double sum = rowSum<double, LPR>(sl_off, col, val, row, valid, sub, xp);
     if (valid && sub == 0) out[row] = xp(row) + omega * dinv[row] * (b[row] - sum);
@@ -614,6 +650,22 @@ void withLpr(int lpr, F&& f) {
         case 16: f(std::integral_constant<int, 16>{}); break;
         default: f(std::integral_constant<int, 32>{}); break;
     }
+}
+
+// Down-sweep of level l (n rows, nnz entries): the smoothed restriction (one launch)
+// or pre-smoothing + member-sum restriction (two launches, the smoothed x stored for
+// the up-sweep). The coarse levels are latency-bound: one launch fewer wins. On the
+// finest level the bytes decide: Rt has about as many entries as A for 3-D stencils
+// (C3 128^3: level-0 down 59.6 us against 46.5 + 10 us, and the up-sweep 63 against
+// 53.5 us when it forms x itself) and fewer for 2-D ones (the cavity: 23.3 against
+// 24.5 + 8 us). PRISM_AMG_RT=0 / 1 forces either on every level.
+bool useRestriction(size_t l, int n, int64_t nnz) {
+    static const int force = [] {
+        const char* e = std::getenv("PRISM_AMG_RT");
+        return e && e[0] ? std::atoi(e) : -1;
+    }();
+    if (force >= 0) return force != 0;
+    return l >= 1 || (n > 0 && (double)nnz / n <= 6.0);
 }
 
 // lanes per row: enough threads to fill the GPU once, at most the mean row length
@@ -1108,7 +1160,7 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
         L0->vals = A.vals;
         levels.push_back(std::move(L0));
         // PRISM_VERBOSE: host time of the setup phases (stream drained around each)
-        double t_match = 0.0, t_gal = 0.0, t_mem = 0.0;
+        double t_match = 0.0, t_gal = 0.0, t_mem = 0.0, t_rt = 0.0;
         auto timed = [&](double& acc, auto&& f) {
             if (!verbose()) return f();
             PB_CUDA(cudaStreamSynchronize(s));
@@ -1148,9 +1200,9 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
             });
             timed(t_mem, [&] {
                 members(arena, L, n2, s);
-                restrictionStructure(arena, L, n2, s);
                 return 0;
             });
+
             levels.push_back(std::move(C));
         }
         coarse_n = levels.back()->n;
@@ -1161,12 +1213,25 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
                 tail = (int)l;
                 break;
             }
+        // the down-sweep of each level that runs its own kernels (above the fused tail)
+        for (size_t l = 0; l + 1 < levels.size() && (tail < 0 || (int)l < tail); ++l) {
+            AmgLevel& L = *levels[l];
+            L.use_rt = useRestriction(l, L.n, L.nnz);
+            if (L.use_rt)
+                timed(t_rt, [&] {
+                    restrictionStructure(arena, L, levels[l + 1]->n, s);
+                    return 0;
+                });
+        }
         if (verbose()) {
             std::fprintf(stderr, "[prism amg] hierarchy:");
             for (auto& L : levels) std::fprintf(stderr, " %d/%lld/%d", L->n, (long long)L->nnz, L->lpr);
             std::fprintf(stderr, " (rows/entries/lanes per row), coarsest %s, fused tail from level %d; matching %.1f ms, "
-                         "galerkin %.1f ms, members %.1f ms\n",
-                         coarse_n <= DENSE_MAX ? "dense" : "Jacobi", tail, t_match, t_gal, t_mem);
+                         "galerkin %.1f ms, members %.1f ms, smoothed restriction %.1f ms (levels:",
+                         coarse_n <= DENSE_MAX ? "dense" : "Jacobi", tail, t_match, t_gal, t_mem, t_rt);
+            for (size_t l = 0; l + 1 < levels.size(); ++l)
+                if (levels[l]->use_rt) std::fprintf(stderr, " %zu/%lld", l, (long long)levels[l]->rt_nnz);
+            std::fprintf(stderr, ")\n");
         }
         if (coarse_n <= DENSE_MAX) {
             coarse_a.alloc(arena, (size_t)coarse_n * coarse_n, s);
@@ -1211,6 +1276,7 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
     }
     for (size_t l = 0; l + 1 < levels.size(); ++l) {
         AmgLevel& L = *levels[l];
+        if (!L.use_rt) continue;
         rt_values_kernel<<<grid(L.rt_nnz), BS, 0, s>>>((int)L.rt_nnz, L.rt_erow.p, L.rt_col.p, L.rt_seg.p,
                                                        L.rt_src.p, L.rt_csr_pos.p, L.agg.p, L.vals, L.dinv.p, omega,
                                                        L.rt_vals.p, mixed ? L.rt_vals32.p : nullptr); countLaunch();
@@ -1351,23 +1417,42 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
     Bufs<T> nb = B(N);
     const bool fine = sample && l == 0;
     const double mat_bytes = (double)L.nnz * (sizeof(T) + 4) + 4.0 * (L.n + 1);
-    // down: bc = Rt b (algorithmic bytes: Rt's entries and columns, its row offsets, b, bc)
-    const double rt_bytes = (double)L.rt_nnz * (sizeof(T) + 4) + 4.0 * (N.n + 1) + (double)sizeof(T) * (L.n + N.n);
-    int slot = fine ? profBegin(PROF_AMG_DOWN, sizeof(T) == 4, rt_bytes, s) : -1;
-    withLpr(L.rt_lpr, [&](auto c) {
-        constexpr int P = decltype(c)::value;
-        launchPdl(down_kernel<T, P>, grid((int64_t)N.n * P), BS, s, N.n, (const int*)L.rt_sl_off.p,
-                  (const int*)L.rt_sl_col.p, CycleData<T>::rt(L), b, nb.b, S);
-    });
-    profEnd(slot, s);
-    // up: the matrix, b, dinv, agg and out per row, the coarse correction(s) per coarse row
+    const T scale = (T)(kc ? A.flex_scale : A.scale);
+    const bool rt = L.use_rt;
+    if (rt) {
+        // down: bc = Rt b (algorithmic bytes: Rt's entries and columns, its row offsets, b, bc)
+        const double rt_bytes =
+            (double)L.rt_nnz * (sizeof(T) + 4) + 4.0 * (N.n + 1) + (double)sizeof(T) * (L.n + N.n);
+        int slot = fine ? profBegin(PROF_AMG_DOWN, sizeof(T) == 4, rt_bytes, s) : -1;
+        withLpr(L.rt_lpr, [&](auto c) {
+            constexpr int P = decltype(c)::value;
+            launchPdl(down_kernel<T, P>, grid((int64_t)N.n * P), BS, s, N.n, (const int*)L.rt_sl_off.p,
+                      (const int*)L.rt_sl_col.p, CycleData<T>::rt(L), b, nb.b, S);
+        });
+        profEnd(slot, s);
+    } else {
+        // down: pre-smoothing with the residual (matrix; b, D^-1 read; x, r written), then
+        // the members' residuals summed per aggregate
+        int slot = fine ? profBegin(PROF_AMG_DOWN, sizeof(T) == 4, mat_bytes + 4.0 * sizeof(T) * L.n, s) : -1;
+        withLpr(L.lpr, [&](auto c) {
+            constexpr int P = decltype(c)::value;
+            launchPdl(pre_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, lb.dinv,
+                      omega, lb.x, lb.res, S);
+        });
+        profEnd(slot, s);
+        launchPdl(restrict_kernel<T>, grid(N.n), BS, s, N.n, (const int*)L.m_off.p, (const int*)L.m_idx.p,
+                  (const T*)lb.res, nb.b, S);
+    }
+    // up: the matrix, b, D^-1 (or x), the aggregate map and out per row, the coarse correction(s)
+    const double up_bytes = mat_bytes + ((rt ? 3.0 : 4.0) * sizeof(T) + 4.0) * L.n;
     if constexpr (sizeof(T) == 8) {
         if (kc && A.kLevel(l + 1)) {
             kStep(A, l + 1, S, s);
-            slot = fine ? profBegin(PROF_AMG_POST, false, mat_bytes + 28.0 * L.n + 16.0 * N.n, s) : -1;
+            const int slot = fine ? profBegin(PROF_AMG_POST, false, up_bytes + 16.0 * N.n, s) : -1;
             withLpr(L.lpr, [&](auto c) {
                 constexpr int P = decltype(c)::value;
-                launchPdl(post_k_kernel<P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b,
+                auto k = rt ? post_k_kernel<P, false> : post_k_kernel<P, true>;
+                launchPdl(k, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, (const double*)lb.x,
                           (const double*)nb.x2, (const double*)N.kz2.p, (const int*)L.agg.p,
                           (const double*)(A.kscal.p + (size_t)KS_N * (l + 1)), lb.dinv, omega, out, S);
             });
@@ -1376,13 +1461,12 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
         }
     }
     vcycle<T>(A, l + 1, nb.b, nb.x2, S, s, false, kc);
-    slot = fine ? profBegin(PROF_AMG_POST, sizeof(T) == 4,
-                            mat_bytes + (3.0 * sizeof(T) + 4.0) * L.n + (double)sizeof(T) * N.n, s)
-                : -1;
+    const int slot = fine ? profBegin(PROF_AMG_POST, sizeof(T) == 4, up_bytes + (double)sizeof(T) * N.n, s) : -1;
     withLpr(L.lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
-        launchPdl(post_kernel<T, P>, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b,
-                  (const T*)nb.x2, (const int*)L.agg.p, (T)(kc ? A.flex_scale : A.scale), lb.dinv, omega, out, S);
+        auto k = rt ? post_kernel<T, P, false> : post_kernel<T, P, true>;
+        launchPdl(k, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, (const T*)lb.x,
+                  (const T*)nb.x2, (const int*)L.agg.p, scale, lb.dinv, omega, out, S);
     });
     profEnd(slot, s);
 }

@@ -45,6 +45,7 @@ struct AmgLevel {
     // (the residual of one damped-Jacobi step from zero, restricted), next-level rows x
     // this level's columns: CSR pattern with the sorted A entries each Rt entry sums
     // (rt_seg/rt_src), SELL layout, FP64 / FP32 values
+    bool use_rt = false;  // down-sweep by Rt (else pre-smoothing + member-sum restriction)
     int rt_lpr = 1, rt_nslices = 0;
     int64_t rt_nnz = 0;
     ArenaBuf<int> rt_rowptr, rt_erow, rt_col, rt_csr_pos, rt_sl_off, rt_sl_col, rt_seg, rt_src;
