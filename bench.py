@@ -266,7 +266,7 @@ def transport_exact(mesh):
 def transport_time_to_tol(mesh, precision, ref, tol=1e-8, preconditioner="auto"):
     """Seconds (CUDA events) for one solve() step from T = 0 (assembly included) to reach
     ||T - x*|| / ||x*|| <= tol: the loosest Krylov tolerance of a 10^-0.5 ladder that meets
-    the error is timed (the fastest of three identical runs, so that a one-off host stall in
+    the error is timed (the fastest of five identical runs, so that a one-off host stall in
     one run does not decide the figure)."""
     import numpy as np
     import torch
@@ -278,7 +278,7 @@ def transport_time_to_tol(mesh, precision, ref, tol=1e-8, preconditioner="auto")
         solver = api.BiCGSTAB(precision=precision, krylov_tol=ktol, krylov_max_iter=100000,
                               preconditioner=preconditioner)
         best = None
-        for rep in range(3):
+        for rep in range(5):
             T, keep, eqn = transport_eqn(mesh)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
