@@ -228,6 +228,11 @@ int prism_scalar_face_values(PrismScalar* s, double* out);
 int prism_scalar_grad(PrismScalar* s, double* grad_out);
 /* computeAllCellGradients (forced sweep) */
 int prism_scalar_compute_gradients(PrismScalar* s);
+/* Scalar::setGradScheme (scalar.cpp:252-258): a new gradient scheme of the given
+ * kind (PRISM_GRAD_*) replaces the field's; its gradients start from zero and are
+ * recomputed on the next request. A vector's component changes alone (a clone
+ * that shared the old scheme keeps it). */
+int prism_scalar_set_grad_scheme(PrismScalar* s, int32_t grad_scheme);
 /* time-step history (field/history.cpp:1-63): setHistorySize (scalar.cpp:306-308;
  * shrinking drops the oldest steps, 0 clears), updatePrevTimeSteps
  * (scalar.cpp:322-324: the current values become step 0), update (scalar.cpp:
@@ -280,6 +285,14 @@ int prism_vector_to_points(PrismVector* v, double* point_data);
 int prism_tensor_create(PrismMesh* mesh, const char* name, const double* values,
                         PrismTensor** out);
 int prism_tensor_destroy(PrismTensor* t);
+
+/* ops::rhieChowCorrectFace over a face-value field, as solvePressureEquation
+ * applies it (SIMPLE.cpp:136-138, operations/rhie_chow.h:47-63): mdot's face
+ * values become U.valueAtFace on every boundary face and the Rhie-Chow corrected
+ * U_f - D_f (grad p_f^calculated - grad p_f^averaged) on every interior face, and
+ * its face fluxes (read with prism_vector_face_flux) their dot products with the
+ * face area vectors. p's gradient is computed first if stale. */
+int prism_rhie_chow(PrismVector* mdot, PrismVector* U, PrismTensor* D, PrismScalar* p);
 
 /* ---- equations ------------------------------------------------------------ */
 int prism_transport_create(PrismScalar* phi, PrismTransport** out);

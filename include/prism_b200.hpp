@@ -164,6 +164,8 @@ class Scalar {
     auto prevPrevValues() const { return getHistory(1); }
     void setFaceValues(const std::vector<double>& fv) { check(prism_scalar_set_face_values(_h.get(), fv.data())); }
     void clearFaceValues() { check(prism_scalar_set_face_values(_h.get(), nullptr)); }
+    // Scalar::setGradScheme (scalar.cpp:252-258) by kind (PRISM_GRAD_*)
+    void setGradScheme(int grad_scheme) { check(prism_scalar_set_grad_scheme(_h.get(), grad_scheme)); }
     auto handle() const -> PrismScalar* { return _h.get(); }
     auto mesh() const -> const std::shared_ptr<mesh::PMesh>& { return _mesh; }
 
@@ -258,6 +260,11 @@ inline auto div(const field::Vector& U) -> field::Scalar {
     PrismScalar* h = nullptr;
     check(prism_ops_div(U.handle(), &h));
     return field::Scalar::adopt(h, U.mesh(), "div(" + U.name() + ")");
+}
+// mdot.mapFaceValues(U.valueAtFace); mdot.mapInteriorFaceValues(rhieChowCorrectFace)
+// (SIMPLE.cpp:136-138, operations/rhie_chow.h:47-63)
+inline void rhieChowFaces(field::Vector& mdot, const field::Vector& U, const field::Tensor& D, field::Scalar& p) {
+    check(prism_rhie_chow(mdot.handle(), U.handle(), D.handle(), p.handle()));
 }
 }  // namespace ops
 

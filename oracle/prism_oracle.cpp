@@ -1462,11 +1462,10 @@ struct PressureResult {
 };
 
 // solvePressureEquation, SIMPLE.cpp:124-196
-PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transport*>& mom, Vector& U, Vector& mdot,
-                                     Scalar& p, std::vector<Report>& rep) {
+// mdot.mapFaceValues(U.valueAtFace); mdot.mapInteriorFaceValues(rhieChowCorrectFace)
+// (SIMPLE.cpp:136-138)
+void rhieChowFaces(Vector& mdot, Vector& U, const Tensor& D, Scalar& p) {
     Mesh* m = p.m;
-    auto D = pressureCoeffs(mom, m);
-    // mdot.mapFaceValues(U.valueAtFace)
     initFaceData(mdot);
     for (int64_t f = m->n_boundary; f < m->nf(); ++f) {
         V3 u = valueAtFace(U, f);
@@ -1481,12 +1480,18 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
             mdot.ff[fid] = dot(u, m->faces[fid].areaVector());
         }
     }
-    // mdot.mapInteriorFaceValues(rhieChowCorrectFace)
     for (int64_t f = m->n_boundary; f < m->nf(); ++f) {
-        V3 u = rhieChow(f, U, *D, p);
+        V3 u = rhieChow(f, U, D, p);
         mdot.fd[f] = u;
         mdot.ff[f] = dot(u, m->faces[f].areaVector());
     }
+}
+
+PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transport*>& mom, Vector& U, Vector& mdot,
+                                     Scalar& p, std::vector<Report>& rep) {
+    Mesh* m = p.m;
+    auto D = pressureCoeffs(mom, m);
+    rhieChowFaces(mdot, U, *D, p);
     // p' field named like p, zero valued, fresh gradient scheme (scalar.cpp:260-304)
     auto pp = std::make_unique<Scalar>();
     pp->m = m;
@@ -1864,6 +1869,14 @@ ORC_API int orc_scalar_compute_gradients(PrismScalar* ps) {
         computeAllCellGradients(*ps->s);
     })
 }
+// Scalar::setGradScheme (scalar.cpp:252-258): a fresh scheme object of the kind
+ORC_API int orc_scalar_set_grad_scheme(PrismScalar* ps, int32_t grad_scheme) {
+    GUARD({
+        CHECK_ARG(ps, "null argument");
+        CHECK_ARG(grad_scheme == PRISM_GRAD_LEAST_SQUARES || grad_scheme == PRISM_GRAD_GREEN_GAUSS, "bad gradient scheme");
+        ps->s->grad = makeGrad(ps->s->m, grad_scheme);
+    })
+}
 
 ORC_API int orc_vector_create(PrismMesh* pm, const char* name, const double* values, int32_t grad_scheme,
                               const PrismBC* bcs, PrismVector** out) {
@@ -2083,6 +2096,13 @@ ORC_API int orc_tensor_create(PrismMesh* pm, const char* name, const double* val
     })
 }
 ORC_API int orc_tensor_destroy(PrismTensor* t) { GUARD({ delete t; }) }
+
+ORC_API int orc_rhie_chow(PrismVector* pmdot, PrismVector* pU, PrismTensor* pD, PrismScalar* pp) {
+    GUARD({
+        CHECK_ARG(pmdot && pU && pD && pp, "null argument");
+        rhieChowFaces(*pmdot->v, *pU->v, *pD->t, *pp->s);
+    })
+}
 
 ORC_API int orc_transport_create(PrismScalar* phi, PrismTransport** out) {
     GUARD({

@@ -140,6 +140,7 @@ SIGNATURES = {
     "scalar_face_values": (C.c_int, [P, pf64]),
     "scalar_grad": (C.c_int, [P, pf64]),
     "scalar_compute_gradients": (C.c_int, [P]),
+    "scalar_set_grad_scheme": (C.c_int, [P, i32]),
     "vector_create": (C.c_int, [P, C.c_char_p, pf64, i32, C.POINTER(BC), PP]),
     "vector_clone": (C.c_int, [P, PP]),
     "vector_destroy": (C.c_int, [P]),
@@ -155,6 +156,7 @@ SIGNATURES = {
     "vector_to_points": (C.c_int, [P, pf64]),
     "tensor_create": (C.c_int, [P, C.c_char_p, pf64, PP]),
     "tensor_destroy": (C.c_int, [P]),
+    "rhie_chow": (C.c_int, [P, P, P, P]),
     "transport_create": (C.c_int, [P, PP]),
     "transport_destroy": (C.c_int, [P]),
     "transport_add_convection": (C.c_int, [P, i32, P]),

@@ -191,6 +191,11 @@ class Scalar:
     def compute_all_cell_gradients(self):
         self.lib.check(self.lib.scalar_compute_gradients(self.h))
 
+    def set_grad_scheme(self, grad_scheme):
+        """Scalar::setGradScheme (scalar.cpp:252-258): A.GRAD_LEAST_SQUARES or
+        A.GRAD_GREEN_GAUSS; the new scheme starts from zero gradients."""
+        self.lib.check(self.lib.scalar_set_grad_scheme(self.h, int(grad_scheme)))
+
     # time-step history (field/history.cpp)
     def set_history_size(self, n):
         self.lib.check(self.lib.scalar_set_history_size(self.h, int(n)))
@@ -385,6 +390,14 @@ class ops:  # noqa: N801  (namespace prism::ops)
                     t[3 * i + j] = g[j][i]
             return Tensor(f"grad({field.name})", mesh, t)
         raise TypeError("ops.grad needs a Scalar or a Vector")
+
+    @staticmethod
+    def rhie_chow(mdot, U, D, p):
+        """mdot's face values from U with ops::rhieChowCorrectFace on the interior faces
+        (SIMPLE.cpp:136-138, rhie_chow.h:47-63): U.valueAtFace on boundary faces,
+        U_f - D_f (grad p_calculated - grad p_averaged) inside; read them back with
+        mdot.face_flux()."""
+        mdot.lib.check(mdot.lib.rhie_chow(mdot.h, U.h, D.h, p.h))
 
     @staticmethod
     def symm(a):

@@ -304,6 +304,28 @@ API int prism_scalar_compute_gradients(PrismScalar* ps) {
         sync(*ps->s->m);
     });
 }
+API int prism_scalar_set_grad_scheme(PrismScalar* ps, int32_t grad) {
+    return guard([&] {
+        ARG(ps, "null argument");
+        ARG(grad == PRISM_GRAD_LEAST_SQUARES || grad == PRISM_GRAD_GREEN_GAUSS, "bad gradient scheme");
+        Scalar& s = *ps->s;
+        auto g = std::make_shared<GradState>();
+        g->type = grad;
+        g->g.alloc(3 * (size_t)s.m->n_pad);
+        g->g.zero(s.m->stream);
+        s.grad = std::move(g);
+        sync(*s.m);
+    });
+}
+API int prism_rhie_chow(PrismVector* pmdot, PrismVector* pU, PrismTensor* pD, PrismScalar* pp) {
+    return guard([&] {
+        ARG(pmdot && pU && pD && pp, "null argument");
+        Mesh& m = *pp->s->m;
+        ARG(pmdot->v->m == &m && pU->v->m == &m && pD->t->m == &m, "fields on different meshes");
+        rhieChowFaces(*pmdot->v, *pU->v, *pD->t, *pp->s);
+        sync(m);
+    });
+}
 API int prism_scalar_set_history_size(PrismScalar* ps, int32_t n) {
     return guard([&] {
         ARG(ps && n >= 0, "bad argument");

@@ -689,6 +689,19 @@ void pisoDefaults(PrismPISOControls* c) {  // PISOControls, PISO.h:11-49
     c->batched_momentum = 0;
 }
 
+// mdot.mapFaceValues(U.valueAtFace); mdot.mapInteriorFaceValues(rhieChowCorrectFace)
+// (SIMPLE.cpp:136-138, operations/rhie_chow.h:47-63)
+void rhieChowFaces(Vector& mdot, Vector& U, const Tensor& D, Scalar& p) {
+    Mesh& m = *p.m;
+    checkVectorFlux(mdot, "GeneralVector::initFaceData()");
+    checkVectorValues(U, "GeneralVector::valueAtFace()");
+    if (m.nf > m.nb) ensureGradient(p);
+    if (!mdot.fd) mdot.fd.alloc(3 * (size_t)std::max(m.nf, 1));
+    if (!mdot.ff) mdot.ff.alloc(std::max(m.nf, 1));
+    launchRhieChow(m.view(), U.view(), D.view(), p.view(), mdot.fd.p, mdot.ff.p, m.stream);
+    mdot.has_fd = mdot.has_ff = true;
+}
+
 namespace {
 
 PrismSolveOpts inner(const PrismSolveOpts& so, int64_t n_iter, double eps, int64_t ref, double refv, bool clear) {
@@ -777,14 +790,7 @@ PressureResult solvePressureEquation(PrismSIMPLEControls c, std::vector<Transpor
     launchDTensor(m.nc, m.pat.diag_pos.p, m.vol.p, mom[0]->A.p, mom[1]->A.p, mom.size() == 3 ? mom[2]->A.p : nullptr,
                   D->d.p, m.n_pad, m.stream);
     for (auto* eq : mom) zeroOutCoeffs(*eq);
-    // mdot.mapFaceValues(U.valueAtFace); mdot.mapInteriorFaceValues(rhieChowCorrectFace)
-    checkVectorFlux(mdot, "GeneralVector::initFaceData()");
-    checkVectorValues(U, "GeneralVector::valueAtFace()");
-    if (m.nf > m.nb) ensureGradient(p);
-    if (!mdot.fd) mdot.fd.alloc(3 * (size_t)std::max(m.nf, 1));
-    if (!mdot.ff) mdot.ff.alloc(std::max(m.nf, 1));
-    launchRhieChow(m.view(), U.view(), D->view(), p.view(), mdot.fd.p, mdot.ff.p, m.stream);
-    mdot.has_fd = mdot.has_ff = true;
+    rhieChowFaces(mdot, U, *D, p);
     // p' named like p, zero valued, with a fresh gradient scheme (scalar.cpp:260-304)
     if (!m.p_corr) {
         m.p_corr = std::make_unique<Scalar>();

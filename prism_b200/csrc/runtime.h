@@ -154,6 +154,9 @@ struct Transport {
 
 // operations (mirroring the reference call structure)
 void ensureGradient(Scalar& s);
+// mdot's face values: U.valueAtFace on boundary faces, ops::rhieChowCorrectFace on
+// interior faces, with the face fluxes
+void rhieChowFaces(Vector& mdot, Vector& U, const Tensor& D, Scalar& p);
 void computeGradient(Scalar& s);
 void updateCoeffs(Transport& eq);
 void relax(Transport& eq);
