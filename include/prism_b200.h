@@ -114,6 +114,12 @@ extern "C" {
 
 #define PRISM_SOLVER_BICGSTAB 0
 #define PRISM_SOLVER_JACOBI 1
+/* flexible conjugate gradients (one previous direction kept) preconditioned by an
+ * FP32 AMG V-cycle, FP64 recurrences: for symmetric positive (semi-)definite
+ * systems; FP64 precision and the AMG (or automatic) preconditioner only. No
+ * counterpart in the reference; SIMPLE/PRIME/PISO use it for the pressure
+ * correction on their own. */
+#define PRISM_SOLVER_FCG 2
 
 #define PRISM_PREC_FP64 0  /* FP64 Krylov */
 #define PRISM_PREC_MIXED 1 /* FP32 BiCGSTAB (FP64 dots) with FP64 reliable updates */

@@ -27,7 +27,7 @@ CONV = {"Upwind": 0, "CentralDifference": 1, "LinearUpwind": 2, "QUICK": 3, "FRO
 CORR_OVER_RELAXED, CORR_MINIMUM, CORR_ORTHOGONAL = 0, 1, 2
 SRC_CONSTANT, SRC_DIVERGENCE, SRC_GRADIENT = 0, 1, 2
 SIGN_POSITIVE, SIGN_NEGATIVE = 0, 1
-SOLVER_BICGSTAB, SOLVER_JACOBI = 0, 1
+SOLVER_BICGSTAB, SOLVER_JACOBI, SOLVER_FCG = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 TEMPORAL_BACKWARD_EULER, TEMPORAL_ADAM_MOULTON = 0, 1
 PC_AUTO, PC_JACOBI, PC_AMG = 0, 1, 2

@@ -642,6 +642,12 @@ class Jacobi(_Solver):
     method = A.SOLVER_JACOBI
 
 
+class FCG(_Solver):
+    """Flexible CG with an FP32 AMG V-cycle (FP64 recurrences), for symmetric positive
+    (semi-)definite systems; no counterpart in the reference."""
+    method = A.SOLVER_FCG
+
+
 # ---- pressure-velocity coupling ------------------------------------------------------
 @dataclass
 class SIMPLEControls:

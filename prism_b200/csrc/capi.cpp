@@ -823,7 +823,10 @@ API int prism_solve_csr(int64_t n, const int64_t* rowptr, const int64_t* col, co
         } else {
             Amg amg;
             DevBuf<int> d_rp, d_col;
-            const bool use_amg = choosePreconditioner(o->preconditioner, n) == PRISM_PC_AMG;
+            const bool fcg = o->method == PRISM_SOLVER_FCG;
+            if (fcg && (o->precision != PRISM_PREC_FP64 || o->preconditioner == PRISM_PC_JACOBI))
+                fail(PRISM_BAD_ARG, "flexible CG runs in FP64 with the AMG preconditioner");
+            const bool use_amg = fcg || choosePreconditioner(o->preconditioner, n) == PRISM_PC_AMG;
             if (use_amg) {
                 std::vector<int> rp32(rowptr, rowptr + n + 1), col32(col, col + rowptr[n]);
                 d_rp.upload(rp32, s);
@@ -831,7 +834,8 @@ API int prism_solve_csr(int64_t n, const int64_t* rowptr, const int64_t* col, co
             }
             k = bicgstab(A, d_b.p, d_x.p, o->krylov_tol > 0 ? o->krylov_tol : 1e-12,
                          o->krylov_max_iter > 0 ? o->krylov_max_iter : 2 * n, o->precision,
-                         o->inner_tol > 0 ? o->inner_tol : 0.1, kw, s, use_amg ? &amg : nullptr, d_rp.p, d_col.p);
+                         o->inner_tol > 0 ? o->inner_tol : 0.1, kw, s, use_amg ? &amg : nullptr, d_rp.p, d_col.p,
+                         fcg);
         }
         double res = scaledResidual(A, d_b.p, d_x.p, kw, s);
         d_x.download(x, n, s);

@@ -584,7 +584,16 @@ static bool flexibleFor(const Transport& eq, const PrismSolveOpts& o, const Amg*
         const char* e = std::getenv("PRISM_PRESSURE_SOLVER");
         return !(e && std::strcmp(e, "bicgstab") == 0);
     }();
+    if (o.method == PRISM_SOLVER_FCG) return true;
     return on && eq.spd && amg && o.method == PRISM_SOLVER_BICGSTAB && o.precision == PRISM_PREC_FP64;
+}
+
+// PRISM_SOLVER_FCG's requirements: FP64, and the AMG preconditioner (its own choice
+// under PRISM_PC_AUTO)
+static void checkFcg(const PrismSolveOpts& o) {
+    if (o.method != PRISM_SOLVER_FCG) return;
+    if (o.precision != PRISM_PREC_FP64) fail(PRISM_BAD_ARG, "flexible CG runs in FP64 (precision PRISM_PREC_FP64)");
+    if (o.preconditioner == PRISM_PC_JACOBI) fail(PRISM_BAD_ARG, "flexible CG needs the AMG preconditioner");
 }
 
 namespace {
@@ -600,6 +609,7 @@ PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o);
 
 // ISolver::solve (numerics/solver.cpp:27-82)
 PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
+    checkFcg(o);
     if (g_capture) return solveCaptured(eq, o);
     Scalar& phi = *eq.phi;
     Mesh& m = *phi.m;
@@ -616,7 +626,7 @@ PrismSolveResult solve(Transport& eq, const PrismSolveOpts& o) {
     const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
     const double itol = o.inner_tol > 0 ? o.inner_tol : 0.1;
     Amg* amg = nullptr;
-    if (o.method != PRISM_SOLVER_JACOBI && pcFor(eq, o, A) == PRISM_PC_AMG) {
+    if (o.method == PRISM_SOLVER_FCG || (o.method != PRISM_SOLVER_JACOBI && pcFor(eq, o, A) == PRISM_PC_AMG)) {
         if (!eq.amg) eq.amg = std::make_shared<Amg>();
         amg = eq.amg.get();
     }
@@ -1213,8 +1223,8 @@ PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o) {
     Scalar& phi = *eq.phi;
     Mesh& m = *phi.m;
     if (g_capture->m != &m) fail(PRISM_BAD_ARG, "a graph step spans more than one mesh");
-    if (o.method != PRISM_SOLVER_BICGSTAB || o.precision != PRISM_PREC_FP64)
-        fail(PRISM_BAD_ARG, "graph mode runs FP64 BiCGSTAB only");
+    if ((o.method != PRISM_SOLVER_BICGSTAB && o.method != PRISM_SOLVER_FCG) || o.precision != PRISM_PREC_FP64)
+        fail(PRISM_BAD_ARG, "graph mode runs FP64 BiCGSTAB or flexible CG only");
     if (g_capture->used >= GRAPH_SLOTS) fail(PRISM_BAD_ARG, "too many solves in one graph step");
     const int slot = g_capture->used++;
     SolveCtl* ctl = m.graph_ctl.p + slot;
@@ -1227,7 +1237,7 @@ PrismSolveResult solveCaptured(Transport& eq, const PrismSolveOpts& o) {
     const double ktol = o.krylov_tol > 0 ? o.krylov_tol : 1e-12;
     const long long kmax = o.krylov_max_iter > 0 ? o.krylov_max_iter : 2LL * m.nc;
     Amg* amg = nullptr;
-    if (pcFor(eq, o, A) == PRISM_PC_AMG) {
+    if (o.method == PRISM_SOLVER_FCG || pcFor(eq, o, A) == PRISM_PC_AMG) {
         if (!eq.amg) eq.amg = std::make_shared<Amg>();
         amg = eq.amg.get();
     }
@@ -1323,10 +1333,12 @@ int runAsGraph(Mesh& m, const std::function<void()>& f) {
 
 bool graphReady(const Transport& eq, const PrismSolveOpts& o) {
     const Mesh& m = *eq.phi->m;
-    if (o.method != PRISM_SOLVER_BICGSTAB || o.precision != PRISM_PREC_FP64) return false;
+    if ((o.method != PRISM_SOLVER_BICGSTAB && o.method != PRISM_SOLVER_FCG) || o.precision != PRISM_PREC_FP64)
+        return false;
     if (!eq.A || !eq.b || m.kw.n != m.n_pad) return false;
-    int pc = choosePreconditioner(o.preconditioner, m.nc);
-    if (o.preconditioner == PRISM_PC_AUTO && pc == PRISM_PC_AMG && !eq.spd && autoJacobiRatio() > 0.0) {
+    int pc = o.method == PRISM_SOLVER_FCG ? PRISM_PC_AMG : choosePreconditioner(o.preconditioner, m.nc);
+    if (o.method != PRISM_SOLVER_FCG && o.preconditioner == PRISM_PC_AUTO && pc == PRISM_PC_AMG && !eq.spd &&
+        autoJacobiRatio() > 0.0) {
         if (eq.auto_pc == 0) return false;  // chosen on an ordinary solve first
         pc = eq.auto_pc;
     }

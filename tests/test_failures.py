@@ -163,3 +163,28 @@ def test_gpu_batch_statuses(gpu):
         p[1].set_values(np.zeros(p[0].n_cells))
     res = capped.solve([probs[0][3], probs[2][3]])
     assert all(r.status == A.NOT_CONVERGED for r in res)
+
+
+# ---------------------------------------------------------------- flexible CG (PRISM_SOLVER_FCG)
+@pytest.mark.gpu
+@pytest.mark.parametrize("graph", [False, True])
+def test_gpu_fcg_statuses(gpu, graph):
+    """Flexible CG reports the same statuses as BiCGSTAB: NONFINITE for NaN in b,
+    NOT_CONVERGED at the Krylov cap, and BAD_ARG for what it cannot run."""
+    mesh, P, S, eqn = poisson(gpu, n=32)
+    solver = api.FCG(graph=graph)
+    good = solver.solve(eqn, 2, 1e-10)  # builds what graph mode replays
+    assert good.status == A.OK and good.converged
+    P.set_values(np.zeros(mesh.n_cells))
+    r = api.FCG(krylov_max_iter=1, graph=graph).solve(eqn, 1, 1e-10)
+    assert r.status == A.NOT_CONVERGED and not r.converged and r.krylov_iterations <= 1
+    s = S.values()
+    s[37] = np.nan
+    S.set_values(s)
+    P.set_values(np.zeros(mesh.n_cells))
+    r = solver.solve(eqn, 2, 1e-10)
+    assert r.status == A.NONFINITE and not r.converged
+    for bad in (api.FCG(precision=A.PREC_MIXED), api.FCG(preconditioner="jacobi")):
+        with pytest.raises(PrismError) as e:
+            bad.solve(eqn, 1, 1e-10)
+        assert e.value.status == A.BAD_ARG

@@ -55,6 +55,27 @@ def test_solve_graph_matches_ordinary(gpu, preconditioner, n_iter, eps):
           f"outer {[r.iteration for r in out[True][1]]}")
 
 
+@pytest.mark.parametrize("n_iter, eps", [(1, 0.0), (3, 1e-30)])
+def test_fcg_solve_graph_matches_ordinary(gpu, n_iter, eps):
+    """Flexible CG (PRISM_SOLVER_FCG) in graph mode, bit for bit against the ordinary path."""
+    out = {}
+    for graph in (False, True):
+        mesh, P, eqn, exact = cases.poisson_c1(64, gpu)
+        solver = api.FCG(krylov_tol=1e-11, graph=graph)
+        res = []
+
+        def from_zero():  # every solve starts from P = 0, so each one iterates
+            P.set_values(np.zeros(mesh.n_cells))
+            return solver.solve(eqn, n_iter, eps)
+        launches = _graph_launches(gpu, lambda: res.extend(from_zero() for _ in range(3)))
+        assert launches == (2 if graph else 0)
+        out[graph] = (P.values(), res)
+    np.testing.assert_array_equal(out[True][0], out[False][0])
+    for a, b in zip(out[True][1], out[False][1]):
+        _same_results(a, b)
+    print(f"flexible CG n_iter={n_iter}: krylov its {[r.krylov_iterations for r in out[True][1]]}")
+
+
 def test_mixed_precision_runs_ordinarily(gpu):
     out = {}
     for graph in (False, True):

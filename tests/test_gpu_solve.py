@@ -50,6 +50,21 @@ def test_poisson_c1_solve(gpu, orc, precision):
     assert res["gpu"][1].converged
 
 
+@pytest.mark.parametrize("n", [32, 128])
+def test_poisson_c1_flexible_cg(gpu, orc, n):
+    """PRISM_SOLVER_FCG (flexible CG, FP32 AMG V-cycle) on the symmetric C1 Poisson system,
+    at its stated 128^2 too, against the oracle's ILUT-BiCGSTAB."""
+    res = {}
+    for name, lib, solver in (("gpu", gpu, api.FCG(krylov_tol=1e-12)), ("orc", orc, api.BiCGSTAB())):
+        mesh, P, eqn, exact = cases.poisson_c1(n, lib)
+        r = solver.solve(eqn, 3, 1e-10)
+        res[name] = (P.values(), r)
+    err = cases.rel_l2(res["gpu"][0], res["orc"][0])
+    print(f"C1 {n}x{n} flexible CG: rel L2 vs oracle {err:.3e}, krylov it {res['gpu'][1].krylov_iterations}")
+    assert err < SOL_TOL
+    assert res["gpu"][1].converged and res["gpu"][1].status == A.OK
+
+
 @pytest.mark.parametrize("name", ["poisson_hex", "poisson_wedge", "versteeg_advection_1d"])
 def test_reference_cases(gpu, name):
     ref = cases.load_oracle_results(name)
