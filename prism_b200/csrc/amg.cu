@@ -715,6 +715,9 @@ struct TailLevel {
     const int* agg;    // row -> aggregate of the next level
     const int* m_off;  // aggregate -> member rows (restriction to the next level)
     const int* m_idx;
+    const int* rt_sl_off;  // smoothed restriction to the next level (TailParams::rt)
+    const int* rt_col;
+    const T* rt_val;
     T *b, *x, *x2, *res;
 };
 template <typename T>
@@ -724,6 +727,7 @@ struct TailParams {
     const T* inv;  // dense inverse of the coarsest level, or null for Jacobi sweeps
     T omega, scale;
     const KState* S;
+    int rt;  // every level but the coarsest has its smoothed restriction: one down phase per level
     TailLevel<T> L[TAIL_MAX_LEVELS];
 };
 
@@ -751,10 +755,21 @@ __global__ void __launch_bounds__(TAIL_BS) tail_kernel(const __grid_constant__ T
     const int g = (int)cl.block_rank() * TAIL_BS + threadIdx.x;
     const int lane = threadIdx.x & 31, gw = g >> 5, nw = nthreads >> 5;
     const T omega = P.omega, scale = P.scale;
-    // down: pre-smoothing from zero with the residual, then restriction
+    // down: the next level's right-hand side by the smoothed restriction (one phase), or
+    // pre-smoothing from zero with the residual, then restriction (two phases)
     for (int l = 0; l + 1 < P.nlev; ++l) {
         const TailLevel<T>& L = P.L[l];
         const T* b = l == 0 ? P.b0 : L.b;
+        const TailLevel<T>& N = P.L[l + 1];
+        if (P.rt) {
+            tailRows(N.n, g, nthreads, [&](int c, bool valid, int sub) {
+                const T sum = rowSum<T, TAIL_LPR>(L.rt_sl_off, L.rt_col, L.rt_val, c, valid, sub,
+                                                  [&](int j) { return __ldcg(b + j); });
+                if (valid && sub == 0) N.b[c] = sum;
+            });
+            cl.sync();
+            continue;
+        }
         tailRows(L.n, g, nthreads, [&](int row, bool valid, int sub) {
             const T sum = rowSum<T, TAIL_LPR>(L.sl_off, L.col, L.val, row, valid, sub,
                                               [&](int c) { return omega * L.dinv[c] * __ldcg(b + c); });
@@ -765,7 +780,6 @@ __global__ void __launch_bounds__(TAIL_BS) tail_kernel(const __grid_constant__ T
             }
         });
         cl.sync();
-        const TailLevel<T>& N = P.L[l + 1];
         tailRows(N.n, g, nthreads, [&](int c, bool valid, int sub) {
             T sum = 0;
             if (valid)
@@ -810,13 +824,14 @@ __global__ void __launch_bounds__(TAIL_BS) tail_kernel(const __grid_constant__ T
         const TailLevel<T>& L = P.L[l];
         const T* xc = P.L[l + 1].x2;
         const T* b = l == 0 ? P.b0 : L.b;
+        // the pre-smoothed x = omega D^-1 b: stored by the pre-smoothing phase, or formed here
+        auto xp = [&](int c) {
+            const T xs = P.rt ? omega * L.dinv[c] * __ldcg(b + c) : __ldcg(L.x + c);
+            return xs + scale * __ldcg(xc + L.agg[c]);
+        };
         tailRows(L.n, g, nthreads, [&](int row, bool valid, int sub) {
-            const T sum = rowSum<T, TAIL_LPR>(L.sl_off, L.col, L.val, row, valid, sub,
-                                              [&](int c) { return __ldcg(L.x + c) + scale * __ldcg(xc + L.agg[c]); });
-            if (valid && sub == 0) {
-                const T xp = __ldcg(L.x + row) + scale * __ldcg(xc + L.agg[row]);
-                L.x2[row] = xp + omega * L.dinv[row] * (__ldcg(b + row) - sum);
-            }
+            const T sum = rowSum<T, TAIL_LPR>(L.sl_off, L.col, L.val, row, valid, sub, xp);
+            if (valid && sub == 0) L.x2[row] = xp(row) + omega * L.dinv[row] * (__ldcg(b + row) - sum);
         });
         if (l > 0) cl.sync();
     }
@@ -1213,8 +1228,8 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
                 tail = (int)l;
                 break;
             }
-        // the down-sweep of each level that runs its own kernels (above the fused tail)
-        for (size_t l = 0; l + 1 < levels.size() && (tail < 0 || (int)l < tail); ++l) {
+        // the down-sweep of each level but the coarsest (the fused tail's levels too)
+        for (size_t l = 0; l + 1 < levels.size(); ++l) {
             AmgLevel& L = *levels[l];
             L.use_rt = useRestriction(l, L.n, L.nnz);
             if (L.use_rt)
@@ -1378,11 +1393,17 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
             t.agg = X.agg.p;
             t.m_off = X.m_off.p;
             t.m_idx = X.m_idx.p;
+            t.rt_sl_off = X.rt_sl_off.p;
+            t.rt_col = X.rt_sl_col.p;
+            t.rt_val = CycleData<T>::rt(X);
             t.b = xb.b;
             t.x = xb.x;
             t.x2 = k == 0 ? out : xb.x2;
             t.res = xb.res;
         }
+        P.rt = 1;
+        for (int k = 0; k + 1 < P.nlev; ++k)
+            if (!A.levels[l + k]->use_rt || !P.L[k].rt_val) P.rt = 0;
         launchTail<T>(P, s);
         return;
     }
