@@ -695,13 +695,14 @@ __global__ void coarse_solve_kernel(int n, const T* __restrict__ inv, const T* _
 // coarsest level too large for a dense inverse: a few damped Jacobi sweeps
 // ---------------------------------------------------------------- fused coarse tail
 // The levels from the first one with at most tailMaxRows() rows down to the
-// coarsest run in one launch of a thread-block cluster: the pre-smoothing and
-// residual, restriction, coarsest solve and prolongation/post-smoothing phases
-// of all those levels are separated by cluster barriers instead of kernel
-// boundaries, which on levels this small cost more than the work itself. One
-// warp walks a 32-row slice at a time (one row per lane, slots in order, so the
-// sums round as in the single-lane kernels above). Vectors written inside the
-// launch are read through L2 (ld.global.cg); matrices with ordinary loads.
+// coarsest run in one launch of a thread-block cluster: the down phases (the
+// smoothed restriction, or pre-smoothing with the residual and then the
+// restriction), the coarsest solve and the prolongation/post-smoothing phases of
+// all those levels are separated by cluster barriers instead of kernel
+// boundaries, which on levels this small cost more than the work itself. Rows
+// take TAIL_LPR lanes each (slots in order per lane, as in the separate kernels).
+// Vectors written inside the launch are read through L2 (ld.global.cg); matrices
+// with ordinary loads.
 constexpr int TAIL_MAX_LEVELS = 16;
 constexpr int TAIL_BS = 1024;
 
