@@ -112,3 +112,26 @@ def test_step_graph_matches_ordinary(gpu, algo, preconditioner):
         assert np.array_equal([(e.initial_residual, e.final_residual) for e in rg],
                               [(e.initial_residual, e.final_residual) for e in ro])
     print(f"{algo} ({preconditioner}): last step reports {[(e.field_name, e.n_iterations) for e in out[True][3][-1]]}")
+
+
+@pytest.mark.parametrize("kcycle", [None, "1"])
+def test_simple_graph_at_amg_sizes(gpu, kcycle, monkeypatch):
+    """SIMPLE steps of a 192 x 192 cavity (36,864 cells: the automatic preconditioner
+    measures the momentum matrices and keeps Jacobi, the pressure correction runs
+    flexible CG with the FP32 V-cycle, or with a K-cycle level) as one graph launch
+    each, bit for bit against the ordinary path."""
+    if kcycle:
+        monkeypatch.setenv("PRISM_AMG_KCYCLE", kcycle)
+    out = {}
+    for graph in (False, True):
+        mesh, U, p, nu, mdot, eqs = cases.cavity(192, gpu)
+        driver = api.IncompressibleSIMPLE(api.SIMPLEControls(), solver=api.BiCGSTAB(graph=graph))
+        reports = []
+        launches = _graph_launches(gpu, lambda: reports.extend(driver.step(eqs, U, mdot, p) for _ in range(4)))
+        assert launches == (3 if graph else 0)
+        out[graph] = (U.values(), p.values(), mdot.face_flux(), reports)
+    for i, k in enumerate(("U", "p", "mdot")):
+        np.testing.assert_array_equal(out[True][i], out[False][i], err_msg=k)
+    for rg, ro in zip(out[True][3], out[False][3]):
+        assert np.array_equal([(e.initial_residual, e.final_residual) for e in rg],
+                              [(e.initial_residual, e.final_residual) for e in ro])

@@ -50,6 +50,27 @@ def test_poisson_c1_solve(gpu, orc, precision):
     assert res["gpu"][1].converged
 
 
+def test_auto_preconditioner_picks_by_diagonal_dominance(gpu):
+    """PRISM_PC_AUTO at AMG sizes (36,864 rows): an equation relaxed by 0.7 is diagonally
+    dominant (off-diagonal row sums 0.7 of the diagonal) and keeps Jacobi, bit for bit
+    the solve that asks for Jacobi; the same equation unrelaxed gets AMG, bit for bit the
+    solve that asks for AMG."""
+    def solve(pc, urf):
+        mesh, U, p, nu, mdot, eqs = cases.cavity(192, gpu)
+        U.set_values(np.random.default_rng(5).normal(size=(3, mesh.n_cells)) * 0.1)
+        eq = eqs[0]
+        eq.set_under_relax_factor(urf)
+        r = api.BiCGSTAB(preconditioner=pc, krylov_tol=1e-12).solve(eq, 1, 0.0)
+        return U.values()[0], r.krylov_iterations
+    for urf, expect in ((0.7, "jacobi"), (1.0, "amg")):
+        auto, its = solve("auto", urf)
+        forced, its_f = solve(expect, urf)
+        other, _ = solve("amg" if expect == "jacobi" else "jacobi", urf)
+        print(f"urf {urf}: auto took {expect} ({its} Krylov iterations, forced {its_f})")
+        np.testing.assert_array_equal(auto, forced)
+        assert not np.array_equal(auto, other)
+
+
 @pytest.mark.parametrize("n", [32, 128])
 def test_poisson_c1_flexible_cg(gpu, orc, n):
     """PRISM_SOLVER_FCG (flexible CG, FP32 AMG V-cycle) on the symmetric C1 Poisson system,
