@@ -282,6 +282,48 @@ __global__ void rt_values_kernel(int nnz, const int* __restrict__ erow, const in
     if (out32) out32[csr_pos[e]] = (float)v;
 }
 
+// SELL-C-sigma order of the smoothed restriction's rows: within each window of RT_SIGMA
+// rows, longest first (a stable sort keeps equal lengths in row order), so that the
+// rows sharing a 32-row slice have similar lengths and the slices little padding
+constexpr int RT_SIGMA = 256;
+__global__ void rt_order_keys_kernel(int n, const int* rowptr, unsigned* keys, int* rows) {
+    const int c = blockIdx.x * BS + threadIdx.x;
+    if (c >= n) return;
+    const int len = min(rowptr[c + 1] - rowptr[c], 255);
+    keys[c] = ((unsigned)(c / RT_SIGMA) << 8) | (unsigned)(255 - len);
+    rows[c] = c;
+}
+// slots of each slice in the permuted order: 32 x the longest of its rows
+__global__ void rt_slice_len_kernel(int n, int nslices, const int* rowptr, const int* perm, int* slice_entries) {
+    const int sl = blockIdx.x * BS + threadIdx.x;
+    if (sl >= nslices) return;
+    int w = 0;
+    for (int l = 0; l < 32; ++l) {
+        const int r = sl * 32 + l;
+        if (r < n) w = max(w, rowptr[perm[r] + 1] - rowptr[perm[r]]);
+    }
+    slice_entries[sl] = 32 * w;
+}
+// slot row r holds row perm[r]; padded slots read column 0 (value 0)
+__global__ void rt_fill_kernel(int n, int nslices, const int* rowptr, const int* col, const int* perm,
+                               const int* sl_off, int* sl_col, int* csr_pos) {
+    const int r = blockIdx.x * BS + threadIdx.x;
+    if (r >= nslices * 32) return;
+    const int s = r >> 5, lane = r & 31;
+    const int base = sl_off[s], width = (sl_off[s + 1] - base) >> 5;
+    const int c = r < n ? perm[r] : -1;
+    const int len = c >= 0 ? rowptr[c + 1] - rowptr[c] : 0;
+    for (int j = 0; j < width; ++j) {
+        const int pos = base + 32 * j + lane;
+        if (j < len) {
+            sl_col[pos] = col[rowptr[c] + j];
+            csr_pos[rowptr[c] + j] = pos;
+        } else {
+            sl_col[pos] = 0;
+        }
+    }
+}
+
 __global__ void entry_rows_kernel(int n, const int* rowptr, int* erow) {
     const int r = blockIdx.x * BS + threadIdx.x;
     if (r >= n) return;
@@ -464,15 +506,15 @@ __global__ void restrict_kernel(int nc, const int* m_off, const int* m_idx, cons
 // restriction: pre-smoothing from zero, residual and restriction in one pass)
 template <typename T, int LPR>
 __global__ void __launch_bounds__(BS) down_kernel(int nc, const int* __restrict__ sl_off, const int* __restrict__ col,
-                                                  const T* __restrict__ val, const T* __restrict__ b,
-                                                  T* __restrict__ bc, const KState* S) {
+                                                  const T* __restrict__ val, const int* __restrict__ perm,
+                                                  const T* __restrict__ b, T* __restrict__ bc, const KState* S) {
     pdlEnter();
     if (S && S->done) return;
     const int gt = blockIdx.x * BS + threadIdx.x;
-    const int row = gt / LPR, sub = gt % LPR;
+    const int row = gt / LPR, sub = gt % LPR;  // slot row; it holds row perm[row] of Rt
     const bool valid = row < nc;
     const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, [&](int j) { return b[j]; });
-    if (valid && sub == 0) bc[row] = sum;
+    if (valid && sub == 0) bc[perm[row]] = sum;
 }
 
 // prolongation and post-smoothing: out = xp + omega D^-1 (b - A xp), xp = x + scale * xc[agg]
@@ -716,9 +758,10 @@ struct TailLevel {
     const int* agg;    // row -> aggregate of the next level
     const int* m_off;  // aggregate -> member rows (restriction to the next level)
     const int* m_idx;
-    const int* rt_sl_off;  // smoothed restriction to the next level (TailParams::rt)
-    const int* rt_col;
+    const int* rt_sl_off;  // smoothed restriction to the next level (TailParams::rt), slot rows
+    const int* rt_col;     // in the order rt_perm gives
     const T* rt_val;
+    const int* rt_perm;
     T *b, *x, *x2, *res;
 };
 template <typename T>
@@ -766,7 +809,7 @@ __global__ void __launch_bounds__(TAIL_BS) tail_kernel(const __grid_constant__ T
             tailRows(N.n, g, nthreads, [&](int c, bool valid, int sub) {
                 const T sum = rowSum<T, TAIL_LPR>(L.rt_sl_off, L.rt_col, L.rt_val, c, valid, sub,
                                                   [&](int j) { return __ldcg(b + j); });
-                if (valid && sub == 0) N.b[c] = sum;
+                if (valid && sub == 0) N.b[L.rt_perm[c]] = sum;
             });
             cl.sync();
             continue;
@@ -1046,11 +1089,24 @@ void restrictionStructure(DevArena& ar, AmgLevel& L, int nc, cudaStream_t s) {
     PB_CUDA(cudaMemcpyAsync(L.rt_rowptr.p + nc, &nnz, sizeof(int), cudaMemcpyHostToDevice, s));
     L.rt_erow.alloc(ar, std::max(nnz, 1), s);
     entry_rows_kernel<<<grid(nc), BS, 0, s>>>(nc, L.rt_rowptr.p, L.rt_erow.p); countLaunch();
-    // SELL layout (rows: aggregates; padded slots point at column 0 with value 0)
+    // SELL-C-sigma layout (rows: aggregates, reordered within windows; padded slots
+    // point at column 0 with value 0)
     L.rt_nslices = ceil_div(nc, 32);
+    {
+        TmpBuf<unsigned> keys(nc, s), keys_s(nc, s);
+        TmpBuf<int> rows(nc, s);
+        L.rt_perm.alloc(ar, std::max(nc, 1), s);
+        rt_order_keys_kernel<<<grid(nc), BS, 0, s>>>(nc, L.rt_rowptr.p, keys.p, rows.p); countLaunch();
+        int end_bit = 8;
+        while (end_bit < 32 && (1u << (end_bit - 8)) <= (unsigned)(nc / RT_SIGMA)) ++end_bit;
+        size_t tbo = 0;
+        PB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tbo, keys.p, keys_s.p, rows.p, L.rt_perm.p, nc, 0, end_bit, s));
+        TmpBuf<unsigned char> tmpo(std::max<size_t>(tbo, 1), s);
+        PB_CUDA(cub::DeviceRadixSort::SortPairs(tmpo.p, tbo, keys.p, keys_s.p, rows.p, L.rt_perm.p, nc, 0, end_bit, s));
+    }
     TmpBuf<int> se(L.rt_nslices + 1, s);
     PB_CUDA(cudaMemsetAsync(se.p + L.rt_nslices, 0, sizeof(int), s));
-    rowlen_slice_kernel<<<grid(L.rt_nslices), BS, 0, s>>>(nc, L.rt_nslices, L.rt_rowptr.p, se.p); countLaunch();
+    rt_slice_len_kernel<<<grid(L.rt_nslices), BS, 0, s>>>(nc, L.rt_nslices, L.rt_rowptr.p, L.rt_perm.p, se.p); countLaunch();
     L.rt_sl_off.alloc(ar, L.rt_nslices + 1, s);
     size_t tb3 = 0;
     PB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb3, se.p, L.rt_sl_off.p, L.rt_nslices + 1, s));
@@ -1061,10 +1117,9 @@ void restrictionStructure(DevArena& ar, AmgLevel& L, int nc, cudaStream_t s) {
     PB_CUDA(cudaStreamSynchronize(s));
     L.rt_sl_col.alloc(ar, std::max(sell, 1), s);
     L.rt_csr_pos.alloc(ar, std::max(nnz, 1), s);
-    TmpBuf<int> dummy_diag(nc, s);
-    sell_fill_kernel<<<grid((int64_t)L.rt_nslices * 32), BS, 0, s>>>(nc, L.rt_nslices, L.rt_rowptr.p, L.rt_col.p,
-                                                                      L.rt_sl_off.p, L.rt_sl_col.p, L.rt_csr_pos.p,
-                                                                      dummy_diag.p); countLaunch();
+    rt_fill_kernel<<<grid((int64_t)L.rt_nslices * 32), BS, 0, s>>>(nc, L.rt_nslices, L.rt_rowptr.p, L.rt_col.p,
+                                                                    L.rt_perm.p, L.rt_sl_off.p, L.rt_sl_col.p,
+                                                                    L.rt_csr_pos.p); countLaunch();
     L.rt_vals.alloc(ar, std::max(sell, 1), s);
     L.rt_vals.zero(s);
     L.rt_lpr = lanesPerRow(nc, nnz);
@@ -1397,6 +1452,7 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
             t.rt_sl_off = X.rt_sl_off.p;
             t.rt_col = X.rt_sl_col.p;
             t.rt_val = CycleData<T>::rt(X);
+            t.rt_perm = X.rt_perm.p;
             t.b = xb.b;
             t.x = xb.x;
             t.x2 = k == 0 ? out : xb.x2;
@@ -1449,7 +1505,7 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
         withLpr(L.rt_lpr, [&](auto c) {
             constexpr int P = decltype(c)::value;
             launchPdl(down_kernel<T, P>, grid((int64_t)N.n * P), BS, s, N.n, (const int*)L.rt_sl_off.p,
-                      (const int*)L.rt_sl_col.p, CycleData<T>::rt(L), b, nb.b, S);
+                      (const int*)L.rt_sl_col.p, CycleData<T>::rt(L), (const int*)L.rt_perm.p, b, nb.b, S);
         });
         profEnd(slot, s);
     } else {

@@ -49,6 +49,7 @@ struct AmgLevel {
     int rt_lpr = 1, rt_nslices = 0;
     int64_t rt_nnz = 0;
     ArenaBuf<int> rt_rowptr, rt_erow, rt_col, rt_csr_pos, rt_sl_off, rt_sl_col, rt_seg, rt_src;
+    ArenaBuf<int> rt_perm;  // SELL slot row -> row of Rt (rows ordered by length within windows)
     ArenaBuf<double> rt_vals;
     ArenaBuf<float> rt_vals32;
 };
