@@ -1,5 +1,6 @@
 // krylov.cu -- SELL-32 SpMV and the BiCGSTAB / Jacobi steps of solver::BiCGSTAB
-// and solver::Jacobi (numerics/bicgstab.cpp:7-9, numerics/jacobi.cpp:5-9).
+// and solver::Jacobi (numerics/bicgstab.cpp:7-9, numerics/jacobi.cpp:5-9), and
+// flexible CG for symmetric systems (the pressure correction; PRISM_SOLVER_FCG).
 //
 // The reference solves every step() with Eigen's BiCGSTAB + IncompleteLUT to
 // machine precision. Here each step runs BiCGSTAB (van der Vorst 1992, the
@@ -234,8 +235,9 @@ __global__ void __launch_bounds__(BS) init_kernel(int n, T* __restrict__ r, cons
     }
 }
 
-// ---- flexible CG (FP64, AMG K-cycle preconditioner B): per iteration
-//   z = B r                                          AMG (applyK)
+// ---- flexible CG (FP64 recurrences; B one AMG cycle: the FP32 V-cycle, or the FP64
+// cycle with K-cycle levels): per iteration
+//   z = B r                                          AMG (apply32 / applyK)
 //   u = A z ; z.q, z.u, z.r                          SpMV + fused dots
 //   beta = (z.q)/dq ; dq' = z.u - beta (z.q) ; dr' = z.r - beta dr ; alpha = dr'/dq'
 //   d = z - beta d ; q = u - beta q ; x += alpha d ; r -= alpha q ; r.r, d.q, d.r

@@ -1,4 +1,4 @@
-// krylov.h -- BiCGSTAB / Jacobi steps and the scaled residual on a SELL-32 matrix.
+// krylov.h -- BiCGSTAB / flexible-CG / Jacobi steps and the scaled residual on a SELL-32 matrix.
 #pragma once
 
 #include "common.h"
