@@ -1352,6 +1352,12 @@ void Amg::setup(const SellMatrix& A, const int* rowptr, const int* col, bool mix
                                                        L.rt_src.p, L.rt_csr_pos.p, L.agg.p, L.vals, L.dinv.p, omega,
                                                        L.rt_vals.p, mixed ? L.rt_vals32.p : nullptr); countLaunch();
     }
+    if (verbose() && !capturing(s) && generation != reported_generation) {
+        reported_generation = generation;
+        std::fprintf(stderr, "[prism amg] hierarchy memory: %.1f MB taken, %.1f MB reserved (fine matrix %.1f MB)\n",
+                     arena.used() / 1e6, arena.reserved() / 1e6,
+                     (double)levels[0]->sell_nnz * (sizeof(double) + sizeof(int)) / 1e6);
+    }
     if (coarse_inv.p) {
         const AmgLevel& C = *levels.back();
         const int n = coarse_n;

@@ -68,6 +68,7 @@ struct Amg {
     // setup() then keeps the hierarchy's values instead of recomputing the same ones
     bool values_current = false;
     uint64_t generation = 0;  // new process-wide value whenever a buffer of the hierarchy is (re)allocated
+    uint64_t reported_generation = 0;  // PRISM_VERBOSE: the generation whose memory was last printed
     int tail = -1;            // first level of the fused coarse tail (-1: every level launches its own kernels)
     // V-cycle smoother weight and coarse-correction factor; the pressure-correction
     // equation of SIMPLE/PRIME/PISO gains from a larger over-correction

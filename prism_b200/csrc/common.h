@@ -183,6 +183,13 @@ public:
         return reinterpret_cast<T*>(p);
     }
     Mark mark() const { return {cur_, off_}; }
+    // bytes taken (up to the current position) and bytes held in chunks
+    size_t used() const {
+        size_t u = off_;
+        for (size_t i = 0; i < cur_ && i < chunks_.size(); ++i) u += chunks_[i].size;
+        return chunks_.empty() ? 0 : u;
+    }
+    size_t reserved() const { return total_; }
     void rewind(const Mark& m) {
         cur_ = m.chunk;
         off_ = m.off;
