@@ -517,26 +517,58 @@ __global__ void __launch_bounds__(BS) down_kernel(int nc, const int* __restrict_
     if (valid && sub == 0) bc[perm[row]] = sum;
 }
 
+// The finer level's xp = x + scale xc[agg] (prolongated correction plus pre-smoothed
+// x), written by the coarser level's up-sweep as soon as each coarse value is known:
+// xpv[i] = x[i] + scale out[c] for every member i of aggregate c, with x stored by the
+// finer level's pre-smoothing or formed as omega D^-1 b. The finer level's up-sweep
+// then gathers one vector per slot instead of three.
+template <typename T>
+struct FineProlong {
+    const int* m_off;  // the finer level's aggregates (= this level's rows) -> members
+    const int* m_idx;
+    const T* x;  // stored pre-smoothed x, or null
+    const T* dinv;
+    const T* b;
+    T omega, scale;
+    T* xpv;  // null: nothing to write
+};
+
 // prolongation and post-smoothing: out = xp + omega D^-1 (b - A xp), xp = x + scale * xc[agg]
-// with x = omega D^-1 b the pre-smoothed solution: stored by pre_kernel (SX), or formed
-// where it is read (after the smoothed restriction)
-template <typename T, int LPR, bool SX>
+// with x = omega D^-1 b the pre-smoothed solution. XM: 0, x formed where it is read
+// (after the smoothed restriction); 1, x stored by pre_kernel; 2, xp precomputed by the
+// coarser level (xpv). fp: this level's values prolongated to the finer level (FineProlong).
+template <typename T, int LPR, int XM>
 __global__ void __launch_bounds__(BS) post_kernel(int n, const int* __restrict__ sl_off, const int* __restrict__ col,
                                                   const T* __restrict__ val, const T* __restrict__ b,
                                                   const T* __restrict__ x, const T* __restrict__ xc,
                                                   const int* __restrict__ agg, T scale, const T* __restrict__ dinv,
-                                                  T omega, T* __restrict__ out, const KState* S) {
+                                                  T omega, T* __restrict__ out, const T* __restrict__ xpv,
+                                                  const FineProlong<T> fp, const KState* S) {
     pdlEnter();
     if (S && S->done) return;
     const int gt = blockIdx.x * BS + threadIdx.x;
     const int row = gt / LPR, sub = gt % LPR;
     const bool valid = row < n;
     auto xp = [&](int c) {
-        if constexpr (SX) return x[c] + scale * xc[agg[c]];
+        if constexpr (XM == 2) return xpv[c];
+        else if constexpr (XM == 1) return x[c] + scale * xc[agg[c]];
         else return omega * dinv[c] * b[c] + scale * xc[agg[c]];
     };
     const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, xp);
-    if (valid && sub == 0) out[row] = xp(row) + omega * dinv[row] * (b[row] - sum);
+    T o = 0;
+    if (valid && sub == 0) {
+        o = xp(row) + omega * dinv[row] * (b[row] - sum);
+        out[row] = o;
+    }
+    if (fp.xpv) {  // uniform: every lane takes part in the broadcast
+        o = __shfl_sync(0xffffffffu, o, (int)(threadIdx.x & 31) & ~(LPR - 1));
+        if (valid)
+            for (int q = fp.m_off[row] + sub; q < fp.m_off[row + 1]; q += LPR) {
+                const int i = fp.m_idx[q];
+                const T base = fp.x ? fp.x[i] : fp.omega * fp.dinv[i] * fp.b[i];
+                fp.xpv[i] = base + fp.scale * o;
+            }
+    }
 }
 
 // ---- K-cycle (FP64): two flexible-CG steps on a coarse level
@@ -1400,7 +1432,24 @@ Bufs<double> bufs64(AmgLevel& L) { return {L.b.p, L.x.p, L.x2.p, L.res.p, L.dinv
 Bufs<float> bufs32(AmgLevel& L) { return {L.b32.p, L.x32.p, L.x232.p, L.res32.p, L.dinv32.p}; }
 
 template <typename T>
-void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s, bool sample, bool kc);
+bool vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s, bool sample, bool kc,
+            const FineProlong<T>* fp = nullptr);
+
+// Whether the coarser level writes level L's xp during its up-sweep (FineProlong). It
+// saves two gathers per slot in L's up-sweep and costs the coarser up-sweep one
+// scattered write per member: a gain where L's rows are long and a loss on the 2-D
+// five-point level 0. Levels with more than 6 entries per row take it, measured on one
+// B200: 3-D 128^3 Poisson 91.4 against 95.7 ms (FP64 cycle), 95.0 against 99.0 ms
+// (FP32 cycle); 1448^2 cavity SIMPLE 24.34 against 23.94 it/s (23.75 with level 0
+// fused too). PRISM_AMG_PROLONG=0 / 1 forces it off / on.
+bool prolongFuse(const AmgLevel& L) {
+    static const int force = [] {
+        const char* e = std::getenv("PRISM_AMG_PROLONG");
+        return e && e[0] ? std::atoi(e) : -1;
+    }();
+    if (force >= 0) return force != 0;
+    return L.n > 0 && (double)L.nnz / L.n > 6.0;
+}
 
 // K-cycle on level k (FP64): z1 = N.x2 and z2 = N.kz2 from two cycles, the
 // combination coefficients in the level's scalars (see k_first_kernel)
@@ -1424,8 +1473,11 @@ void kStep(Amg& A, size_t k, const KState* S, cudaStream_t s) {
     });
 }
 
+// One cycle from level l: out = B b. fp (optional): the finer level's request for its xp
+// (FineProlong), written by this level's up-sweep; returns whether it was.
 template <typename T>
-void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s, bool sample, bool kc) {
+bool vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t s, bool sample, bool kc,
+            const FineProlong<T>* fp) {
     AmgLevel& L = *A.levels[l];
     auto B = [&](AmgLevel& X) {
         if constexpr (sizeof(T) == 8) return bufs64(X);
@@ -1468,7 +1520,7 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
         for (int k = 0; k + 1 < P.nlev; ++k)
             if (!A.levels[l + k]->use_rt || !P.L[k].rt_val) P.rt = 0;
         launchTail<T>(P, s);
-        return;
+        return false;
     }
     Bufs<T> lb = B(L);
     const T omega = (T)A.omega;
@@ -1495,7 +1547,7 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
                 cur = dst;
             }
         }
-        return;
+        return false;
     }
     AmgLevel& N = *A.levels[l + 1];
     Bufs<T> nb = B(N);
@@ -1541,18 +1593,23 @@ void vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
                           (const double*)(A.kscal.p + (size_t)KS_N * (l + 1)), lb.dinv, omega, out, S);
             });
             profEnd(slot, s);
-            return;
+            return false;
         }
     }
-    vcycle<T>(A, l + 1, nb.b, nb.x2, S, s, false, kc);
-    const int slot = fine ? profBegin(PROF_AMG_POST, sizeof(T) == 4, up_bytes + (double)sizeof(T) * N.n, s) : -1;
+    // this level's xp, written by the coarser level's up-sweep into the free res vector
+    const FineProlong<T> mine{L.m_off.p, L.m_idx.p, rt ? nullptr : (const T*)lb.x, lb.dinv, b, omega, scale, lb.res};
+    const bool have_xp = vcycle<T>(A, l + 1, nb.b, nb.x2, S, s, false, kc, prolongFuse(L) ? &mine : nullptr);
+    const FineProlong<T> request = fp ? *fp : FineProlong<T>{};
+    const double post_bytes = have_xp ? mat_bytes + 4.0 * sizeof(T) * L.n : up_bytes + (double)sizeof(T) * N.n;
+    const int slot = fine ? profBegin(PROF_AMG_POST, sizeof(T) == 4, post_bytes, s) : -1;
     withLpr(L.lpr, [&](auto c) {
         constexpr int P = decltype(c)::value;
-        auto k = rt ? post_kernel<T, P, false> : post_kernel<T, P, true>;
+        auto k = have_xp ? post_kernel<T, P, 2> : rt ? post_kernel<T, P, 0> : post_kernel<T, P, 1>;
         launchPdl(k, grid((int64_t)L.n * P), BS, s, L.n, L.sl_off, L.sl_col, vals, b, (const T*)lb.x,
-                  (const T*)nb.x2, (const int*)L.agg.p, scale, lb.dinv, omega, out, S);
+                  (const T*)nb.x2, (const int*)L.agg.p, scale, lb.dinv, omega, out, (const T*)lb.res, request, S);
     });
     profEnd(slot, s);
+    return fp != nullptr;
 }
 
 }  // namespace
