@@ -23,7 +23,7 @@ namespace pb {
 
 namespace {
 
-__device__ __align__(256) double g_jacobi_scratch[PRISM_NOALLOC_MAX_ROWS];
+static __device__ __align__(256) double g_jacobi_scratch[PRISM_NOALLOC_MAX_ROWS];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
