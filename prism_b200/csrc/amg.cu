@@ -450,8 +450,13 @@ __global__ void __launch_bounds__(1024) gauss_jordan_kernel(int n, const double*
 // few, long rows: more lanes per row keep enough loads in flight.
 
 // sum_j A[row, c_j] * xf(c_j); the result is valid in every lane of the row's group
-// (a look-ahead of 4 slots per lane measured slower for the post-smoothing kernel)
-template <typename T, int LPR, typename F>
+// (a look-ahead of 4 slots per lane measured slower for the post-smoothing kernel).
+// CS: the matrix is loaded with the evict-first hint (ld.global.cs), for the finest
+// level's restriction Rt, which no other kernel reads: its lines then leave the L2
+// first and the vectors stay (level-0 down-sweep of the 2.1M-cell cavity: 28.6 ->
+// 23.9 us live). The level-0 A is not hinted: the SpMV that follows the post-smoothing
+// shares its column indices, and hinting both kernels made them 1-2% slower.
+template <typename T, int LPR, bool CS = false, typename F>
 __device__ __forceinline__ T rowSum(const int* __restrict__ sl_off, const int* __restrict__ col,
                                     const T* __restrict__ val, int row, bool valid, int sub, F xf) {
     T sum = 0;
@@ -461,7 +466,8 @@ __device__ __forceinline__ T rowSum(const int* __restrict__ sl_off, const int* _
         const int bo = s0 + (row & 31);
         for (int j = sub; j < width; j += LPR) {
             const int p = bo + 32 * j;
-            sum += val[p] * xf(col[p]);
+            if constexpr (CS) sum += __ldcs(val + p) * xf(__ldcs(col + p));
+            else sum += val[p] * xf(col[p]);
         }
     }
     if constexpr (LPR > 1) {
@@ -503,8 +509,9 @@ __global__ void restrict_kernel(int nc, const int* m_off, const int* m_idx, cons
 }
 
 // down-sweep of a level: the next level's right-hand side bc = Rt b (smoothed
-// restriction: pre-smoothing from zero, residual and restriction in one pass)
-template <typename T, int LPR>
+// restriction: pre-smoothing from zero, residual and restriction in one pass); CS on
+// the finest level (Rt loaded evict-first, rowSum)
+template <typename T, int LPR, bool CS = false>
 __global__ void __launch_bounds__(BS) down_kernel(int nc, const int* __restrict__ sl_off, const int* __restrict__ col,
                                                   const T* __restrict__ val, const int* __restrict__ perm,
                                                   const T* __restrict__ b, T* __restrict__ bc, const KState* S) {
@@ -513,7 +520,7 @@ __global__ void __launch_bounds__(BS) down_kernel(int nc, const int* __restrict_
     const int gt = blockIdx.x * BS + threadIdx.x;
     const int row = gt / LPR, sub = gt % LPR;  // slot row; it holds row perm[row] of Rt
     const bool valid = row < nc;
-    const T sum = rowSum<T, LPR>(sl_off, col, val, row, valid, sub, [&](int j) { return b[j]; });
+    const T sum = rowSum<T, LPR, CS>(sl_off, col, val, row, valid, sub, [&](int j) { return b[j]; });
     if (valid && sub == 0) bc[perm[row]] = sum;
 }
 
@@ -1562,7 +1569,8 @@ bool vcycle(Amg& A, size_t l, const T* b, T* out, const KState* S, cudaStream_t 
         int slot = fine ? profBegin(PROF_AMG_DOWN, sizeof(T) == 4, rt_bytes, s) : -1;
         withLpr(L.rt_lpr, [&](auto c) {
             constexpr int P = decltype(c)::value;
-            launchPdl(down_kernel<T, P>, grid((int64_t)N.n * P), BS, s, N.n, (const int*)L.rt_sl_off.p,
+            auto k = l == 0 ? down_kernel<T, P, true> : down_kernel<T, P, false>;
+            launchPdl(k, grid((int64_t)N.n * P), BS, s, N.n, (const int*)L.rt_sl_off.p,
                       (const int*)L.rt_sl_col.p, CycleData<T>::rt(L), (const int*)L.rt_perm.p, b, nb.b, S);
         });
         profEnd(slot, s);
