@@ -1,6 +1,11 @@
 // capi.cpp -- the extern "C" entry points of include/prism_b200.h.
 // Every entry point converts library exceptions into a status code and keeps a
 // thread-local message for prism_last_error(); nothing throws across the ABI.
+// Every entry point is also an NVTX range named after it, so that a profiler's
+// timeline (Nsight Systems, ncu --nvtx) shows which library call issued which
+// kernels; without a tool attached the NVTX calls return at once.
+#include <nvtx3/nvToolsExt.h>
+
 #include <cstring>
 #include <new>
 
@@ -32,8 +37,16 @@ struct PrismBatch {
 namespace {
 thread_local std::string g_last_error;
 
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 template <typename F>
-int guard(F&& f) {
+int guardNamed(const char* name, F&& f) {
+    NvtxRange range(name);
     try {
         f();
         return PRISM_OK;
@@ -48,6 +61,8 @@ int guard(F&& f) {
         return PRISM_INTERNAL;
     }
 }
+// guard([&] { ... }) inside an entry point: the range takes the entry point's name
+#define guard(...) guardNamed(__func__, __VA_ARGS__)
 #define ARG(cond, msg) \
     if (!(cond)) fail(PRISM_BAD_ARG, msg)
 
