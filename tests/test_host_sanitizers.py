@@ -1,4 +1,5 @@
-"""The host mesh builder under AddressSanitizer and UndefinedBehaviorSanitizer (CPU).
+"""Host code under AddressSanitizer and UndefinedBehaviorSanitizer (CPU): the
+library's host mesh builder, and the CPU oracle every parity test compares with.
 
 prism_b200/csrc/mesh_build.cpp is the index-heavy host part of the library: UNV
 elements to faces (counting-sort face matching, the reference's face order,
@@ -10,6 +11,12 @@ reference's meshes and on generated hex and tet boxes, plain and renumbered
 (forward and reversed). Any sanitizer report makes the child exit non-zero. The
 arrays it builds are compared with the oracle's converter along the way, so the
 run covers what the device upload reads.
+
+The oracle (oracle/prism_oracle.cpp) is compiled the same way and runs the
+reference's own test cases and the synthetic configurations (SIMPLE, transient,
+advection, MUSCL transport with Green-Gauss gradients, least squares on tets,
+renumbered meshes, diagnostics); every result must equal, bit for bit, the one of
+the ordinary oracle build.
 """
 import os
 import shutil
@@ -19,6 +26,7 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SRC = os.path.join(ROOT, "oracle", "prism_oracle.cpp")
 SHIM = os.path.join(ROOT, "tests", "cpp", "mesh_build_check.cpp")
 BUILDER = os.path.join(ROOT, "prism_b200", "csrc", "mesh_build.cpp")
 
@@ -129,3 +137,92 @@ def test_mesh_builder_under_asan_and_ubsan(tmp_path):
                        timeout=600)
     assert r.returncode == 0, (r.returncode, r.stdout[-2000:], r.stderr[-4000:])
     assert "sanitized host mesh builds: 24" in r.stdout, r.stdout[-2000:]
+
+
+ORACLE_CHILD = r"""
+import ctypes as C
+import sys
+
+import numpy as np
+
+sys.path.insert(0, sys.argv[2])
+import oracle
+from prism_b200 import _abi as A
+from prism_b200 import api, meshgen
+from tests import cases
+
+san, plain = A.bind(C.CDLL(sys.argv[1]), "orc_"), oracle.lib()
+
+
+def same(a, b, what):
+    a, b = np.asarray(a), np.asarray(b)
+    assert a.shape == b.shape, what
+    if a.dtype.kind in "fc":
+        assert np.array_equal(a, b, equal_nan=True), what
+    else:
+        assert np.array_equal(a, b), what
+
+
+def refcases(lib):
+    out = {}
+    for name in ("cavity_hex", "versteeg_advection_1d", "versteeg_trans_1d", "poisson_wedge"):
+        r = cases.run_reference_test(name, lib)
+        out[name] = r if isinstance(r, dict) else {"x": r}
+    unv, case, _ = cases.load_golden("duct_simple")
+    out["duct"] = cases.simple_reference(unv, case, lib, 8, symmetry=True)
+    return out
+
+
+def synthetic(lib):
+    out = {}
+    mesh, T, U, eqn = cases.transport_c3(6, lib, conv="MUSCL")
+    for _ in range(2):
+        api.BiCGSTAB().solve(eqn, 2, 1e-12)
+    out["muscl"] = T.values()
+    c = cases.adjoint_c5(2, lib)
+    api.BiCGSTAB().solve(c["eqn"], 5, 1e-12)
+    out["tets_ls"] = c["T"].values()
+    m2, U2, p2, nu2, mdot2, eqs2 = cases.cavity(12, lib)
+    simple = api.IncompressibleSIMPLE(api.SIMPLEControls(), solver=api.BiCGSTAB())
+    for _ in range(4):
+        simple.step(eqs2, U2, mdot2, p2)
+    out["cavity_U"], out["cavity_p"] = U2.values(), p2.values()
+    out["div"] = api.ops.div(mdot2).values()
+    unv = meshgen.shuffle_cells(meshgen.box_hex(5, 4, 3, jitter=0.1, seed=4), seed=5)
+    mesh = api.Mesh(unv, cases.box_case({"T": {"left": ("fixed", 1.0)}}), lib=lib)
+    mesh.reorder(reverse=True)
+    T = api.Scalar("T", mesh, 0.0)
+    eqn = api.Transport(api.diffusion.Corrected(api.Scalar("k", mesh, 1.0), T))
+    api.BiCGSTAB().solve(eqn, 3, 1e-12)
+    out["reordered"] = T.values()
+    return out
+
+
+checked = 0
+for name, fn in (("reference cases", refcases), ("synthetic", synthetic)):
+    a, b = fn(san), fn(plain)
+    for k in b:
+        if isinstance(b[k], dict):
+            for kk in b[k]:
+                same(a[k][kk], b[k][kk], f"{k}.{kk}")
+                checked += 1
+        else:
+            same(a[k], b[k], k)
+            checked += 1
+print(f"sanitized oracle results equal: {checked}")
+"""
+
+
+def test_oracle_under_asan_and_ubsan(tmp_path):
+    gxx, asan, _ = _toolchain()
+    so = str(tmp_path / "liboracle_sanitized.so")
+    cmd = [gxx, "-std=c++20", "-O1", "-g", "-fno-omit-frame-pointer", "-fsanitize=address,undefined",
+           "-fno-sanitize-recover=undefined", "-fPIC", "-shared", "-fvisibility=hidden", "-ffp-contract=off",
+           ORACLE_SRC, "-o", so]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    env = dict(os.environ, LD_PRELOAD=asan, ASAN_OPTIONS="detect_leaks=0:abort_on_error=0:exitcode=23",
+               UBSAN_OPTIONS="halt_on_error=1:print_stacktrace=1:exitcode=24")
+    r = subprocess.run([sys.executable, "-c", ORACLE_CHILD, so, ROOT], env=env, capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, (r.returncode, r.stdout[-2000:], r.stderr[-4000:])
+    assert "sanitized oracle results equal" in r.stdout, r.stdout[-2000:]
